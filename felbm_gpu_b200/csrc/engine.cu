@@ -1,0 +1,970 @@
+// Host side of the B200 engine: brick/site layout builder, device state,
+// step sequencing (plain launches and CUDA graphs), state transfer and the
+// C-ABI of include/felbm_b200.h.
+//
+// It plays the role of the reference's struct MultiPhaseGPU
+// (include/felbm_gpu/multiphase_gpu.cuh:23-783); the reference's per-site
+// neighbour/case tables (:93-193), streaming source table (:196-208) and
+// in-place op program (:213-283) are replaced by the brick occupancy layout
+// of layout.hpp, from which the kernels derive the same cases.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/felbm_b200.h"
+#include "fe_internal.hpp"
+#include "kernels.cuh"
+
+namespace fe {
+
+static thread_local std::string g_last_error;
+int fe_fail(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+void fe_clear_error() { g_last_error.clear(); }
+
+#define FE_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t err_ = (call);                                                                     \
+    if (err_ != cudaSuccess)                                                                       \
+      return fe_fail(FE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err_) + " (" +   \
+                                      __FILE__ + ":" + std::to_string(__LINE__) + ")");            \
+  } while (0)
+
+static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  auto spread = [](uint64_t v) {
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+static int ilog2(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+
+// Host copy of one lattice's brick layout.
+struct HostLayout {
+  int nx, ny, nz, lb[3], nb[3], words;
+  int64_t n;
+  std::vector<int32_t> brick_grid, base, brick_xyz, ref_of, site_of_ref;
+  std::vector<uint64_t> mask;
+  int nbricks() const { return (int)brick_xyz.size() / 3; }
+};
+
+// Brick shape: 8x8x8 for 3-D lattices, 16x16x1 for quasi-2-D ones (nz == 1),
+// each axis clamped to the next power of two of its extent.
+static void brick_shape(int nx, int ny, int nz, int lb[3]) {
+  const int N[3] = {nx, ny, nz};
+  int B[3] = {8, 8, 8};
+  if (nz == 1) { B[0] = 16; B[1] = 16; B[2] = 1; }
+  for (int a = 0; a < 3; ++a) {
+    if (N[a] == 1) B[a] = 1;
+    else B[a] = std::min(B[a], 1 << ilog2(N[a]));
+    lb[a] = ilog2(B[a]);
+  }
+}
+
+static void build_layout(const uint8_t* solid, int nx, int ny, int nz, const int lb_in[3], HostLayout& L) {
+  L.nx = nx; L.ny = ny; L.nz = nz;
+  for (int a = 0; a < 3; ++a) L.lb[a] = lb_in[a];
+  const int B[3] = {1 << L.lb[0], 1 << L.lb[1], 1 << L.lb[2]};
+  const int N[3] = {nx, ny, nz};
+  for (int a = 0; a < 3; ++a) L.nb[a] = (N[a] + B[a] - 1) / B[a];
+  const int C = B[0] * B[1] * B[2];
+  L.words = (C + 63) / 64;
+  const int64_t total = (int64_t)nx * ny * nz;
+  // reference order: fluid nodes by increasing node index
+  std::vector<int32_t> ref_of_node(total, -1);
+  int64_t nref = 0;
+  for (int64_t node = 0; node < total; ++node)
+    if (!solid[node]) ref_of_node[node] = (int32_t)nref++;
+  L.n = nref;
+  // active bricks in Morton order
+  struct Bk { uint64_t key; int bx, by, bz; };
+  std::vector<Bk> bricks;
+  const int64_t nbt = (int64_t)L.nb[0] * L.nb[1] * L.nb[2];
+  std::vector<int32_t> cnt(nbt, 0);
+  for (int64_t node = 0; node < total; ++node) {
+    if (solid[node]) continue;
+    const int x = (int)(node % nx), y = (int)((node / nx) % ny), z = (int)(node / ((int64_t)nx * ny));
+    ++cnt[(x >> L.lb[0]) + (int64_t)L.nb[0] * ((y >> L.lb[1]) + (int64_t)L.nb[1] * (z >> L.lb[2]))];
+  }
+  for (int bz = 0; bz < L.nb[2]; ++bz)
+    for (int by = 0; by < L.nb[1]; ++by)
+      for (int bx = 0; bx < L.nb[0]; ++bx)
+        if (cnt[bx + (int64_t)L.nb[0] * (by + (int64_t)L.nb[1] * bz)] > 0)
+          bricks.push_back({morton3(bx, by, bz), bx, by, bz});
+  std::sort(bricks.begin(), bricks.end(), [](const Bk& a, const Bk& b) { return a.key < b.key; });
+  const int nbk = (int)bricks.size();
+  L.brick_grid.assign(nbt, -1);
+  L.brick_xyz.resize((size_t)nbk * 3);
+  L.mask.assign((size_t)nbk * L.words, 0ull);
+  L.base.assign((size_t)nbk * L.words, 0);
+  L.ref_of.assign(L.n, 0);
+  L.site_of_ref.assign(L.n, 0);
+  int64_t site = 0;
+  for (int b = 0; b < nbk; ++b) {
+    const Bk& k = bricks[b];
+    L.brick_grid[k.bx + (int64_t)L.nb[0] * (k.by + (int64_t)L.nb[1] * k.bz)] = b;
+    L.brick_xyz[b * 3 + 0] = k.bx; L.brick_xyz[b * 3 + 1] = k.by; L.brick_xyz[b * 3 + 2] = k.bz;
+    for (int w = 0; w < L.words; ++w) L.base[(size_t)b * L.words + w] = (int32_t)site + 0;  // fixed below
+    int64_t s0 = site;
+    for (int s = 0; s < C; ++s) {
+      const int w = s >> 6;
+      if ((s & 63) == 0) L.base[(size_t)b * L.words + w] = (int32_t)s0;
+      const int lx = s & (B[0] - 1), ly = (s >> L.lb[0]) & (B[1] - 1), lz = s >> (L.lb[0] + L.lb[1]);
+      const int x = k.bx * B[0] + lx, y = k.by * B[1] + ly, z = k.bz * B[2] + lz;
+      if (x >= nx || y >= ny || z >= nz) continue;
+      const int64_t node = x + (int64_t)nx * (y + (int64_t)ny * z);
+      if (solid[node]) continue;
+      L.mask[(size_t)b * L.words + w] |= 1ull << (s & 63);
+      L.ref_of[s0] = ref_of_node[node];
+      L.site_of_ref[ref_of_node[node]] = (int32_t)s0;
+      ++s0;
+    }
+    site = s0;
+  }
+}
+
+// Dynamic shared memory of a pass with halo H and real size rs; nfield tiles.
+static size_t tile_bytes(const HostLayout& L, int H, int rs, int nfield) {
+  const int N[3] = {L.nx, L.ny, L.nz};
+  int64_t t = 1;
+  for (int a = 0; a < 3; ++a) t *= (1 << L.lb[a]) + (N[a] > 1 ? 2 * H : 0);
+  auto al = [](int64_t b) { return (b + 15) & ~int64_t(15); };
+  return (size_t)(al(t * 4) + nfield * al(t * rs));
+}
+
+enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
+
+struct Engine {
+  fe_params P{};
+  int storage = FE_F64;
+  int device = 0;
+  HostLayout L;
+  LatDesc hd{};               // host copy of the descriptor
+  LatDesc* d_desc = nullptr;
+  int2* d_work = nullptr;
+  Ctl* d_ctl = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  double* d_tmp = nullptr;    // 2*Vn doubles for state/field transfer
+  int64_t tmp_len = 0;
+  double* d_partm = nullptr;
+  int parity = 0;             // buffer holding the current state
+  int64_t t_host = 0;
+  int64_t launches = 0;
+  size_t smem_p1 = 0, smem_p2 = 0, smem_p4 = 0;
+  bool open_bnd = false;
+  cudaGraphExec_t graph1[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+  cudaEvent_t ev_stats = nullptr;
+  bool stats_pending = false;
+  double* h_stats = nullptr;  // pinned [6]
+  double target_mass_host = 0.0;
+
+  ~Engine() { release(); }
+  void release() {
+    for (int p = 0; p < 2; ++p) {
+      if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
+      if (graph2[p]) cudaGraphExecDestroy(graph2[p]);
+      graph1[p] = graph2[p] = nullptr;
+    }
+    for (void* a : allocs) cudaFree(a);
+    allocs.clear();
+    if (d_tmp) cudaFree(d_tmp);
+    d_tmp = nullptr;
+    if (h_stats) cudaFreeHost(h_stats);
+    h_stats = nullptr;
+    if (ev_stats) cudaEventDestroy(ev_stats);
+    ev_stats = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+  }
+
+  template <class T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t err = cudaMalloc(&q, bytes);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      return fe_fail(FE_ERR_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(err));
+    }
+    allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return FE_OK;
+  }
+
+  size_t pop_size() const {
+    return storage == FE_F64 ? 8 : (storage == FE_F32 ? 4 : 2);
+  }
+  size_t fld_size() const { return storage == FE_F64 ? 8 : 4; }
+
+  void fill_prm() {
+    DevPrm& d = hd.prm;
+    d.rho0 = P.rho0; d.rho1 = P.rho1; d.drho = P.rho0 - P.rho1;
+    d.kappa = P.kappa; d.four_beta = 4.0 * P.beta; d.bnd_coeff = P.bnd_coeff;
+    d.tau0 = P.tau0; d.tau1 = P.tau1; d.mobility = P.mobility;
+    d.gx = P.gx; d.gy = P.gy; d.gz = P.gz; d.fx = P.fx; d.fy = P.fy; d.fz = P.fz;
+    d.mrt_lambda = P.mrt_lambda;
+    for (int q = 0; q < 7; ++q) {
+      d.rate_mode[q] = P.mrt_rate_mode[q];
+      d.rate_value[q] = P.mrt_rate_value[q];
+    }
+    d.use_mrt = P.use_mrt; d.hbb = P.use_halfway_bb; d.correct_mass = P.correct_op_mass;
+    d.forcing_timedep = P.forcing_timedep; d.forcing_period = P.forcing_period;
+    d.c_ref = P.c_ref; d.p_ref = P.p_ref;
+    // 16-bit deviations: h_k - w_k c_ref spans about w_k, g_k - w_k p_ref about
+    // w_k |p|; a power-of-two scale keeps the stored values near 1.
+    d.h_scale = storage >= FE_F16S ? 64.0 : 1.0;
+    d.g_scale = storage >= FE_F16S ? 64.0 : 1.0;
+  }
+  int upload_desc() {
+    FE_CUDA(cudaMemcpyAsync(d_desc, &hd, sizeof(LatDesc), cudaMemcpyHostToDevice, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+
+  int create(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid, int dev) {
+    P = *p;
+    storage = P.storage;
+    if (storage < FE_F64 || storage > FE_BF16S) return fe_fail(FE_ERR_ARG, "unknown storage");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      return fe_fail(FE_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (dev >= 0) FE_CUDA(cudaSetDevice(dev));
+    FE_CUDA(cudaGetDevice(&device));
+    FE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    int lb[3];
+    brick_shape(nx, ny, nz, lb);
+    build_layout(solid, nx, ny, nz, lb, L);
+    if (L.n == 0) return fe_fail(FE_ERR_ARG, "geometry has no fluid site");
+    if (L.n >= (int64_t)1 << 31) return fe_fail(FE_ERR_ARG, "more than 2^31 sites");
+    const int nbk = L.nbricks();
+    LatDesc& D = hd;
+    D.nx = nx; D.ny = ny; D.nz = nz;
+    D.lbx = L.lb[0]; D.lby = L.lb[1]; D.lbz = L.lb[2];
+    D.nbx = L.nb[0]; D.nby = L.nb[1]; D.nbz = L.nb[2];
+    D.words = L.words;
+    D.nbricks = nbk;
+    D.n = L.n;
+    D.n_pad = (L.n + AOSOA - 1) / AOSOA * AOSOA;
+    int rc;
+    int32_t *bg, *bs, *bx, *rf;
+    uint64_t* mk;
+    if ((rc = alloc(&bg, L.brick_grid.size()))) return rc;
+    if ((rc = alloc(&mk, L.mask.size()))) return rc;
+    if ((rc = alloc(&bs, L.base.size()))) return rc;
+    if ((rc = alloc(&bx, L.brick_xyz.size()))) return rc;
+    if ((rc = alloc(&rf, L.ref_of.size()))) return rc;
+    FE_CUDA(cudaMemcpy(bg, L.brick_grid.data(), L.brick_grid.size() * 4, cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemcpy(mk, L.mask.data(), L.mask.size() * 8, cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemcpy(bs, L.base.data(), L.base.size() * 4, cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemcpy(bx, L.brick_xyz.data(), L.brick_xyz.size() * 4, cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemcpy(rf, L.ref_of.data(), L.ref_of.size() * 4, cudaMemcpyHostToDevice));
+    D.brick_grid = bg; D.mask = mk; D.base = bs; D.brick_xyz = bx; D.ref_of = rf;
+    const size_t popn = (size_t)Q * D.n_pad;
+    for (int b = 0; b < 2; ++b)
+      for (int f = 0; f < 2; ++f) {
+        unsigned char* q;
+        if ((rc = alloc(&q, popn * pop_size()))) return rc;
+        FE_CUDA(cudaMemset(q, 0, popn * pop_size()));
+        D.pop[b][f] = q;
+      }
+    void** flds[] = {&D.c, &D.p, &D.jx, &D.jy, &D.jz, &D.mu, &D.lapmu};
+    for (void** f : flds) {
+      unsigned char* q;
+      if ((rc = alloc(&q, (size_t)D.n * fld_size()))) return rc;
+      FE_CUDA(cudaMemset(q, 0, (size_t)D.n * fld_size()));
+      *f = q;
+    }
+    if ((rc = alloc(&D.part1, (size_t)nbk * 2))) return rc;
+    if ((rc = alloc(&D.part4, (size_t)nbk * 6))) return rc;
+    FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * 6 * 8));
+    if ((rc = alloc(&d_partm, (size_t)nbk * 2))) return rc;
+    if ((rc = alloc(&d_ctl, 1))) return rc;
+    Ctl c0{};
+    c0.ff_manual = 1.0;
+    FE_CUDA(cudaMemcpy(d_ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice));
+    D.ctl = d_ctl;
+    fill_prm();
+    if ((rc = alloc(&d_desc, 1))) return rc;
+    std::vector<int2> work(nbk);
+    for (int b = 0; b < nbk; ++b) work[b] = make_int2(0, b);
+    if ((rc = alloc(&d_work, work.size()))) return rc;
+    FE_CUDA(cudaMemcpy(d_work, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    const int rs = (int)fld_size();
+    smem_p1 = tile_bytes(L, 1, rs, 0);
+    smem_p2 = tile_bytes(L, 1, rs, 1);
+    smem_p4 = tile_bytes(L, 2, rs, 3);
+    if ((rc = set_smem_attrs())) return rc;
+    FE_CUDA(cudaMallocHost(&h_stats, 6 * sizeof(double)));
+    FE_CUDA(cudaEventCreateWithFlags(&ev_stats, cudaEventDisableTiming));
+    return upload_desc();
+  }
+
+  template <class S>
+  int set_smem_attrs_t() {
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p4));
+    return FE_OK;
+  }
+  int set_smem_attrs() {
+    if (smem_p4 <= 48 * 1024) return FE_OK;
+    switch (storage) {
+      case FE_F64: return set_smem_attrs_t<StF64>();
+      case FE_F32: return set_smem_attrs_t<StF32>();
+      case FE_F16S: return set_smem_attrs_t<StF16S>();
+      default: return set_smem_attrs_t<StBF16S>();
+    }
+  }
+
+  // ---- one step (plain launches) -----------------------------------------
+  template <class S>
+  void launch_step_t(int par, cudaStream_t st, cudaEvent_t* ev) {
+    const int nb = hd.nbricks;
+    auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
+    rec(0);
+    k_moments<S><<<nb, CTA, smem_p1, st>>>(d_desc, d_work, par);
+    rec(1);
+    if (open_bnd) {
+      const int nio = hd.n_inlet + hd.n_outlet;
+      if (nio) k_bc_fields<S><<<(nio + 255) / 256, 256, 0, st>>>(d_desc, 0);
+      if (hd.prm.copy_to_buf && hd.n_buf) k_bc_buffers<S><<<(hd.n_buf + 255) / 256, 256, 0, st>>>(d_desc, 0);
+      launches += (nio ? 1 : 0) + ((hd.prm.copy_to_buf && hd.n_buf) ? 1 : 0);
+    }
+    rec(2);
+    k_cfield<S, 0><<<nb, CTA, smem_p2, st>>>(d_desc, d_work, FieldOut{});
+    rec(3);
+    k_lapmu<S><<<nb, CTA, smem_p2, st>>>(d_desc, d_work);
+    rec(4);
+    if (hd.prm.use_mrt) k_collide<S, 1><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
+    else k_collide<S, 0><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
+    rec(5);
+    launches += 4;
+  }
+  void launch_step(int par, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+    switch (storage) {
+      case FE_F64: launch_step_t<StF64>(par, st, ev); break;
+      case FE_F32: launch_step_t<StF32>(par, st, ev); break;
+      case FE_F16S: launch_step_t<StF16S>(par, st, ev); break;
+      default: launch_step_t<StBF16S>(par, st, ev); break;
+    }
+  }
+  int kernels_per_step() const {
+    int k = 4;
+    if (open_bnd) k += (hd.n_inlet + hd.n_outlet ? 1 : 0) + ((hd.prm.copy_to_buf && hd.n_buf) ? 1 : 0);
+    return k;
+  }
+
+  int set_ctl_mode(int run_mode, double ff) {
+    // ff_auto / auto_correct / ff_manual are contiguous in Ctl
+    struct { int32_t auto_correct, ff_auto; double ff_manual; } m{run_mode ? 1 : 0, run_mode ? 1 : 0, ff};
+    static_assert(offsetof(Ctl, ff_auto) == offsetof(Ctl, auto_correct) + 4, "Ctl layout");
+    static_assert(offsetof(Ctl, ff_manual) == offsetof(Ctl, auto_correct) + 8, "Ctl layout");
+    FE_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(d_ctl) + offsetof(Ctl, auto_correct), &m, sizeof(m),
+                            cudaMemcpyHostToDevice, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+
+  double ff_manual = 1.0;
+
+  int step(int nsteps) {
+    int rc;
+    if ((rc = set_ctl_mode(0, ff_manual))) return rc;
+    for (int s = 0; s < nsteps; ++s) {
+      launch_step(parity, stream);
+      parity ^= 1;
+    }
+    FE_CUDA(cudaGetLastError());
+    t_host += nsteps;
+    return FE_OK;
+  }
+
+  int build_graphs() {
+    for (int p = 0; p < 2; ++p) {
+      for (int len = 1; len <= 2; ++len) {
+        cudaGraph_t g;
+        FE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t saved = launches;
+        for (int s = 0; s < len; ++s) launch_step(p ^ (s & 1), stream);
+        launches = saved;
+        cudaError_t e1 = cudaStreamEndCapture(stream, &g);
+        if (e1 != cudaSuccess) return fe_fail(FE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e1));
+        cudaGraphExec_t ex;
+        cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) return fe_fail(FE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+        (len == 1 ? graph1 : graph2)[p] = ex;
+      }
+    }
+    return FE_OK;
+  }
+  void drop_graphs() {
+    for (int p = 0; p < 2; ++p) {
+      if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
+      if (graph2[p]) cudaGraphExecDestroy(graph2[p]);
+      graph1[p] = graph2[p] = nullptr;
+    }
+  }
+
+  int run(int nsteps) {
+    int rc;
+    if ((rc = set_ctl_mode(1, ff_manual))) return rc;
+    if (!graph1[0] && (rc = build_graphs())) return rc;
+    const int kps = kernels_per_step();
+    int s = 0;
+    while (s < nsteps) {
+      if (nsteps - s >= 2) {
+        FE_CUDA(cudaGraphLaunch(graph2[parity], stream));
+        s += 2;  // two steps: parity unchanged
+        launches += 2 * kps;
+      } else {
+        FE_CUDA(cudaGraphLaunch(graph1[parity], stream));
+        parity ^= 1;
+        s += 1;
+        launches += kps;
+      }
+    }
+    t_host += nsteps;
+    FE_CUDA(cudaGetLastError());
+    return FE_OK;
+  }
+
+  int ensure_tmp(int64_t len) {
+    if (tmp_len >= len) return FE_OK;
+    if (d_tmp) cudaFree(d_tmp);
+    d_tmp = nullptr;
+    tmp_len = 0;
+    cudaError_t err = cudaMalloc(&d_tmp, (size_t)len * sizeof(double));
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      return fe_fail(FE_ERR_MEMORY, "transfer buffer");
+    }
+    tmp_len = len;
+    return FE_OK;
+  }
+
+  template <class S>
+  int mass_t() {
+    k_mass<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity, d_partm);
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    return FE_OK;
+  }
+  int mass_pass() {
+    switch (storage) {
+      case FE_F64: return mass_t<StF64>();
+      case FE_F32: return mass_t<StF32>();
+      case FE_F16S: return mass_t<StF16S>();
+      default: return mass_t<StBF16S>();
+    }
+  }
+
+  int read_ctl(Ctl* c) {
+    FE_CUDA(cudaMemcpyAsync(c, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+  int write_ctl_field(size_t off, const void* v, size_t sz) {
+    FE_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(d_ctl) + off, v, sz, cudaMemcpyHostToDevice, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+
+  template <class S>
+  int download_t(double* h, double* g) {
+    const int64_t Vn = (int64_t)Q * hd.n;
+    int rc;
+    if ((rc = ensure_tmp(2 * Vn))) return rc;
+    Ctl c;
+    if ((rc = read_ctl(&c))) return rc;
+    int apply = 0;
+    if (c.pending && hd.prm.correct_mass) {
+      if ((rc = mass_t<S>())) return rc;
+      apply = 1;
+    }
+    k_download_state<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity, d_tmp, d_tmp + Vn, apply);
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    FE_CUDA(cudaMemcpyAsync(h, d_tmp, Vn * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaMemcpyAsync(g, d_tmp + Vn, Vn * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+  int download(double* h, double* g) {
+    switch (storage) {
+      case FE_F64: return download_t<StF64>(h, g);
+      case FE_F32: return download_t<StF32>(h, g);
+      case FE_F16S: return download_t<StF16S>(h, g);
+      default: return download_t<StBF16S>(h, g);
+    }
+  }
+
+  template <class S>
+  int upload_t(const double* h, const double* g) {
+    const int64_t Vn = (int64_t)Q * hd.n;
+    int rc;
+    if ((rc = ensure_tmp(2 * Vn))) return rc;
+    FE_CUDA(cudaMemcpyAsync(d_tmp, h, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
+    FE_CUDA(cudaMemcpyAsync(d_tmp + Vn, g, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
+    k_upload_state<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity, d_tmp, d_tmp + Vn);
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    int32_t zero = 0;
+    if ((rc = write_ctl_field(offsetof(Ctl, pending), &zero, 4))) return rc;
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+  int upload(const double* h, const double* g) {
+    switch (storage) {
+      case FE_F64: return upload_t<StF64>(h, g);
+      case FE_F32: return upload_t<StF32>(h, g);
+      case FE_F16S: return upload_t<StF16S>(h, g);
+      default: return upload_t<StBF16S>(h, g);
+    }
+  }
+
+  // download()/download_raw(): P1 (+BC) and P2 in output mode, no step.
+  template <class S>
+  int fields_t(const fe_fields* f) {
+    const int64_t n = hd.n;
+    int rc;
+    if ((rc = ensure_tmp(7 * n))) return rc;
+    Ctl c;
+    if ((rc = read_ctl(&c))) return rc;
+    if ((rc = set_ctl_mode(0, ff_manual))) return rc;
+    // P1 with the queued correction (pending stays set: no collision runs)
+    k_moments<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity);
+    if (open_bnd) {
+      const int nio = hd.n_inlet + hd.n_outlet;
+      if (nio) k_bc_fields<S><<<(nio + 255) / 256, 256, 0, stream>>>(d_desc, 0);
+      if (hd.prm.copy_to_buf && hd.n_buf) k_bc_buffers<S><<<(hd.n_buf + 255) / 256, 256, 0, stream>>>(d_desc, 0);
+    }
+    FieldOut o{d_tmp + 0 * n, d_tmp + 1 * n, d_tmp + 2 * n, d_tmp + 3 * n, d_tmp + 4 * n, d_tmp + 5 * n, d_tmp + 6 * n};
+    k_cfield<S, 1><<<hd.nbricks, CTA, smem_p2, stream>>>(d_desc, d_work, o);
+    launches += 2;
+    FE_CUDA(cudaGetLastError());
+    double* dst[7] = {f->rho, f->c, f->ux, f->uy, f->uz, f->p, f->mu};
+    for (int q = 0; q < 7; ++q)
+      if (dst[q]) FE_CUDA(cudaMemcpyAsync(dst[q], d_tmp + q * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    // the moment pass leaves lambda for the collision of a step; a download
+    // does not consume the queued correction
+    double zero = 0.0;
+    return write_ctl_field(offsetof(Ctl, lambda), &zero, 8);
+  }
+  int fields(const fe_fields* f) {
+    switch (storage) {
+      case FE_F64: return fields_t<StF64>(f);
+      case FE_F32: return fields_t<StF32>(f);
+      case FE_F16S: return fields_t<StF16S>(f);
+      default: return fields_t<StBF16S>(f);
+    }
+  }
+
+  int stats_launch() {
+    k_stats_finalize<<<1, CTA, 0, stream>>>(d_desc, 0);
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    FE_CUDA(cudaMemcpyAsync(h_stats, reinterpret_cast<char*>(d_ctl) + offsetof(Ctl, stats), 6 * sizeof(double),
+                            cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaEventRecord(ev_stats, stream));
+    stats_pending = true;
+    return FE_OK;
+  }
+  int stats_collect(double out[6]) {
+    if (!stats_pending) return fe_fail(FE_ERR_STATE, "no flow statistics pending");
+    FE_CUDA(cudaEventSynchronize(ev_stats));
+    for (int q = 0; q < 6; ++q) out[q] = h_stats[q];
+    stats_pending = false;
+    return FE_OK;
+  }
+};
+
+}  // namespace fe
+
+using fe::Engine;
+
+struct fe_engine {
+  Engine e;
+};
+
+static const char* FE_VERSION = "felbm_b200 0.1 (sm_100a)";
+
+#define FE_GUARD(e) \
+  if (!(e)) return fe_fail(FE_ERR_ARG, "null engine")
+
+extern "C" {
+
+const char* fe_last_error(void) { return fe::g_last_error.c_str(); }
+const char* fe_version(void) { return FE_VERSION; }
+
+int fe_params_default(fe_params* p) {
+  if (!p) return fe_fail(FE_ERR_ARG, "null params");
+  std::memset(p, 0, sizeof(*p));
+  p->rho0 = 1.0; p->rho1 = 1.0; p->tau0 = 1.0; p->tau1 = 1.0;
+  p->interface_width = 4.0; p->surface_tension = 1e-3; p->mobility_coeff = 0.02; p->phi = 0.0;
+  p->forcing_timedep = FE_FORCING_CONSTANT; p->forcing_period = 10000.0;
+  p->use_mrt = 0; p->mrt_lambda = 0.1875;
+  for (int q = 1; q < 7; ++q) p->mrt_rate_mode[q] = fe::mrt_reference_mode(q);
+  p->use_halfway_bb = 1;
+  p->storage = FE_F64;
+  p->c_ref = 0.5; p->p_ref = 0.0;
+  return fe_params_derive(p);
+}
+
+int fe_params_derive(fe_params* p) {
+  if (!p) return fe_fail(FE_ERR_ARG, "null params");
+  if (p->interface_width <= 0) return fe_fail(FE_ERR_ARG, "interface_width must be > 0");
+  p->kappa = 1.5 * p->interface_width * p->surface_tension;
+  p->beta = 12.0 * p->surface_tension / p->interface_width;
+  p->mobility = p->beta != 0.0 ? p->mobility_coeff / p->beta : 0.0;
+  p->bnd_coeff = (std::fabs(p->kappa) < 1e-16) ? 0.0 : p->phi / p->kappa;
+  return FE_OK;
+}
+
+int fe_engine_create(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid, int device,
+                     fe_engine** out) {
+  if (!p || !solid || !out || nx < 1 || ny < 1 || nz < 1) return fe_fail(FE_ERR_ARG, "fe_engine_create: bad arguments");
+  *out = nullptr;
+  fe_engine* e = new (std::nothrow) fe_engine();
+  if (!e) return fe_fail(FE_ERR_MEMORY, "host allocation");
+  const int rc = e->e.create(p, nx, ny, nz, solid, device);
+  if (rc) {
+    delete e;
+    return rc;
+  }
+  *out = e;
+  return FE_OK;
+}
+
+int fe_engine_destroy(fe_engine* e) {
+  if (!e) return FE_OK;
+  cudaStreamSynchronize(e->e.stream);
+  delete e;
+  return FE_OK;
+}
+
+int fe_engine_size(const fe_engine* e, int64_t* n, int64_t* vn) {
+  FE_GUARD(e);
+  if (n) *n = e->e.hd.n;
+  if (vn) *vn = (int64_t)fe::Q * e->e.hd.n;
+  return FE_OK;
+}
+
+void* fe_engine_stream(fe_engine* e) { return e ? (void*)e->e.stream : nullptr; }
+
+int fe_set_params(fe_engine* e, const fe_params* p) {
+  FE_GUARD(e);
+  if (!p) return fe_fail(FE_ERR_ARG, "null params");
+  if (p->storage != e->e.storage) return fe_fail(FE_ERR_ARG, "storage cannot change after create");
+  if (p->correct_op_mass && e->e.open_bnd)
+    return fe_fail(FE_ERR_ARG, "correct_op_mass must be false with open boundaries");
+  // fill_prm leaves the open-boundary block of fe_set_open_bnd untouched
+  e->e.P = *p;
+  e->e.fill_prm();
+  e->e.drop_graphs();
+  return e->e.upload_desc();
+}
+
+int fe_upload_state(fe_engine* e, const double* h, const double* g, int64_t vn) {
+  FE_GUARD(e);
+  if (!h || !g || vn != (int64_t)fe::Q * e->e.hd.n) return fe_fail(FE_ERR_ARG, "fe_upload_state: size mismatch");
+  return e->e.upload(h, g);
+}
+
+int fe_download_state(fe_engine* e, double* h, double* g, int64_t vn) {
+  FE_GUARD(e);
+  if (!h || !g || vn != (int64_t)fe::Q * e->e.hd.n) return fe_fail(FE_ERR_ARG, "fe_download_state: size mismatch");
+  return e->e.download(h, g);
+}
+
+int fe_set_open_bnd(fe_engine* e, const fe_open_bnd* b) {
+  FE_GUARD(e);
+  if (!b) return fe_fail(FE_ERR_ARG, "null open boundary");
+  Engine& E = e->e;
+  if (E.P.correct_op_mass)
+    return fe_fail(FE_ERR_ARG, "correct_op_mass must be false with open boundaries (felbm_gpu_main.cu:245-252)");
+  if (E.open_bnd) return fe_fail(FE_ERR_STATE, "open boundaries already set");
+  const int64_t n = E.hd.n;
+  auto check = [&](const int32_t* a, int cnt) {
+    if (cnt < 0 || (cnt > 0 && !a)) return false;
+    for (int j = 0; j < cnt; ++j)
+      if (a[j] < 0 || a[j] >= n) return false;
+    return true;
+  };
+  if (!check(b->inlet, b->n_inlet) || !check(b->outlet, b->n_outlet) ||
+      !check(b->buf_verts, b->n_buf) || !check(b->buf_refs, b->n_buf))
+    return fe_fail(FE_ERR_ARG, "fe_set_open_bnd: site index out of range");
+  // convert reference-order site indices to engine order
+  auto conv = [&](const int32_t* a, int cnt) {
+    std::vector<int32_t> v(cnt);
+    for (int j = 0; j < cnt; ++j) v[j] = E.L.site_of_ref[a[j]];
+    return v;
+  };
+  std::vector<int32_t> io = conv(b->inlet, b->n_inlet), out = conv(b->outlet, b->n_outlet);
+  io.insert(io.end(), out.begin(), out.end());
+  std::vector<int32_t> bv = conv(b->buf_verts, b->n_buf), br = conv(b->buf_refs, b->n_buf);
+  // flags (multiphase_gpu.cuh:378-389 for BC_PROC)
+  std::vector<uint8_t> flag(n, 0);
+  std::vector<int32_t> src(n, 0);
+  const bool in_proc = b->use_in_vel || b->use_in_prs || b->use_in_fluid;
+  const bool out_proc = b->use_out_prs || b->use_out_fluid;
+  for (int j = 0; j < b->n_inlet; ++j) {
+    const int32_t i = io[j];
+    flag[i] |= fe::BC_SITE | (in_proc ? fe::BC_PROC : 0) | (b->copy_to_buffers ? 0 : fe::BC_G_OVER);
+    src[i] = i;
+  }
+  for (int j = 0; j < b->n_outlet; ++j) {
+    const int32_t i = io[b->n_inlet + j];
+    flag[i] |= fe::BC_SITE | (out_proc ? fe::BC_PROC : 0) | (b->copy_to_buffers ? 0 : fe::BC_G_OVER);
+    src[i] = i;
+  }
+  if (b->copy_to_buffers)
+    for (int j = 0; j < b->n_buf; ++j) {
+      flag[bv[j]] |= fe::BC_SITE | fe::BC_PROC | fe::BC_G_OVER;
+      src[bv[j]] = br[j];
+    }
+  int rc;
+  uint8_t* dflag;
+  int32_t *dsrc, *dlist, *dbv = nullptr, *dbr = nullptr;
+  double* dcoord = nullptr;
+  unsigned char *craw, *ubc;
+  if ((rc = E.alloc(&dflag, n))) return rc;
+  if ((rc = E.alloc(&dsrc, n))) return rc;
+  if ((rc = E.alloc(&dlist, io.size()))) return rc;
+  if ((rc = E.alloc(&craw, n * E.fld_size()))) return rc;
+  if ((rc = E.alloc(&ubc, 3 * n * E.fld_size()))) return rc;
+  FE_CUDA(cudaMemcpy(dflag, flag.data(), n, cudaMemcpyHostToDevice));
+  FE_CUDA(cudaMemcpy(dsrc, src.data(), n * 4, cudaMemcpyHostToDevice));
+  if (!io.empty()) FE_CUDA(cudaMemcpy(dlist, io.data(), io.size() * 4, cudaMemcpyHostToDevice));
+  FE_CUDA(cudaMemset(craw, 0, n * E.fld_size()));
+  FE_CUDA(cudaMemset(ubc, 0, 3 * n * E.fld_size()));
+  if (b->inlet_coord && b->n_inlet) {
+    if ((rc = E.alloc(&dcoord, b->n_inlet))) return rc;
+    FE_CUDA(cudaMemcpy(dcoord, b->inlet_coord, b->n_inlet * 8, cudaMemcpyHostToDevice));
+  }
+  if (b->n_buf) {
+    if ((rc = E.alloc(&dbv, b->n_buf))) return rc;
+    if ((rc = E.alloc(&dbr, b->n_buf))) return rc;
+    FE_CUDA(cudaMemcpy(dbv, bv.data(), b->n_buf * 4, cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemcpy(dbr, br.data(), b->n_buf * 4, cudaMemcpyHostToDevice));
+  }
+  fe::LatDesc& D = E.hd;
+  D.bcflag = dflag; D.bcsrc = dsrc; D.bc_list = dlist; D.bc_coord = dcoord;
+  D.c_raw_bc = craw; D.u_bc = ubc;
+  D.n_inlet = b->n_inlet; D.n_outlet = b->n_outlet; D.n_buf = b->copy_to_buffers ? b->n_buf : 0;
+  D.buf_verts = dbv; D.buf_refs = dbr;
+  fe::DevPrm& d = D.prm;
+  d.open_bnd = 1; d.copy_to_buf = b->copy_to_buffers;
+  d.use_in_vel = b->use_in_vel; d.use_in_prs = b->use_in_prs; d.use_in_fluid = b->use_in_fluid;
+  d.use_out_prs = b->use_out_prs; d.use_out_fluid = b->use_out_fluid;
+  d.u_in[0] = b->u_in_x; d.u_in[1] = b->u_in_y; d.u_in[2] = b->u_in_z;
+  d.p_in = b->p_in; d.p_out = b->p_out; d.c_out_fixed = b->c_out_fixed; d.rho_out_fixed = b->rho_out_fixed;
+  d.inlet_c_a = b->inlet_c_a; d.inlet_mode = b->inlet_mode;
+  d.inlet_period = b->inlet_period; d.inlet_duty = b->inlet_duty; d.inlet_ramp = b->inlet_ramp;
+  d.split_pos = b->split_pos;
+  E.open_bnd = true;
+  E.drop_graphs();
+  return E.upload_desc();
+}
+
+int fe_step(fe_engine* e, int nsteps) {
+  FE_GUARD(e);
+  if (nsteps < 0) return fe_fail(FE_ERR_ARG, "nsteps < 0");
+  return e->e.step(nsteps);
+}
+
+int fe_run(fe_engine* e, int nsteps) {
+  FE_GUARD(e);
+  if (nsteps < 0) return fe_fail(FE_ERR_ARG, "nsteps < 0");
+  return e->e.run(nsteps);
+}
+
+int fe_set_time(fe_engine* e, int64_t t) {
+  FE_GUARD(e);
+  e->e.t_host = t;
+  return e->e.write_ctl_field(offsetof(fe::Ctl, t), &t, 8);
+}
+
+int fe_get_time(const fe_engine* e, int64_t* t) {
+  FE_GUARD(e);
+  fe::Ctl c;
+  int rc = const_cast<Engine&>(e->e).read_ctl(&c);
+  if (rc) return rc;
+  if (t) *t = c.t;
+  return FE_OK;
+}
+
+int fe_set_forcing_factor(fe_engine* e, double ff) {
+  FE_GUARD(e);
+  e->e.ff_manual = ff;
+  return FE_OK;
+}
+
+int fe_apply_mass_correction(fe_engine* e, double* drift) {
+  FE_GUARD(e);
+  Engine& E = e->e;
+  if (!E.P.correct_op_mass) {
+    if (drift) *drift = 0.0;
+    return FE_OK;
+  }
+  int32_t one = 1;
+  int rc;
+  if (drift) {
+    // queue, then form M and lambda now so that the drift can be returned
+    if ((rc = E.write_ctl_field(offsetof(fe::Ctl, pending), &one, 4))) return rc;
+    if ((rc = E.mass_pass())) return rc;
+    fe::Ctl c;
+    if ((rc = E.read_ctl(&c))) return rc;
+    *drift = c.drift;
+    return FE_OK;
+  }
+  return E.write_ctl_field(offsetof(fe::Ctl, pending), &one, 4);
+}
+
+int fe_record_target_mass(fe_engine* e) {
+  FE_GUARD(e);
+  Engine& E = e->e;
+  int rc;
+  if ((rc = E.mass_pass())) return rc;
+  fe::Ctl c;
+  if ((rc = E.read_ctl(&c))) return rc;
+  // a queued correction moves the total to the old target; record that value
+  double m = c.M;
+  if (c.pending && E.hd.prm.correct_mass && c.W > 0.0 && c.lambda != 0.0) m = c.M - c.lambda * c.W;
+  E.target_mass_host = m;
+  return E.write_ctl_field(offsetof(fe::Ctl, target_mass), &m, 8);
+}
+
+int fe_set_target_mass(fe_engine* e, double m0) {
+  FE_GUARD(e);
+  e->e.target_mass_host = m0;
+  return e->e.write_ctl_field(offsetof(fe::Ctl, target_mass), &m0, 8);
+}
+
+int fe_get_target_mass(const fe_engine* e, double* m0) {
+  FE_GUARD(e);
+  if (m0) *m0 = e->e.target_mass_host;
+  return FE_OK;
+}
+
+int fe_current_mass(fe_engine* e, double* m) {
+  FE_GUARD(e);
+  Engine& E = e->e;
+  int rc;
+  if ((rc = E.mass_pass())) return rc;
+  fe::Ctl c;
+  if ((rc = E.read_ctl(&c))) return rc;
+  double v = c.M;
+  if (c.pending && E.hd.prm.correct_mass && c.W > 0.0 && c.lambda != 0.0) v = c.M - c.lambda * c.W;
+  if (m) *m = v;
+  return FE_OK;
+}
+
+int fe_download_fields(fe_engine* e, const fe_fields* f) {
+  FE_GUARD(e);
+  if (!f) return fe_fail(FE_ERR_ARG, "null fields");
+  return e->e.fields(f);
+}
+
+int fe_flow_stats(fe_engine* e, double out[6]) {
+  FE_GUARD(e);
+  int rc;
+  if ((rc = e->e.stats_launch())) return rc;
+  return e->e.stats_collect(out);
+}
+int fe_flow_stats_launch(fe_engine* e) {
+  FE_GUARD(e);
+  return e->e.stats_launch();
+}
+int fe_flow_stats_ready(fe_engine* e, int* ready) {
+  FE_GUARD(e);
+  if (!ready) return fe_fail(FE_ERR_ARG, "null");
+  if (!e->e.stats_pending) { *ready = 0; return FE_OK; }
+  cudaError_t q = cudaEventQuery(e->e.ev_stats);
+  if (q != cudaSuccess && q != cudaErrorNotReady) return fe_fail(FE_ERR_CUDA, cudaGetErrorString(q));
+  *ready = (q == cudaSuccess) ? 1 : 0;
+  return FE_OK;
+}
+int fe_flow_stats_collect(fe_engine* e, double out[6]) {
+  FE_GUARD(e);
+  return e->e.stats_collect(out);
+}
+
+int fe_time_run(fe_engine* e, int nsteps, float* ms_total) {
+  FE_GUARD(e);
+  Engine& E = e->e;
+  cudaEvent_t a, b;
+  FE_CUDA(cudaEventCreate(&a));
+  FE_CUDA(cudaEventCreate(&b));
+  int rc = E.set_ctl_mode(1, E.ff_manual);
+  if (!rc && !E.graph1[0]) rc = E.build_graphs();
+  if (rc) { cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
+  FE_CUDA(cudaStreamSynchronize(E.stream));
+  FE_CUDA(cudaEventRecord(a, E.stream));
+  rc = E.run(nsteps);
+  FE_CUDA(cudaEventRecord(b, E.stream));
+  FE_CUDA(cudaEventSynchronize(b));
+  float ms = 0.f;
+  FE_CUDA(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ms_total) *ms_total = ms;
+  return rc;
+}
+
+// Per-kernel device time over nsteps plain-launched steps: out[0] P1, [1] the
+// open-boundary kernels, [2] P2, [3] P3, [4] P4 (summed ms).
+int fe_time_kernels(fe_engine* e, int nsteps, float* ms, int nk) {
+  FE_GUARD(e);
+  if (!ms || nk < fe::K_N) return fe_fail(FE_ERR_ARG, "need 5 outputs");
+  Engine& E = e->e;
+  cudaEvent_t ev[6];
+  for (auto& x : ev) FE_CUDA(cudaEventCreate(&x));
+  for (int q = 0; q < fe::K_N; ++q) ms[q] = 0.f;
+  int rc = E.set_ctl_mode(1, E.ff_manual);
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; ++s) {
+    E.launch_step(E.parity, E.stream, ev);
+    E.parity ^= 1;
+    FE_CUDA(cudaEventSynchronize(ev[5]));
+    for (int q = 0; q < fe::K_N; ++q) {
+      float t = 0.f;
+      FE_CUDA(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+      ms[q] += t;
+    }
+  }
+  E.t_host += nsteps;
+  for (auto& x : ev) cudaEventDestroy(x);
+  FE_CUDA(cudaGetLastError());
+  return FE_OK;
+}
+
+int fe_launch_count(const fe_engine* e, int64_t* count) {
+  FE_GUARD(e);
+  if (count) *count = e->e.launches;
+  return FE_OK;
+}
+
+}  // extern "C"

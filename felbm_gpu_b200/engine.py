@@ -1,0 +1,236 @@
+"""Python mirror of the reference engine interface over the C-ABI.
+
+``MultiPhaseGPU`` keeps the member names of the reference's
+``struct felbm_gpu::MultiPhaseGPU`` (include/felbm_gpu/multiphase_gpu.cuh):
+``init``-time construction, ``upload_state``, ``set_open_bnd``, ``step``,
+``apply_mass_correction``, ``record_target_mass``, ``set_target_mass`` /
+``get_target_mass``, ``current_mass``, ``download_state``, ``download``,
+``flow_stats`` (+ ``_launch`` / ``_ready`` / ``_collect``), ``state_size``
+and ``free``. Errors raise ``FeError`` instead of exiting the process.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import check, lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i32(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def default_params(**kw) -> capi.FeParams:
+    """Reference defaults (fe_params_default) overridden by keyword cfg keys,
+    then the derived kappa, beta, mobility, bnd_coeff (fe_params_derive)."""
+    p = capi.FeParams()
+    check(lib.fe_params_default(C.byref(p)))
+    for k, v in kw.items():
+        if k == "storage" and isinstance(v, str):
+            v = capi.STORAGE[v]
+        if k in ("mrt_rate_mode", "mrt_rate_value"):
+            arr = getattr(p, k)
+            for i, x in v.items() if isinstance(v, dict) else enumerate(v):
+                arr[i] = x
+            continue
+        if not hasattr(p, k):
+            raise KeyError(f"unknown parameter {k}")
+        setattr(p, k, v)
+    check(lib.fe_params_derive(C.byref(p)))
+    return p
+
+
+@dataclass
+class OpenBoundary:
+    """Open inlet/outlet description (reference set_open_bnd + DevParams block)."""
+    inlet: np.ndarray
+    outlet: np.ndarray
+    inlet_coord: np.ndarray | None = None
+    buf_verts: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    buf_refs: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    copy_to_buffers: bool = False
+    use_in_vel: bool = False
+    use_in_prs: bool = False
+    use_in_fluid: bool = False
+    use_out_prs: bool = False
+    use_out_fluid: bool = False
+    u_in: tuple = (0.0, 0.0, 0.0)
+    p_in: float = 0.0
+    p_out: float = 0.0
+    c_out_fixed: float = 0.0
+    rho_out_fixed: float = 1.0
+    inlet_c_a: float = 1.0
+    inlet_mode: int = 0
+    split_axis: int = 0
+    inlet_period: float = 0.0
+    inlet_duty: float = 0.5
+    inlet_ramp: float = 0.0
+    split_pos: float = 0.0
+
+    def to_c(self):
+        """Build the fe_open_bnd struct; returns (struct, keepalive list)."""
+        keep = []
+        b = capi.FeOpenBnd()
+        a, pa = _i32(self.inlet); keep.append(a)
+        o, po = _i32(self.outlet); keep.append(o)
+        bv, pbv = _i32(self.buf_verts); keep.append(bv)
+        br, pbr = _i32(self.buf_refs); keep.append(br)
+        b.n_inlet, b.inlet = len(a), pa
+        b.n_outlet, b.outlet = len(o), po
+        b.n_buf, b.buf_verts, b.buf_refs = len(bv), pbv, pbr
+        if self.inlet_coord is not None:
+            ic = np.ascontiguousarray(self.inlet_coord, dtype=np.float64)
+            keep.append(ic)
+            b.inlet_coord = _dptr(ic)
+        for k in ("copy_to_buffers", "use_in_vel", "use_in_prs", "use_in_fluid", "use_out_prs", "use_out_fluid",
+                  "inlet_mode", "split_axis"):
+            setattr(b, k, int(getattr(self, k)))
+        b.u_in_x, b.u_in_y, b.u_in_z = self.u_in
+        for k in ("p_in", "p_out", "c_out_fixed", "rho_out_fixed", "inlet_c_a", "inlet_period", "inlet_duty",
+                  "inlet_ramp", "split_pos"):
+            setattr(b, k, float(getattr(self, k)))
+        return b, keep
+
+
+class MultiPhaseGPU:
+    """One lattice on one GPU (reference MultiPhaseGPU, multiphase_gpu.cuh:23)."""
+
+    def __init__(self, params: capi.FeParams, solid: np.ndarray, device: int = -1):
+        solid = np.ascontiguousarray(solid, dtype=np.uint8)
+        if solid.ndim != 3:
+            raise ValueError("solid must be a (nz, ny, nx) array")
+        nz, ny, nx = solid.shape
+        self.shape = (nz, ny, nx)
+        self.params = params
+        h = C.c_void_p()
+        check(lib.fe_engine_create(C.byref(params), nx, ny, nz, solid.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                   device, C.byref(h)))
+        self._h = h
+        n, vn = C.c_int64(), C.c_int64()
+        check(lib.fe_engine_size(self._h, C.byref(n), C.byref(vn)))
+        self.n, self.Vn = n.value, vn.value
+
+    # -- lifecycle --------------------------------------------------------
+    def free(self):
+        if self._h:
+            lib.fe_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def state_size(self) -> int:
+        return self.Vn
+
+    def set_params(self, params: capi.FeParams):
+        self.params = params
+        check(lib.fe_set_params(self._h, C.byref(params)))
+
+    # -- state ------------------------------------------------------------
+    def upload_state(self, h: np.ndarray, g: np.ndarray):
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        check(lib.fe_upload_state(self._h, _dptr(h), _dptr(g), self.Vn))
+
+    def download_state(self):
+        h = np.empty(self.Vn, np.float64)
+        g = np.empty(self.Vn, np.float64)
+        check(lib.fe_download_state(self._h, _dptr(h), _dptr(g), self.Vn))
+        return h, g
+
+    def set_open_bnd(self, ob: OpenBoundary):
+        b, keep = ob.to_c()
+        check(lib.fe_set_open_bnd(self._h, C.byref(b)))
+        del keep
+
+    # -- stepping ---------------------------------------------------------
+    def step(self, nsteps: int = 1):
+        check(lib.fe_step(self._h, nsteps))
+
+    def run(self, nsteps: int):
+        check(lib.fe_run(self._h, nsteps))
+
+    def set_forcing_factor(self, ff: float):
+        check(lib.fe_set_forcing_factor(self._h, ff))
+
+    def set_time(self, t: int):
+        check(lib.fe_set_time(self._h, t))
+
+    def get_time(self) -> int:
+        t = C.c_int64()
+        check(lib.fe_get_time(self._h, C.byref(t)))
+        return t.value
+
+    def apply_mass_correction(self, want_drift: bool = True):
+        d = C.c_double()
+        check(lib.fe_apply_mass_correction(self._h, C.byref(d) if want_drift else None))
+        return d.value if want_drift else None
+
+    def record_target_mass(self):
+        check(lib.fe_record_target_mass(self._h))
+
+    def set_target_mass(self, m0: float):
+        check(lib.fe_set_target_mass(self._h, m0))
+
+    def get_target_mass(self) -> float:
+        d = C.c_double()
+        check(lib.fe_get_target_mass(self._h, C.byref(d)))
+        return d.value
+
+    def current_mass(self) -> float:
+        d = C.c_double()
+        check(lib.fe_current_mass(self._h, C.byref(d)))
+        return d.value
+
+    # -- readout ----------------------------------------------------------
+    def download(self) -> dict:
+        """Fields c, rho, ux, uy, uz, p, mu refreshed from the current state."""
+        out = {k: np.empty(self.n, np.float64) for k in ("rho", "c", "ux", "uy", "uz", "p", "mu")}
+        f = capi.FeFields(*[_dptr(out[k]) for k in ("rho", "c", "ux", "uy", "uz", "p", "mu")])
+        check(lib.fe_download_fields(self._h, C.byref(f)))
+        return out
+
+    def flow_stats(self) -> np.ndarray:
+        out = np.empty(6, np.float64)
+        check(lib.fe_flow_stats(self._h, _dptr(out)))
+        return out
+
+    def flow_stats_launch(self):
+        check(lib.fe_flow_stats_launch(self._h))
+
+    def flow_stats_ready(self) -> bool:
+        r = C.c_int()
+        check(lib.fe_flow_stats_ready(self._h, C.byref(r)))
+        return bool(r.value)
+
+    def flow_stats_collect(self) -> np.ndarray:
+        out = np.empty(6, np.float64)
+        check(lib.fe_flow_stats_collect(self._h, _dptr(out)))
+        return out
+
+    # -- diagnostics ------------------------------------------------------
+    def time_run(self, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib.fe_time_run(self._h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def time_kernels(self, nsteps: int) -> np.ndarray:
+        ms = (C.c_float * 5)()
+        check(lib.fe_time_kernels(self._h, nsteps, ms, 5))
+        return np.array(ms[:], dtype=np.float64)
+
+    def launch_count(self) -> int:
+        c = C.c_int64()
+        check(lib.fe_launch_count(self._h, C.byref(c)))
+        return c.value

@@ -1,0 +1,253 @@
+/*
+ * felbm_b200 — C-ABI of the B200-native Lee–Liu free-energy multiphase D3Q19
+ * step over the sparse fluid-site set of a porous geometry.
+ *
+ * Every entry point replaces one member of the reference's header-only engine
+ * `struct felbm_gpu::MultiPhaseGPU` (include/felbm_gpu/multiphase_gpu.cuh) or a
+ * piece of its driver (src/felbm_gpu_main.cu). The citation above each
+ * declaration names the reference interface it stands for.
+ *
+ * Conventions (differences from the reference are deliberate):
+ *  - every call returns an int status (FE_OK = 0); nothing calls exit()
+ *    (the reference exits the process on any CUDA error, gpu_common.cuh:14-22);
+ *    fe_last_error() returns a message for the last failure on this thread;
+ *  - distributions cross the boundary as double, in the reference's layout
+ *    f[k*n + i], with sites i numbered in the reference order: fluid nodes in
+ *    increasing node index x + nx*(y + ny*z);
+ *  - the engine owns all device memory; host arrays belong to the caller;
+ *  - one engine is driven by one host thread at a time; all its work is
+ *    queued on the engine's own CUDA stream.
+ */
+#ifndef FELBM_B200_H
+#define FELBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FE_OK 0
+#define FE_ERR_ARG 1        /* invalid argument / size mismatch            */
+#define FE_ERR_CUDA 2       /* CUDA runtime error                           */
+#define FE_ERR_NO_DEVICE 3  /* no usable CUDA device                        */
+#define FE_ERR_MEMORY 4     /* device or host allocation refused            */
+#define FE_ERR_STATE 5      /* call not valid in the engine's current state */
+#define FE_ERR_IO 6         /* file could not be read or written            */
+#define FE_ERR_DIVERGED 7   /* non-finite or runaway state detected         */
+
+/* Population storage of the state arrays. Arithmetic is FP64 for FE_F64 and
+ * FP32 in registers for the others; FE_F16S / FE_BF16S store each population as
+ * a scaled deviation from its rest-state value w_k*(c_ref | p_ref). */
+#define FE_F64 0
+#define FE_F32 1
+#define FE_F16S 2
+#define FE_BF16S 3
+
+/* forcing_timedep (reference felbm_gpu_main.cu:587-594) */
+#define FE_FORCING_CONSTANT 0
+#define FE_FORCING_SINUSOIDAL 1
+#define FE_FORCING_SQUARE 2
+
+/* MRT rate kinds (index into mrt_rate_mode / mrt_rate_value) and modes. */
+#define FE_MRT_E 1
+#define FE_MRT_EPS 2
+#define FE_MRT_Q 3
+#define FE_MRT_NU 4
+#define FE_MRT_PI 5
+#define FE_MRT_M 6
+#define FE_RATE_S0 0    /* the site's BGK rate 1/(tau+1/2)               */
+#define FE_RATE_MAGIC 1 /* 2 tau/(2 Lambda + tau), reference default     */
+#define FE_RATE_FIXED 2 /* mrt_rate_value[kind]                          */
+
+/* Physics and solver switches. Field names follow the reference's cfg keys
+ * (params.cfg / settings.cfg) and DevParams (device_engine.cuh:31-59). Fill
+ * the raw keys, then call fe_params_derive() for kappa, beta, mobility and
+ * bnd_coeff (reference compare_cpu_gpu.cu:115-118). */
+typedef struct fe_params {
+  /* params.cfg */
+  double rho0, rho1;             /* phase densities (phase 0 has c = 1)      */
+  double tau0, tau1;             /* relaxation times                         */
+  double interface_width;        /* W                                        */
+  double surface_tension;        /* sigma                                    */
+  double mobility_coeff;         /* mobility = mobility_coeff / beta         */
+  double phi;                    /* wetting potential, 6 sigma cos(theta)    */
+  /* derived by fe_params_derive */
+  double kappa, beta, mobility, bnd_coeff;
+  /* settings.cfg */
+  double gx, gy, gz;             /* acceleration_[xyz]                       */
+  double fx, fy, fz;             /* forcing_[xyz], scaled by forcing_factor  */
+  int forcing_timedep;           /* FE_FORCING_*                             */
+  double forcing_period;
+  int use_mrt;
+  double mrt_lambda;             /* magic parameter, default 0.1875          */
+  int mrt_rate_mode[7];          /* per FE_MRT_* kind; [0] unused            */
+  double mrt_rate_value[7];
+  int use_halfway_bb;
+  int correct_op_mass;
+  /* fast-path switches of the reference (cfg keys). All of them select the
+   * one fused path here; they are kept so configs and logs round-trip. */
+  int stream_matrix_free, grad_matrix_free, fused, fuse_collision;
+  int mrt_fast_transform, stream_inplace;
+  /* storage of the populations, FE_F64 .. FE_BF16S */
+  int storage;
+  /* reference scale of the FE_F16S/FE_BF16S deviations (ignored otherwise) */
+  double c_ref, p_ref;
+} fe_params;
+
+/* Open inlet/outlet (reference MultiPhaseGPU::set_open_bnd,
+ * multiphase_gpu.cuh:369-400, plus the DevParams open-boundary block
+ * device_engine.cuh:45-58 that the driver fills, felbm_gpu_main.cu:334-380).
+ * Node lists are site indices in the reference order. */
+typedef struct fe_open_bnd {
+  int n_inlet;  const int32_t* inlet;
+  const double* inlet_coord;     /* per inlet node, coordinate along split axis
+                                    (modes split/stripes), or NULL */
+  int n_outlet; const int32_t* outlet;
+  int n_buf;    const int32_t* buf_verts; const int32_t* buf_refs;
+  int copy_to_buffers;
+  int use_in_vel, use_in_prs, use_in_fluid, use_out_prs, use_out_fluid;
+  double u_in_x, u_in_y, u_in_z;
+  double p_in, p_out;
+  double c_out_fixed, rho_out_fixed;
+  double inlet_c_a;              /* 1 - inlet_fluid                          */
+  int inlet_mode;                /* 0 single, 1 alternate, 2 split, 3 stripes */
+  int split_axis;
+  double inlet_period, inlet_duty, inlet_ramp, split_pos;
+} fe_open_bnd;
+
+/* Macroscopic fields, each n doubles in the reference site order
+ * (reference RawFields, multiphase_gpu.cuh:730). Any pointer may be NULL. */
+typedef struct fe_fields {
+  double *rho, *c, *ux, *uy, *uz, *p, *mu;
+} fe_fields;
+
+typedef struct fe_engine fe_engine;
+
+/* ---- parameters -------------------------------------------------------- */
+/* Defaults of the reference: switches off, BGK, lambda 0.1875, reference MRT
+ * rate assignment, FP64 storage. */
+int fe_params_default(fe_params* p);
+/* kappa = 1.5 W sigma, beta = 12 sigma / W, mobility = coeff / beta,
+ * bnd_coeff = phi / kappa (reference compare_cpu_gpu.cu:115-118). */
+int fe_params_derive(fe_params* p);
+
+/* ---- lifecycle --------------------------------------------------------- */
+/* Replaces MultiPhaseGPU::init (multiphase_gpu.cuh:75-351). The geometry is a
+ * solid mask over nx*ny*nz nodes (1 = solid), node index x + nx*(y + ny*z);
+ * streaming wraps periodically on every axis (reference README "What is and
+ * isn't periodic"). device < 0 keeps the current device. */
+int fe_engine_create(const fe_params* p, int nx, int ny, int nz,
+                     const uint8_t* solid, int device, fe_engine** out);
+/* Replaces MultiPhaseGPU::free (multiphase_gpu.cuh:759-782). */
+int fe_engine_destroy(fe_engine* e);
+/* Number of sites n and state size Vn = 19 n (reference state_size(),
+ * multiphase_gpu.cuh:457). */
+int fe_engine_size(const fe_engine* e, int64_t* n, int64_t* vn);
+/* Replaces writes to MultiPhaseGPU::params() (multiphase_gpu.cuh:362) for the
+ * physics block; takes effect at the next step. */
+int fe_set_params(fe_engine* e, const fe_params* p);
+/* The CUDA stream the engine queues its work on (cudaStream_t). */
+void* fe_engine_stream(fe_engine* e);
+
+/* ---- state ------------------------------------------------------------- */
+/* Replaces upload_state (multiphase_gpu.cuh:354-359): h, g are Vn doubles. */
+int fe_upload_state(fe_engine* e, const double* h, const double* g, int64_t vn);
+/* Replaces download_state (multiphase_gpu.cuh:449-455); includes a pending
+ * order-parameter mass correction, as the reference's state would. */
+int fe_download_state(fe_engine* e, double* h, double* g, int64_t vn);
+
+/* ---- open boundaries --------------------------------------------------- */
+/* Replaces set_open_bnd + the driver's DevParams fill. Call before stepping. */
+int fe_set_open_bnd(fe_engine* e, const fe_open_bnd* b);
+
+/* ---- stepping ---------------------------------------------------------- */
+/* Replaces MultiPhaseGPU::step() (multiphase_gpu.cuh:522-631), nsteps times,
+ * without mass correction (the driver calls that separately). */
+int fe_step(fe_engine* e, int nsteps);
+/* Replaces apply_mass_correction() (multiphase_gpu.cuh:689-700). When drift
+ * is non-NULL the drift M - M0 is computed now and returned (a blocking
+ * reduction, as in the reference); when NULL the correction is queued and
+ * fused into the next step's moment pass. No-op unless correct_op_mass. */
+int fe_apply_mass_correction(fe_engine* e, double* drift);
+/* The driver's hot loop (felbm_gpu_main.cu:741-745): nsteps x (step + mass
+ * correction), with forcing_factor_at(t) evaluated per step from the
+ * engine's step counter; replayed through a CUDA graph. */
+int fe_run(fe_engine* e, int nsteps);
+/* Step counter t used by forcing_factor_at and by fe_run (the driver's loop
+ * index, felbm_gpu_main.cu:701); set it after a restart. */
+int fe_set_time(fe_engine* e, int64_t t);
+int fe_get_time(const fe_engine* e, int64_t* t);
+/* Replaces the driver's `gpu.P.forcing_factor = ...` (felbm_gpu_main.cu:743)
+ * for fe_step; fe_run computes it from the step counter instead. */
+int fe_set_forcing_factor(fe_engine* e, double ff);
+
+/* ---- order-parameter mass target -------------------------------------- */
+/* record_target_mass / set_target_mass / get_target_mass / current_mass
+ * (multiphase_gpu.cuh:458-459,685-687). */
+int fe_record_target_mass(fe_engine* e);
+int fe_set_target_mass(fe_engine* e, double m0);
+int fe_get_target_mass(const fe_engine* e, double* m0);
+int fe_current_mass(fe_engine* e, double* m);
+
+/* ---- readout ----------------------------------------------------------- */
+/* Replaces download()/download_raw() (multiphase_gpu.cuh:704-757): refresh the
+ * macroscopic fields from the current state (moments, open-boundary field
+ * enforcement, mu, velocity/pressure correction) and copy them out. */
+int fe_download_fields(fe_engine* e, const fe_fields* f);
+/* Replaces flow_stats (multiphase_gpu.cuh:645-651): out = {sum ux, sum uy,
+ * sum uz, sum u^2, sum c, max u^2} of the fields of the last step. */
+int fe_flow_stats(fe_engine* e, double out[6]);
+/* Asynchronous form (flow_stats_launch / _ready / _collect, :658-683). */
+int fe_flow_stats_launch(fe_engine* e);
+int fe_flow_stats_ready(fe_engine* e, int* ready);
+int fe_flow_stats_collect(fe_engine* e, double out[6]);
+
+/* ---- geometry and initial-condition front end -------------------------
+ * Replace the felbm_local DomainInitializer_* / InitializerMultiPhase_* the
+ * reference driver calls (felbm_gpu_main.cu:256-311); seeded and
+ * platform-independent. Masks: nx*ny*nz uint8, 1 = solid. */
+/* Gaussian random field, correlation exp(-r^2/(2 corr_len^2)), fluid below the
+ * porosity quantile, largest cluster percolating along flow_axis kept
+ * (flow_axis < 0: largest cluster; open_flow: no wrap along flow_axis). */
+int fe_geom_grf(int nx, int ny, int nz, double corr_len, double porosity, uint64_t seed,
+                int flow_axis, int open_flow, uint8_t* solid, double* porosity_out);
+/* Random sequential disc pack (radii U[rmin,rmax], periodic gap) extruded in z. */
+int fe_geom_cylinders(int nx, int ny, int nz, double rmin, double rmax, double porosity, double gap,
+                      uint64_t seed, int keep_largest, uint8_t* solid, double* porosity_out);
+/* Up to max_number spheres of one radius, centre distance >= 2r + distance
+ * (compare_cpu_gpu.cu:165-175 "spheres_repulsive"). */
+int fe_geom_spheres(int nx, int ny, int nz, double radius, int max_number, double distance,
+                    uint64_t seed, uint8_t* solid);
+/* Open inlet/outlet padding (empty_layers, buffer_layers, extrude_buffers). */
+int fe_geom_pad_open(const uint8_t* medium, int mx, int my, int mz, int flow_axis, int empty_layers,
+                     int buffer_layers, int* dims_out, uint8_t* out_solid);
+/* SubDomain::inlet_verts/outlet_verts/buffer_verts/buffer_refs of a padded domain. */
+int fe_geom_open_lists(const uint8_t* solid, int nx, int ny, int nz, int flow_axis, int buffer_layers,
+                       int split_axis, int32_t* n_counts, int32_t* inlet, int32_t* outlet,
+                       int32_t* buf_verts, int32_t* buf_refs, double* inlet_coord);
+/* Site count and node index of each site (SubDomain::idx_to_coords). */
+int fe_geom_sites(const uint8_t* solid, int nx, int ny, int nz, int64_t* n, int64_t* nodes);
+/* Order parameter per site: kind 0 uniform, 1 slab_interface, 2 spherical_droplet. */
+int fe_init_order_parameter(const uint8_t* solid, int nx, int ny, int nz, int kind, const double* a,
+                            double width, double* c_out);
+/* Plain equilibrium h, g of per-site fields (u may be NULL). */
+int fe_init_equilibrium(int64_t n, const double* c, const double* p, const double* ux, const double* uy,
+                        const double* uz, double rho0, double rho1, double* h, double* g);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* Time nsteps of fe_run with CUDA events on the engine's stream; ms_total is
+ * the device time, ms_collide the summed device time of the fused collision
+ * kernel measured in a separate instrumented pass of nsteps_collide steps. */
+int fe_time_run(fe_engine* e, int nsteps, float* ms_total);
+int fe_time_kernels(fe_engine* e, int nsteps, float* ms_per_kernel, int nkernels);
+/* Number of kernels the engine launched since creation. */
+int fe_launch_count(const fe_engine* e, int64_t* count);
+const char* fe_last_error(void);
+const char* fe_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FELBM_B200_H */

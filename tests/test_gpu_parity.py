@@ -1,0 +1,85 @@
+"""B200 engine vs the CPU oracle on the same seeded inputs (the reference's
+compare_cpu_gpu design, src/compare_cpu_gpu.cu:244-294: identical initial
+distributions, diff of h, g and of the macroscopic fields).
+
+Tolerances (stated contract): FP64 storage max|dh|, max|dg|, and the fields
+c, rho, u, p, mu <= 1e-12 after 100 steps; FP32 storage <= 1e-6 relative
+(max|d| / max|ref|) after 100 steps.
+"""
+import numpy as np
+import pytest
+
+from cases import CASES, make_case
+from parity import maxdiff, reldiff, run_engine, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-6
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_100_steps(require_gpu, name):
+    case = make_case(name)
+    h, g, f, st, nl = run_engine(case, 100, "f64")
+    ho, go, fo, sto = run_oracle(case, 100)
+    assert nl > 0
+    assert maxdiff(h, ho) <= TOL64, maxdiff(h, ho)
+    assert maxdiff(g, go) <= TOL64, maxdiff(g, go)
+    for k in ("c", "rho", "ux", "uy", "uz", "p", "mu"):
+        assert maxdiff(f[k], fo[k]) <= TOL64, (k, maxdiff(f[k], fo[k]))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_100_steps(require_gpu, name):
+    case = make_case(name)
+    h, g, f, _, _ = run_engine(case, 100, "f32")
+    ho, go, fo, _ = run_oracle(case, 100)
+    assert reldiff(h, ho) <= TOL32, reldiff(h, ho)
+    assert reldiff(g, go) <= TOL32, reldiff(g, go)
+    for k in ("c", "rho", "p"):
+        assert reldiff(f[k], fo[k]) <= TOL32, (k, reldiff(f[k], fo[k]))
+
+
+@pytest.mark.parametrize("name", ["spheres_mrt", "grf_mrt_mass", "openbnd_bgk"])
+def test_step_api_matches_run(require_gpu, name):
+    """fe_step + fe_apply_mass_correction (the reference driver's call pair)
+    gives the same state as the fused fe_run loop."""
+    case = make_case(name)
+    h1, g1, _, _, _ = run_engine(case, 20, "f64", mode="step")
+    h2, g2, _, _, _ = run_engine(case, 20, "f64", mode="run")
+    assert maxdiff(h1, h2) <= 1e-14
+    assert maxdiff(g1, g2) <= 1e-14
+
+
+@pytest.mark.parametrize("name", ["spheres_mrt_wet", "grf_mrt_mass"])
+def test_flow_stats(require_gpu, name):
+    """Monitoring reductions (reference k_flow_stats) of the last step."""
+    case = make_case(name)
+    _, _, _, st, _ = run_engine(case, 30, "f64")
+    _, _, _, sto = run_oracle(case, 30)
+    assert np.allclose(st, sto, rtol=1e-10, atol=1e-14), (st, sto)
+
+
+@pytest.mark.parametrize("storage,tol", [("f64", 1e-12), ("f32", 1e-8)])
+def test_mass_correction_restores_target(require_gpu, storage, tol):
+    """README.md:150-158: the correction restores the total order-parameter
+    mass to M0 up to floating-point summation. Measured on the downloaded
+    state (sum of h in FP64), after 50 and after 200 steps, so a drift that
+    accumulates would show. The FP32 bound is the rounding floor of ~3.6k
+    sites (each site's h rounded to FP32 after the injection)."""
+    from felbm_gpu_b200 import MultiPhaseGPU
+    from parity import with_storage
+    case = make_case("grf_mrt_mass")
+    e = MultiPhaseGPU(with_storage(case.params, storage), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        e.record_target_mass()
+        m0 = e.get_target_mass()
+        for steps in (50, 150):
+            e.run(steps)
+            h, _ = e.download_state()
+            m = float(np.sum(h))
+            assert abs(m - m0) / abs(m0) <= tol, (storage, steps, m, m0)
+    finally:
+        e.free()
