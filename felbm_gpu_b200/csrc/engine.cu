@@ -321,14 +321,23 @@ struct Engine {
     return upload_desc();
   }
 
+  // Opt every pass kernel in to the dynamic shared memory it needs (the
+  // default limit is 48 KB minus the kernel's static TileShared block).
   template <class S>
   int set_smem_attrs_t() {
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p4));
+    const int a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 0>, (cudaFuncAttribute)a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 1>, (cudaFuncAttribute)a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_cfield<S, 0>, (cudaFuncAttribute)a, (int)smem_p2));
+    FE_CUDA(cudaFuncSetAttribute(k_cfield<S, 1>, (cudaFuncAttribute)a, (int)smem_p2));
+    FE_CUDA(cudaFuncSetAttribute(k_lapmu<S>, (cudaFuncAttribute)a, (int)smem_p2));
+    FE_CUDA(cudaFuncSetAttribute(k_moments<S>, (cudaFuncAttribute)a, (int)smem_p1));
+    FE_CUDA(cudaFuncSetAttribute(k_mass<S>, (cudaFuncAttribute)a, (int)smem_p1));
+    FE_CUDA(cudaFuncSetAttribute(k_download_state<S>, (cudaFuncAttribute)a, (int)smem_p1));
+    FE_CUDA(cudaFuncSetAttribute(k_upload_state<S>, (cudaFuncAttribute)a, (int)smem_p1));
     return FE_OK;
   }
   int set_smem_attrs() {
-    if (smem_p4 <= 48 * 1024) return FE_OK;
     switch (storage) {
       case FE_F64: return set_smem_attrs_t<StF64>();
       case FE_F32: return set_smem_attrs_t<StF32>();

@@ -141,13 +141,19 @@ __device__ void tile_setup(const LatDesc& D, int brick, TileShared& ts) {
     const int h = N > 1 ? H : 0;
     const int T = B + 2 * h;
     const int origin = D.brick_xyz[brick * 3 + a] * B - h;
+    // A tile spans B + 2h <= 20 consecutive positions (mod N), which touch at
+    // most 4 distinct bricks per axis (two partial bricks across the wrap);
+    // the bound check below only guards against a layout the host never builds.
     int nu = 0;
-    for (int t = 0; t < T; ++t) {
+    for (int t = 0; t < T && t < MAX_T; ++t) {
       const int X = mod_pos(origin + t, N);
       const int bc = X >> lb;
       int s = 0;
       while (s < nu && ts.ucoord[a][s] != bc) ++s;
-      if (s == nu) { ts.ucoord[a][nu] = bc; ++nu; }
+      if (s == nu) {
+        if (nu == MAX_SEG) { atomicOr(&D.ctl->status, 2); s = 0; }
+        else { ts.ucoord[a][nu] = bc; ++nu; }
+      }
       ts.seg[a][t] = (uint8_t)s;
       ts.loc[a][t] = (uint8_t)(X & (B - 1));
     }
@@ -497,8 +503,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     if (OUT) {
       const int64_t q = D.ref_of[i];
       out.c[q] = (double)c0;
-      out.rho[q] = (flag & BC_SITE) && !Pm.use_in_fluid && !Pm.use_out_fluid ? (double)(rho1 + drho * cm_)
-                                                                               : (double)rho;
+      out.rho[q] = (double)rho;
       out.ux[q] = (double)ux;
       out.uy[q] = (double)uy;
       out.uz[q] = (double)uz;

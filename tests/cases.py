@@ -51,16 +51,21 @@ def make_case(name: str, **over) -> Case:
         p = default_params(**kw)
         h, g = _ic(solid, p, "droplet", 4.0, centre=(8, 8, 8), radius=4.0)
         return Case(name, solid, p, h, g)
-    if name == "cyl2d_mrt":           # quasi-2-D cylinder pack, BASELINE rates, slab, body force
+    if name == "cyl2d_mrt":           # quasi-2-D cylinder pack, slab, body force
+        # rates: the BASELINE's explicit s_e = s_eps = 1.19, s_q = 1.2 (nu from tau),
+        # or with ref_rates=True the reference's own assignment (device_engine.cuh:625),
+        # which is what the reference's kernels can run
+        ref_rates = bool(over.pop("ref_rates", False))
         solid, _ = geometry.cylinders((1, 48, 64), 3.0, 6.0, 0.65, 12345)
         kw = dict(rho0=1.0, rho1=1.0, tau0=1.0, tau1=1.0, surface_tension=1e-3, interface_width=4.0,
                   mobility_coeff=0.02, use_mrt=1, use_halfway_bb=1, gx=1e-5,
                   phi=6 * 1e-3 * np.cos(np.radians(60.0)))
         kw.update(over)
         p = default_params(**kw)
-        for k, v in ((1, 1.19), (2, 1.19), (3, 1.2)):
-            p.mrt_rate_mode[k] = 2
-            p.mrt_rate_value[k] = v
+        if not ref_rates:
+            for k, v in ((1, 1.19), (2, 1.19), (3, 1.2)):
+                p.mrt_rate_mode[k] = 2
+                p.mrt_rate_value[k] = v
         h, g = _ic(solid, p, "slab", 4.0, origin=(0, 0, 0), axis=0, thickness=32)
         return Case(name, solid, p, h, g)
     if name in ("grf_mrt_mass", "grf_bgk_mass"):  # porous GRF, mass correction, wetting, body force

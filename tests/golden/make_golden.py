@@ -29,7 +29,7 @@ from oracle.oracle_py import Oracle  # noqa: E402
 STEPS = 20
 SPECS = [
     ("fluid_bgk", {}), ("spheres_bgk", {}), ("spheres_mrt", {}), ("spheres_mrt_wet", {}),
-    ("cyl2d_mrt", {}), ("grf_mrt_mass", {}), ("grf_bgk_mass", {}),
+    ("cyl2d_mrt", {"ref_rates": True}), ("grf_mrt_mass", {}), ("grf_bgk_mass", {}),
     ("openbnd_bgk", {}), ("openbnd_bgk", {"inlet_mode": 1}), ("openbnd_bgk", {"inlet_mode": 2}),
     ("openbnd_mrt_buf", {}), ("openbnd_mrt_buf", {"inlet_mode": 4}),
 ]
@@ -54,12 +54,14 @@ def main(outdir):
         f = r.fields()
         r.close()
         sel = np.sort(rng.choice(len(h), size=min(1500, len(h)), replace=False))
+        sites = np.sort(rng.choice(o.n, size=min(400, o.n), replace=False))
         tag = name + "".join(f"_{k}{v}" for k, v in kw.items())
-        out = dict(case=name, steps=STEPS, sel=sel, h=h[sel], g=g[sel], h_sum=h.sum(), g_sum=g.sum())
+        out = dict(case=name, steps=STEPS, sel=sel, h=h[sel], g=g[sel], h_sum=h.sum(), g_sum=g.sum(),
+                   sites=sites)
         for k, v in kw.items():
             out["kw_" + k] = np.array(v)
         for k, v in f.items():
-            out["f_" + k] = v
+            out["f_" + k] = v[sites]
         np.savez_compressed(os.path.join(outdir, f"ref_{tag}.npz"), **out)
         print("wrote", tag, "n =", o.n)
 
