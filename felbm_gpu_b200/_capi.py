@@ -104,6 +104,7 @@ SIGNATURES = {
     "fe_flow_stats_launch": (C.c_int, [_vp]),
     "fe_flow_stats_ready": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "fe_flow_stats_collect": (C.c_int, [_vp, _dp]),
+    "fe_mass_weight_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "fe_time_run": (C.c_int, [_vp, C.c_int, _fp]),
     "fe_time_kernels": (C.c_int, [_vp, C.c_int, _fp, C.c_int]),
     "fe_launch_count": (C.c_int, [_vp, _i64p]),

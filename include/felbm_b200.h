@@ -236,6 +236,24 @@ int fe_init_order_parameter(const uint8_t* solid, int nx, int ny, int nz, int ki
 int fe_init_equilibrium(int64_t n, const double* c, const double* p, const double* ux, const double* uy,
                         const double* uz, double rho0, double rho1, double* h, double* g);
 
+/* ---- allocation-free reduction -----------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory (their pool allocator owns the GPU's memory, or their loop must not
+ * enter cudaMalloc/cudaFree, which can synchronize the device): the
+ * order-parameter mass M = sum_i c_i and interface weight
+ * W = sum_i max(c_i (1 - c_i), 0), c_i = sum_k h[k*n + i], of FP64
+ * populations h in the caller's device memory, written to d_out[0], d_out[1]
+ * (caller's device memory) on `stream` (cudaStream_t, NULL = legacy default).
+ * It allocates nothing: its partial sums live in one fixed array of 262,400
+ * bytes inside the library, present on every GPU that loads the library
+ * until the process exits. n above FE_NOALLOC_MAX_SITES is rejected with
+ * FE_ERR_ARG. All calls on a device share that array: calls whose work
+ * overlaps on the GPU race and give wrong results. The first call on each
+ * device sets up the array's address (with that device current); make it
+ * before starting any stream capture. */
+#define FE_NOALLOC_MAX_SITES 33554432LL
+int fe_mass_weight_noalloc(const double* d_h, int64_t n, double* d_out, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* Time nsteps of fe_run with CUDA events on the engine's stream; ms_total is
  * the device time, ms_collide the summed device time of the fused collision
