@@ -65,11 +65,15 @@ def dist_env():
 
 
 def workload(size: int, seed: int = 2024):
+    """The production dispersion configuration: fluid physics of the
+    reference's cfg/3d_image/params.cfg (rho0 = rho1 = 1, tau = 0.9, W = 5,
+    sigma = 0.0083, mobility_coeff 0.02) with a 45 degree contact angle
+    (phi = 6 sigma cos 45) and body force 1e-6 along x."""
     from felbm_gpu_b200 import default_params, geometry
     shape = (size, size, size)
     solid, por = geometry.grf(shape, 6.0, 0.37, seed, flow_axis=0)
-    sigma, W = 1e-3, 4.0
-    p = default_params(rho0=1.0, rho1=1.0, tau0=1.0, tau1=1.0, surface_tension=sigma, interface_width=W,
+    sigma, W = 0.0083, 5.0
+    p = default_params(rho0=1.0, rho1=1.0, tau0=0.9, tau1=0.9, surface_tension=sigma, interface_width=W,
                        mobility_coeff=0.02, phi=6 * sigma * np.cos(np.radians(45.0)), gx=1e-6,
                        use_mrt=1, use_halfway_bb=1, correct_op_mass=1,
                        stream_matrix_free=1, grad_matrix_free=1, fused=1, fuse_collision=1,

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/felbm_b200.h"
+#include "collide.cuh"
 #include "fe_internal.hpp"
 #include "kernels.cuh"
 
@@ -38,6 +39,21 @@ void fe_clear_error() { g_last_error.clear(); }
                                       __FILE__ + ":" + std::to_string(__LINE__) + ")");            \
   } while (0)
 
+// Run CALL with S (storage traits) and Sh (brick shape) bound to the engine's.
+// Inside CALL, write template argument commas as FE_COMMA.
+#define FE_COMMA ,
+#define FE_DISPATCH(E, CALL)                                                   \
+  switch ((E).storage * 2 + (E).shape2d) {                                     \
+    case 0: { using S = StF64; using Sh = Shape3D; CALL; } break;              \
+    case 1: { using S = StF64; using Sh = Shape2D; CALL; } break;              \
+    case 2: { using S = StF32; using Sh = Shape3D; CALL; } break;              \
+    case 3: { using S = StF32; using Sh = Shape2D; CALL; } break;              \
+    case 4: { using S = StF16S; using Sh = Shape3D; CALL; } break;             \
+    case 5: { using S = StF16S; using Sh = Shape2D; CALL; } break;             \
+    case 6: { using S = StBF16S; using Sh = Shape3D; CALL; } break;            \
+    default: { using S = StBF16S; using Sh = Shape2D; CALL; } break;           \
+  }
+
 static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   auto spread = [](uint64_t v) {
     v &= 0x1fffff;
@@ -51,37 +67,26 @@ static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   return spread(x) | (spread(y) << 1) | (spread(z) << 2);
 }
 
-static int ilog2(int v) {
-  int l = 0;
-  while ((1 << l) < v) ++l;
-  return l;
-}
-
 // Host copy of one lattice's brick layout.
 struct HostLayout {
   int nx, ny, nz, lb[3], nb[3], words;
+  bool shape2d;
   int64_t n;
-  std::vector<int32_t> brick_grid, base, brick_xyz, ref_of, site_of_ref;
+  std::vector<int32_t> brick_grid, base, brick_xyz, ref_of, site_of_ref, node_of;
   std::vector<uint64_t> mask;
+  std::vector<BrickRec> rec;
   int nbricks() const { return (int)brick_xyz.size() / 3; }
 };
 
-// Brick shape: 8x8x8 for 3-D lattices, 16x16x1 for quasi-2-D ones (nz == 1),
-// each axis clamped to the next power of two of its extent.
-static void brick_shape(int nx, int ny, int nz, int lb[3]) {
-  const int N[3] = {nx, ny, nz};
-  int B[3] = {8, 8, 8};
-  if (nz == 1) { B[0] = 16; B[1] = 16; B[2] = 1; }
-  for (int a = 0; a < 3; ++a) {
-    if (N[a] == 1) B[a] = 1;
-    else B[a] = std::min(B[a], 1 << ilog2(N[a]));
-    lb[a] = ilog2(B[a]);
-  }
-}
-
-static void build_layout(const uint8_t* solid, int nx, int ny, int nz, const int lb_in[3], HostLayout& L) {
+// Brick shape: 8x8x8 (Shape3D) for 3-D lattices, 16x16x1 (Shape2D) for
+// quasi-2-D ones (nz == 1). Axes shorter than the brick simply leave slots
+// empty; tile positions wrap periodically, so any extent works.
+static int build_layout(const uint8_t* solid, int nx, int ny, int nz, HostLayout& L) {
   L.nx = nx; L.ny = ny; L.nz = nz;
-  for (int a = 0; a < 3; ++a) L.lb[a] = lb_in[a];
+  L.shape2d = nz == 1;
+  L.lb[0] = L.shape2d ? 4 : 3;
+  L.lb[1] = L.shape2d ? 4 : 3;
+  L.lb[2] = L.shape2d ? 0 : 3;
   const int B[3] = {1 << L.lb[0], 1 << L.lb[1], 1 << L.lb[2]};
   const int N[3] = {nx, ny, nz};
   for (int a = 0; a < 3; ++a) L.nb[a] = (N[a] + B[a] - 1) / B[a];
@@ -94,7 +99,6 @@ static void build_layout(const uint8_t* solid, int nx, int ny, int nz, const int
   for (int64_t node = 0; node < total; ++node)
     if (!solid[node]) ref_of_node[node] = (int32_t)nref++;
   L.n = nref;
-  // active bricks in Morton order
   struct Bk { uint64_t key; int bx, by, bz; };
   std::vector<Bk> bricks;
   const int64_t nbt = (int64_t)L.nb[0] * L.nb[1] * L.nb[2];
@@ -117,37 +121,64 @@ static void build_layout(const uint8_t* solid, int nx, int ny, int nz, const int
   L.base.assign((size_t)nbk * L.words, 0);
   L.ref_of.assign(L.n, 0);
   L.site_of_ref.assign(L.n, 0);
+  L.node_of.assign(L.n, 0);
   int64_t site = 0;
   for (int b = 0; b < nbk; ++b) {
     const Bk& k = bricks[b];
     L.brick_grid[k.bx + (int64_t)L.nb[0] * (k.by + (int64_t)L.nb[1] * k.bz)] = b;
     L.brick_xyz[b * 3 + 0] = k.bx; L.brick_xyz[b * 3 + 1] = k.by; L.brick_xyz[b * 3 + 2] = k.bz;
-    for (int w = 0; w < L.words; ++w) L.base[(size_t)b * L.words + w] = (int32_t)site + 0;  // fixed below
-    int64_t s0 = site;
     for (int s = 0; s < C; ++s) {
       const int w = s >> 6;
-      if ((s & 63) == 0) L.base[(size_t)b * L.words + w] = (int32_t)s0;
+      if ((s & 63) == 0) L.base[(size_t)b * L.words + w] = (int32_t)site;
       const int lx = s & (B[0] - 1), ly = (s >> L.lb[0]) & (B[1] - 1), lz = s >> (L.lb[0] + L.lb[1]);
       const int x = k.bx * B[0] + lx, y = k.by * B[1] + ly, z = k.bz * B[2] + lz;
       if (x >= nx || y >= ny || z >= nz) continue;
       const int64_t node = x + (int64_t)nx * (y + (int64_t)ny * z);
       if (solid[node]) continue;
       L.mask[(size_t)b * L.words + w] |= 1ull << (s & 63);
-      L.ref_of[s0] = ref_of_node[node];
-      L.site_of_ref[ref_of_node[node]] = (int32_t)s0;
-      ++s0;
+      L.ref_of[site] = ref_of_node[node];
+      L.site_of_ref[ref_of_node[node]] = (int32_t)site;
+      L.node_of[site] = (int32_t)node;
+      ++site;
     }
-    site = s0;
   }
-}
-
-// Dynamic shared memory of a pass with halo H and real size rs; nfield tiles.
-static size_t tile_bytes(const HostLayout& L, int H, int rs, int nfield) {
-  const int N[3] = {L.nx, L.ny, L.nz};
-  int64_t t = 1;
-  for (int a = 0; a < 3; ++a) t *= (1 << L.lb[a]) + (N[a] > 1 ? 2 * H : 0);
-  auto al = [](int64_t b) { return (b + 15) & ~int64_t(15); };
-  return (size_t)(al(t * 4) + nfield * al(t * rs));
+  // per-brick records: per-axis tile tables over coordinates [-HMAX, B+HMAX)
+  // (wrapped periodically) and the ids of the neighbour bricks they touch
+  L.rec.assign(nbk, BrickRec{});
+  for (int b = 0; b < nbk; ++b) {
+    BrickRec& R = L.rec[b];
+    std::memset(&R, 0, sizeof(R));
+    int ucoord[3][4], nseg[3];
+    for (int a = 0; a < 3; ++a) {
+      const bool halo = !(L.shape2d && a == 2);
+      const int T = halo ? B[a] + 2 * HMAX : 1;
+      const int origin = L.brick_xyz[b * 3 + a] * B[a] - (halo ? HMAX : 0);
+      nseg[a] = 0;
+      for (int t = 0; t < T; ++t) {
+        const int X = ((origin + t) % N[a] + N[a]) % N[a];
+        const int bc = X >> L.lb[a];
+        int s = 0;
+        while (s < nseg[a] && ucoord[a][s] != bc) ++s;
+        if (s == nseg[a]) {
+          if (nseg[a] == 4) return fe_fail(FE_ERR_ARG, "brick tile touches more than 4 bricks along an axis");
+          ucoord[a][nseg[a]++] = bc;
+        }
+        R.seg[a][t] = (uint8_t)s;
+        R.loc[a][t] = (uint8_t)(X & (B[a] - 1));
+      }
+    }
+    for (int q = 0; q < 64; ++q) R.nbr[q] = -1;
+    for (int sz = 0; sz < nseg[2]; ++sz)
+      for (int sy = 0; sy < nseg[1]; ++sy)
+        for (int sx = 0; sx < nseg[0]; ++sx)
+          R.nbr[sx + 4 * (sy + 4 * sz)] =
+              L.brick_grid[ucoord[0][sx] + (int64_t)L.nb[0] * (ucoord[1][sy] + (int64_t)L.nb[1] * ucoord[2][sz])];
+    R.first = L.base[(size_t)b * L.words];
+    int c = 0;
+    for (int w = 0; w < L.words; ++w) c += __builtin_popcountll(L.mask[(size_t)b * L.words + w]);
+    R.cnt = c;
+  }
+  return FE_OK;
 }
 
 enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
@@ -155,6 +186,7 @@ enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
 struct Engine {
   fe_params P{};
   int storage = FE_F64;
+  int shape2d = 0;
   int device = 0;
   HostLayout L;
   LatDesc hd{};               // host copy of the descriptor
@@ -163,14 +195,15 @@ struct Engine {
   Ctl* d_ctl = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
-  double* d_tmp = nullptr;    // 2*Vn doubles for state/field transfer
+  double* d_tmp = nullptr;    // state/field transfer buffer
   int64_t tmp_len = 0;
   double* d_partm = nullptr;
   int parity = 0;             // buffer holding the current state
   int64_t t_host = 0;
   int64_t launches = 0;
-  size_t smem_p1 = 0, smem_p2 = 0, smem_p4 = 0;
+  size_t smem_p4 = 0;
   bool open_bnd = false;
+  double ff_manual = 1.0;
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
   cudaGraphExec_t graph2[2] = {nullptr, nullptr};
   cudaEvent_t ev_stats = nullptr;
@@ -180,11 +213,7 @@ struct Engine {
 
   ~Engine() { release(); }
   void release() {
-    for (int p = 0; p < 2; ++p) {
-      if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
-      if (graph2[p]) cudaGraphExecDestroy(graph2[p]);
-      graph1[p] = graph2[p] = nullptr;
-    }
+    drop_graphs();
     for (void* a : allocs) cudaFree(a);
     allocs.clear();
     if (d_tmp) cudaFree(d_tmp);
@@ -210,10 +239,15 @@ struct Engine {
     *p = static_cast<T*>(q);
     return FE_OK;
   }
-
-  size_t pop_size() const {
-    return storage == FE_F64 ? 8 : (storage == FE_F32 ? 4 : 2);
+  template <class T>
+  int upload_vec(T** p, const std::vector<T>& v) {
+    int rc = alloc(p, v.size());
+    if (rc) return rc;
+    if (!v.empty()) FE_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return FE_OK;
   }
+
+  size_t pop_size() const { return storage == FE_F64 ? 8 : (storage == FE_F32 ? 4 : 2); }
   size_t fld_size() const { return storage == FE_F64 ? 8 : 4; }
 
   void fill_prm() {
@@ -253,11 +287,11 @@ struct Engine {
     if (dev >= 0) FE_CUDA(cudaSetDevice(dev));
     FE_CUDA(cudaGetDevice(&device));
     FE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    int lb[3];
-    brick_shape(nx, ny, nz, lb);
-    build_layout(solid, nx, ny, nz, lb, L);
+    int rc = build_layout(solid, nx, ny, nz, L);
+    if (rc) return rc;
     if (L.n == 0) return fe_fail(FE_ERR_ARG, "geometry has no fluid site");
     if (L.n >= (int64_t)1 << 31) return fe_fail(FE_ERR_ARG, "more than 2^31 sites");
+    shape2d = L.shape2d ? 1 : 0;
     const int nbk = L.nbricks();
     LatDesc& D = hd;
     D.nx = nx; D.ny = ny; D.nz = nz;
@@ -267,20 +301,16 @@ struct Engine {
     D.nbricks = nbk;
     D.n = L.n;
     D.n_pad = (L.n + AOSOA - 1) / AOSOA * AOSOA;
-    int rc;
     int32_t *bg, *bs, *bx, *rf;
     uint64_t* mk;
-    if ((rc = alloc(&bg, L.brick_grid.size()))) return rc;
-    if ((rc = alloc(&mk, L.mask.size()))) return rc;
-    if ((rc = alloc(&bs, L.base.size()))) return rc;
-    if ((rc = alloc(&bx, L.brick_xyz.size()))) return rc;
-    if ((rc = alloc(&rf, L.ref_of.size()))) return rc;
-    FE_CUDA(cudaMemcpy(bg, L.brick_grid.data(), L.brick_grid.size() * 4, cudaMemcpyHostToDevice));
-    FE_CUDA(cudaMemcpy(mk, L.mask.data(), L.mask.size() * 8, cudaMemcpyHostToDevice));
-    FE_CUDA(cudaMemcpy(bs, L.base.data(), L.base.size() * 4, cudaMemcpyHostToDevice));
-    FE_CUDA(cudaMemcpy(bx, L.brick_xyz.data(), L.brick_xyz.size() * 4, cudaMemcpyHostToDevice));
-    FE_CUDA(cudaMemcpy(rf, L.ref_of.data(), L.ref_of.size() * 4, cudaMemcpyHostToDevice));
-    D.brick_grid = bg; D.mask = mk; D.base = bs; D.brick_xyz = bx; D.ref_of = rf;
+    BrickRec* rec;
+    if ((rc = upload_vec(&bg, L.brick_grid))) return rc;
+    if ((rc = upload_vec(&mk, L.mask))) return rc;
+    if ((rc = upload_vec(&bs, L.base))) return rc;
+    if ((rc = upload_vec(&bx, L.brick_xyz))) return rc;
+    if ((rc = upload_vec(&rf, L.ref_of))) return rc;
+    if ((rc = upload_vec(&rec, L.rec))) return rc;
+    D.brick_grid = bg; D.mask = mk; D.base = bs; D.brick_xyz = bx; D.ref_of = rf; D.rec = rec;
     const size_t popn = (size_t)Q * D.n_pad;
     for (int b = 0; b < 2; ++b)
       for (int f = 0; f < 2; ++f) {
@@ -297,8 +327,8 @@ struct Engine {
       *f = q;
     }
     if ((rc = alloc(&D.part1, (size_t)nbk * 2))) return rc;
-    if ((rc = alloc(&D.part4, (size_t)nbk * 6))) return rc;
-    FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * 6 * 8));
+    if ((rc = alloc(&D.part4, (size_t)nbk * WARPS * 6))) return rc;
+    FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * WARPS * 6 * 8));
     if ((rc = alloc(&d_partm, (size_t)nbk * 2))) return rc;
     if ((rc = alloc(&d_ctl, 1))) return rc;
     Ctl c0{};
@@ -309,83 +339,68 @@ struct Engine {
     if ((rc = alloc(&d_desc, 1))) return rc;
     std::vector<int2> work(nbk);
     for (int b = 0; b < nbk; ++b) work[b] = make_int2(0, b);
-    if ((rc = alloc(&d_work, work.size()))) return rc;
-    FE_CUDA(cudaMemcpy(d_work, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    const int rs = (int)fld_size();
-    smem_p1 = tile_bytes(L, 1, rs, 0);
-    smem_p2 = tile_bytes(L, 1, rs, 1);
-    smem_p4 = tile_bytes(L, 2, rs, 3);
-    if ((rc = set_smem_attrs())) return rc;
+    if ((rc = upload_vec(&d_work, work))) return rc;
+    FE_DISPATCH(*this, rc = set_attrs<S FE_COMMA Sh>());
+    if (rc) return rc;
     FE_CUDA(cudaMallocHost(&h_stats, 6 * sizeof(double)));
     FE_CUDA(cudaEventCreateWithFlags(&ev_stats, cudaEventDisableTiming));
     return upload_desc();
   }
 
-  // Opt every pass kernel in to the dynamic shared memory it needs (the
-  // default limit is 48 KB minus the kernel's static TileShared block).
-  template <class S>
-  int set_smem_attrs_t() {
-    const int a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 0>, (cudaFuncAttribute)a, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, 1>, (cudaFuncAttribute)a, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_cfield<S, 0>, (cudaFuncAttribute)a, (int)smem_p2));
-    FE_CUDA(cudaFuncSetAttribute(k_cfield<S, 1>, (cudaFuncAttribute)a, (int)smem_p2));
-    FE_CUDA(cudaFuncSetAttribute(k_lapmu<S>, (cudaFuncAttribute)a, (int)smem_p2));
-    FE_CUDA(cudaFuncSetAttribute(k_moments<S>, (cudaFuncAttribute)a, (int)smem_p1));
-    FE_CUDA(cudaFuncSetAttribute(k_mass<S>, (cudaFuncAttribute)a, (int)smem_p1));
-    FE_CUDA(cudaFuncSetAttribute(k_download_state<S>, (cudaFuncAttribute)a, (int)smem_p1));
-    FE_CUDA(cudaFuncSetAttribute(k_upload_state<S>, (cudaFuncAttribute)a, (int)smem_p1));
+  // Dynamic shared memory of the collide pass (CollideSmem).
+  template <class S, class Sh>
+  int set_attrs() {
+    smem_p4 = CollideSmem<Sh, typename S::real>::BYTES;
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 0>, a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 1>, a, (int)smem_p4));
     return FE_OK;
   }
-  int set_smem_attrs() {
-    switch (storage) {
-      case FE_F64: return set_smem_attrs_t<StF64>();
-      case FE_F32: return set_smem_attrs_t<StF32>();
-      case FE_F16S: return set_smem_attrs_t<StF16S>();
-      default: return set_smem_attrs_t<StBF16S>();
-    }
-  }
+
+  // The momentum fields are read by P2 only for the drho pressure correction,
+  // and by the open-boundary kernels.
+  bool need_j() const { return hd.prm.drho != 0.0 || open_bnd; }
 
   // ---- one step (plain launches) -----------------------------------------
   template <class S>
+  void launch_bc(cudaStream_t st) {
+    const int nio = hd.n_inlet + hd.n_outlet, nb = hd.n_buf, nall = nio + nb;
+    if (nio) { k_bc_fields<S><<<(nio + 127) / 128, 128, 0, st>>>(d_desc, 0); ++launches; }
+    if (nb) { k_bc_buffers<S><<<(nb + 127) / 128, 128, 0, st>>>(d_desc, 0); ++launches; }
+    if (nall) { k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, 0); ++launches; }
+  }
+  template <class S, class Sh>
   void launch_step_t(int par, cudaStream_t st, cudaEvent_t* ev) {
     const int nb = hd.nbricks;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
     rec(0);
-    k_moments<S><<<nb, CTA, smem_p1, st>>>(d_desc, d_work, par);
+    k_moments<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work, par, need_j() ? 1 : 0);
     rec(1);
-    if (open_bnd) {
-      const int nio = hd.n_inlet + hd.n_outlet;
-      if (nio) k_bc_fields<S><<<(nio + 255) / 256, 256, 0, st>>>(d_desc, 0);
-      if (hd.prm.copy_to_buf && hd.n_buf) k_bc_buffers<S><<<(hd.n_buf + 255) / 256, 256, 0, st>>>(d_desc, 0);
-      launches += (nio ? 1 : 0) + ((hd.prm.copy_to_buf && hd.n_buf) ? 1 : 0);
-    }
+    if (open_bnd) launch_bc<S>(st);
     rec(2);
-    k_cfield<S, 0><<<nb, CTA, smem_p2, st>>>(d_desc, d_work, FieldOut{});
+    k_cfield<S, Sh, 0><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
     rec(3);
-    k_lapmu<S><<<nb, CTA, smem_p2, st>>>(d_desc, d_work);
+    k_lapmu<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work);
     rec(4);
-    if (hd.prm.use_mrt) k_collide<S, 1><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
-    else k_collide<S, 0><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
+    if (hd.prm.use_mrt) k_collide<S, Sh, 1><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
+    else k_collide<S, Sh, 0><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
     rec(5);
     launches += 4;
   }
   void launch_step(int par, cudaStream_t st, cudaEvent_t* ev = nullptr) {
-    switch (storage) {
-      case FE_F64: launch_step_t<StF64>(par, st, ev); break;
-      case FE_F32: launch_step_t<StF32>(par, st, ev); break;
-      case FE_F16S: launch_step_t<StF16S>(par, st, ev); break;
-      default: launch_step_t<StBF16S>(par, st, ev); break;
-    }
+    FE_DISPATCH(*this, launch_step_t<S FE_COMMA Sh>(par, st, ev));
   }
   int kernels_per_step() const {
     int k = 4;
-    if (open_bnd) k += (hd.n_inlet + hd.n_outlet ? 1 : 0) + ((hd.prm.copy_to_buf && hd.n_buf) ? 1 : 0);
+    if (open_bnd) {
+      const int nio = hd.n_inlet + hd.n_outlet;
+      k += (nio ? 1 : 0) + (hd.n_buf ? 1 : 0) + (nio + hd.n_buf ? 1 : 0);
+    }
     return k;
   }
 
   int set_ctl_mode(int run_mode, double ff) {
-    // ff_auto / auto_correct / ff_manual are contiguous in Ctl
+    // auto_correct, ff_auto, ff_manual are contiguous in Ctl
     struct { int32_t auto_correct, ff_auto; double ff_manual; } m{run_mode ? 1 : 0, run_mode ? 1 : 0, ff};
     static_assert(offsetof(Ctl, ff_auto) == offsetof(Ctl, auto_correct) + 4, "Ctl layout");
     static_assert(offsetof(Ctl, ff_manual) == offsetof(Ctl, auto_correct) + 8, "Ctl layout");
@@ -394,8 +409,6 @@ struct Engine {
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
   }
-
-  double ff_manual = 1.0;
 
   int step(int nsteps) {
     int rc;
@@ -473,20 +486,11 @@ struct Engine {
     return FE_OK;
   }
 
-  template <class S>
-  int mass_t() {
-    k_mass<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity, d_partm);
+  int mass_pass() {
+    FE_DISPATCH(*this, (k_mass<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, d_partm)));
     ++launches;
     FE_CUDA(cudaGetLastError());
     return FE_OK;
-  }
-  int mass_pass() {
-    switch (storage) {
-      case FE_F64: return mass_t<StF64>();
-      case FE_F32: return mass_t<StF32>();
-      case FE_F16S: return mass_t<StF16S>();
-      default: return mass_t<StBF16S>();
-    }
   }
 
   int read_ctl(Ctl* c) {
@@ -500,8 +504,7 @@ struct Engine {
     return FE_OK;
   }
 
-  template <class S>
-  int download_t(double* h, double* g) {
+  int download(double* h, double* g) {
     const int64_t Vn = (int64_t)Q * hd.n;
     int rc;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
@@ -509,10 +512,11 @@ struct Engine {
     if ((rc = read_ctl(&c))) return rc;
     int apply = 0;
     if (c.pending && hd.prm.correct_mass) {
-      if ((rc = mass_t<S>())) return rc;
+      if ((rc = mass_pass())) return rc;
       apply = 1;
     }
-    k_download_state<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity, d_tmp, d_tmp + Vn, apply);
+    FE_DISPATCH(*this, (k_download_state<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, d_tmp,
+                                                                                  d_tmp + Vn, apply)));
     ++launches;
     FE_CUDA(cudaGetLastError());
     FE_CUDA(cudaMemcpyAsync(h, d_tmp, Vn * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -520,23 +524,15 @@ struct Engine {
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
   }
-  int download(double* h, double* g) {
-    switch (storage) {
-      case FE_F64: return download_t<StF64>(h, g);
-      case FE_F32: return download_t<StF32>(h, g);
-      case FE_F16S: return download_t<StF16S>(h, g);
-      default: return download_t<StBF16S>(h, g);
-    }
-  }
 
-  template <class S>
-  int upload_t(const double* h, const double* g) {
+  int upload(const double* h, const double* g) {
     const int64_t Vn = (int64_t)Q * hd.n;
     int rc;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
     FE_CUDA(cudaMemcpyAsync(d_tmp, h, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
     FE_CUDA(cudaMemcpyAsync(d_tmp + Vn, g, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
-    k_upload_state<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity, d_tmp, d_tmp + Vn);
+    FE_DISPATCH(*this, (k_upload_state<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, d_tmp,
+                                                                                d_tmp + Vn)));
     ++launches;
     FE_CUDA(cudaGetLastError());
     int32_t zero = 0;
@@ -544,55 +540,36 @@ struct Engine {
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
   }
-  int upload(const double* h, const double* g) {
-    switch (storage) {
-      case FE_F64: return upload_t<StF64>(h, g);
-      case FE_F32: return upload_t<StF32>(h, g);
-      case FE_F16S: return upload_t<StF16S>(h, g);
-      default: return upload_t<StBF16S>(h, g);
-    }
-  }
 
   // download()/download_raw(): P1 (+BC) and P2 in output mode, no step.
-  template <class S>
-  int fields_t(const fe_fields* f) {
+  template <class S, class Sh>
+  void fields_launch(FieldOut o) {
+    k_moments<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, 1);
+    if (open_bnd) launch_bc<S>(stream);
+    k_cfield<S, Sh, 1><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
+    launches += 2;
+  }
+  int fields(const fe_fields* f) {
     const int64_t n = hd.n;
     int rc;
     if ((rc = ensure_tmp(7 * n))) return rc;
-    Ctl c;
-    if ((rc = read_ctl(&c))) return rc;
+    // the moment pass forms the lambda of a queued correction (the pending flag
+    // stays set: no collision runs, so the correction is still owed)
     if ((rc = set_ctl_mode(0, ff_manual))) return rc;
-    // P1 with the queued correction (pending stays set: no collision runs)
-    k_moments<S><<<hd.nbricks, CTA, smem_p1, stream>>>(d_desc, d_work, parity);
-    if (open_bnd) {
-      const int nio = hd.n_inlet + hd.n_outlet;
-      if (nio) k_bc_fields<S><<<(nio + 255) / 256, 256, 0, stream>>>(d_desc, 0);
-      if (hd.prm.copy_to_buf && hd.n_buf) k_bc_buffers<S><<<(hd.n_buf + 255) / 256, 256, 0, stream>>>(d_desc, 0);
-    }
-    FieldOut o{d_tmp + 0 * n, d_tmp + 1 * n, d_tmp + 2 * n, d_tmp + 3 * n, d_tmp + 4 * n, d_tmp + 5 * n, d_tmp + 6 * n};
-    k_cfield<S, 1><<<hd.nbricks, CTA, smem_p2, stream>>>(d_desc, d_work, o);
-    launches += 2;
+    FieldOut o{d_tmp + 0 * n, d_tmp + 1 * n, d_tmp + 2 * n, d_tmp + 3 * n, d_tmp + 4 * n, d_tmp + 5 * n,
+               d_tmp + 6 * n};
+    FE_DISPATCH(*this, fields_launch<S FE_COMMA Sh>(o));
     FE_CUDA(cudaGetLastError());
     double* dst[7] = {f->rho, f->c, f->ux, f->uy, f->uz, f->p, f->mu};
     for (int q = 0; q < 7; ++q)
       if (dst[q]) FE_CUDA(cudaMemcpyAsync(dst[q], d_tmp + q * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     FE_CUDA(cudaStreamSynchronize(stream));
-    // the moment pass leaves lambda for the collision of a step; a download
-    // does not consume the queued correction
     double zero = 0.0;
     return write_ctl_field(offsetof(Ctl, lambda), &zero, 8);
   }
-  int fields(const fe_fields* f) {
-    switch (storage) {
-      case FE_F64: return fields_t<StF64>(f);
-      case FE_F32: return fields_t<StF32>(f);
-      case FE_F16S: return fields_t<StF16S>(f);
-      default: return fields_t<StBF16S>(f);
-    }
-  }
 
   int stats_launch() {
-    k_stats_finalize<<<1, CTA, 0, stream>>>(d_desc, 0);
+    FE_DISPATCH(*this, (k_stats_finalize<Sh><<<1, CTA, 0, stream>>>(d_desc, 0)));
     ++launches;
     FE_CUDA(cudaGetLastError());
     FE_CUDA(cudaMemcpyAsync(h_stats, reinterpret_cast<char*>(d_ctl) + offsetof(Ctl, stats), 6 * sizeof(double),
@@ -618,7 +595,7 @@ struct fe_engine {
   Engine e;
 };
 
-static const char* FE_VERSION = "felbm_b200 0.1 (sm_100a)";
+static const char* FE_VERSION = "felbm_b200 0.2 (sm_100a)";
 
 #define FE_GUARD(e) \
   if (!(e)) return fe_fail(FE_ERR_ARG, "null engine")
@@ -731,10 +708,20 @@ int fe_set_open_bnd(fe_engine* e, const fe_open_bnd* b) {
     for (int j = 0; j < cnt; ++j) v[j] = E.L.site_of_ref[a[j]];
     return v;
   };
+  const int nbuf = b->copy_to_buffers ? b->n_buf : 0;
   std::vector<int32_t> io = conv(b->inlet, b->n_inlet), out = conv(b->outlet, b->n_outlet);
   io.insert(io.end(), out.begin(), out.end());
-  std::vector<int32_t> bv = conv(b->buf_verts, b->n_buf), br = conv(b->buf_refs, b->n_buf);
-  // flags (multiphase_gpu.cuh:378-389 for BC_PROC)
+  std::vector<int32_t> bv = conv(b->buf_verts, nbuf), br = conv(b->buf_refs, nbuf);
+  // node coordinates of inlet, outlet and buffer sites (for k_bc_final)
+  std::vector<int32_t> xyz;
+  for (const std::vector<int32_t>* lst : {&io, &bv})
+    for (int32_t i : *lst) {
+      const int64_t node = E.L.node_of[i];
+      xyz.push_back((int32_t)(node % E.hd.nx));
+      xyz.push_back((int32_t)((node / E.hd.nx) % E.hd.ny));
+      xyz.push_back((int32_t)(node / ((int64_t)E.hd.nx * E.hd.ny)));
+    }
+  // flags (BC_PROC as the is_processed mask, multiphase_gpu.cuh:378-389)
   std::vector<uint8_t> flag(n, 0);
   std::vector<int32_t> src(n, 0);
   const bool in_proc = b->use_in_vel || b->use_in_prs || b->use_in_fluid;
@@ -749,40 +736,34 @@ int fe_set_open_bnd(fe_engine* e, const fe_open_bnd* b) {
     flag[i] |= fe::BC_SITE | (out_proc ? fe::BC_PROC : 0) | (b->copy_to_buffers ? 0 : fe::BC_G_OVER);
     src[i] = i;
   }
-  if (b->copy_to_buffers)
-    for (int j = 0; j < b->n_buf; ++j) {
-      flag[bv[j]] |= fe::BC_SITE | fe::BC_PROC | fe::BC_G_OVER;
-      src[bv[j]] = br[j];
-    }
+  for (int j = 0; j < nbuf; ++j) {
+    flag[bv[j]] |= fe::BC_SITE | fe::BC_PROC | fe::BC_G_OVER;
+    src[bv[j]] = br[j];
+  }
   int rc;
   uint8_t* dflag;
-  int32_t *dsrc, *dlist, *dbv = nullptr, *dbr = nullptr;
+  int32_t *dsrc, *dlist, *dxyz, *dbv = nullptr, *dbr = nullptr;
   double* dcoord = nullptr;
   unsigned char *craw, *ubc;
-  if ((rc = E.alloc(&dflag, n))) return rc;
-  if ((rc = E.alloc(&dsrc, n))) return rc;
-  if ((rc = E.alloc(&dlist, io.size()))) return rc;
+  if ((rc = E.upload_vec(&dflag, flag))) return rc;
+  if ((rc = E.upload_vec(&dsrc, src))) return rc;
+  if ((rc = E.upload_vec(&dlist, io))) return rc;
+  if ((rc = E.upload_vec(&dxyz, xyz))) return rc;
   if ((rc = E.alloc(&craw, n * E.fld_size()))) return rc;
   if ((rc = E.alloc(&ubc, 3 * n * E.fld_size()))) return rc;
-  FE_CUDA(cudaMemcpy(dflag, flag.data(), n, cudaMemcpyHostToDevice));
-  FE_CUDA(cudaMemcpy(dsrc, src.data(), n * 4, cudaMemcpyHostToDevice));
-  if (!io.empty()) FE_CUDA(cudaMemcpy(dlist, io.data(), io.size() * 4, cudaMemcpyHostToDevice));
   FE_CUDA(cudaMemset(craw, 0, n * E.fld_size()));
   FE_CUDA(cudaMemset(ubc, 0, 3 * n * E.fld_size()));
   if (b->inlet_coord && b->n_inlet) {
-    if ((rc = E.alloc(&dcoord, b->n_inlet))) return rc;
-    FE_CUDA(cudaMemcpy(dcoord, b->inlet_coord, b->n_inlet * 8, cudaMemcpyHostToDevice));
+    if ((rc = E.upload_vec(&dcoord, std::vector<double>(b->inlet_coord, b->inlet_coord + b->n_inlet)))) return rc;
   }
-  if (b->n_buf) {
-    if ((rc = E.alloc(&dbv, b->n_buf))) return rc;
-    if ((rc = E.alloc(&dbr, b->n_buf))) return rc;
-    FE_CUDA(cudaMemcpy(dbv, bv.data(), b->n_buf * 4, cudaMemcpyHostToDevice));
-    FE_CUDA(cudaMemcpy(dbr, br.data(), b->n_buf * 4, cudaMemcpyHostToDevice));
+  if (nbuf) {
+    if ((rc = E.upload_vec(&dbv, bv))) return rc;
+    if ((rc = E.upload_vec(&dbr, br))) return rc;
   }
   fe::LatDesc& D = E.hd;
-  D.bcflag = dflag; D.bcsrc = dsrc; D.bc_list = dlist; D.bc_coord = dcoord;
+  D.bcflag = dflag; D.bcsrc = dsrc; D.bc_list = dlist; D.bc_coord = dcoord; D.bc_xyz = dxyz;
   D.c_raw_bc = craw; D.u_bc = ubc;
-  D.n_inlet = b->n_inlet; D.n_outlet = b->n_outlet; D.n_buf = b->copy_to_buffers ? b->n_buf : 0;
+  D.n_inlet = b->n_inlet; D.n_outlet = b->n_outlet; D.n_buf = nbuf;
   D.buf_verts = dbv; D.buf_refs = dbr;
   fe::DevPrm& d = D.prm;
   d.open_bnd = 1; d.copy_to_buf = b->copy_to_buffers;
@@ -840,16 +821,14 @@ int fe_apply_mass_correction(fe_engine* e, double* drift) {
   }
   int32_t one = 1;
   int rc;
-  if (drift) {
-    // queue, then form M and lambda now so that the drift can be returned
-    if ((rc = E.write_ctl_field(offsetof(fe::Ctl, pending), &one, 4))) return rc;
-    if ((rc = E.mass_pass())) return rc;
-    fe::Ctl c;
-    if ((rc = E.read_ctl(&c))) return rc;
-    *drift = c.drift;
-    return FE_OK;
-  }
-  return E.write_ctl_field(offsetof(fe::Ctl, pending), &one, 4);
+  if ((rc = E.write_ctl_field(offsetof(fe::Ctl, pending), &one, 4))) return rc;
+  if (!drift) return FE_OK;
+  // form M and lambda now so that the drift can be returned
+  if ((rc = E.mass_pass())) return rc;
+  fe::Ctl c;
+  if ((rc = E.read_ctl(&c))) return rc;
+  *drift = c.drift;
+  return FE_OK;
 }
 
 int fe_record_target_mass(fe_engine* e) {
@@ -924,12 +903,12 @@ int fe_flow_stats_collect(fe_engine* e, double out[6]) {
 int fe_time_run(fe_engine* e, int nsteps, float* ms_total) {
   FE_GUARD(e);
   Engine& E = e->e;
+  int rc = E.set_ctl_mode(1, E.ff_manual);
+  if (!rc && !E.graph1[0]) rc = E.build_graphs();
+  if (rc) return rc;
   cudaEvent_t a, b;
   FE_CUDA(cudaEventCreate(&a));
   FE_CUDA(cudaEventCreate(&b));
-  int rc = E.set_ctl_mode(1, E.ff_manual);
-  if (!rc && !E.graph1[0]) rc = E.build_graphs();
-  if (rc) { cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
   FE_CUDA(cudaStreamSynchronize(E.stream));
   FE_CUDA(cudaEventRecord(a, E.stream));
   rc = E.run(nsteps);

@@ -10,20 +10,24 @@
 //   P3 k_lapmu    mu stencil -> Laplacian of mu
 //   P4 k_collide  c, p stencils to distance 2, lap(mu) to distance 1, pull g:
 //                 equilibria + Guo force + BGK/MRT relaxation, write h, g
-// Every CTA owns one brick: it stages the site indices of the brick plus a
-// halo into shared memory (from the per-brick occupancy words), stages the
-// stencil fields into shared memory tiles, and then runs one thread per fluid
-// site of the brick. All stencil case logic (central / one-sided / biased,
-// halfway bounce-back) is derived from tile occupancy, so no per-site tables
-// are read from HBM.
+// Every CTA owns one brick. Its prologue reads the brick's precomputed record
+// (neighbour-brick ids and per-axis tile tables, built on the host) and the
+// occupancy words of the neighbour bricks into shared memory; from those it
+// resolves the site index of every tile position (brick + halo) without
+// further global traffic, stages the stencil fields into shared-memory tiles
+// (solid positions hold NaN, so one load gives value and occupancy), then runs
+// one thread per fluid site of the brick. All stencil case logic (central /
+// one-sided / biased, halfway bounce-back, wetting) is derived from tile
+// occupancy with selects, so no per-site tables are read from HBM.
 //
 // Streaming is pull, fused into P1 and P4: the post-collision value f*_k at
 // x - e_k moves to site x, or f*_opp(k)(x) when x - e_k is solid (halfway
 // bounce-back). The state between steps is therefore post-collision; uploads
 // and downloads apply the (bijective) pull permutation.
 #pragma once
-#include <cuda_fp16.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <cstdint>
 
 #include "d3q19.hpp"
@@ -74,7 +78,6 @@ __device__ __forceinline__ int64_t pidx(int64_t i, int k) {
   return (i >> 5) * (int64_t)(Q * AOSOA) + k * AOSOA + (i & (AOSOA - 1));
 }
 
-// Shift parameters for the 16-bit formats (unused otherwise).
 struct Shift {
   float ref, inv_scale, scale;
 };
@@ -89,8 +92,8 @@ __device__ __forceinline__ typename S::real ld_pop(const typename S::pop* __rest
   }
 }
 template <class S>
-__device__ __forceinline__ void st_pop(typename S::pop* __restrict__ a, int64_t idx, int k,
-                                       typename S::real v, const Shift& sh) {
+__device__ __forceinline__ void st_pop(typename S::pop* __restrict__ a, int64_t idx, int k, typename S::real v,
+                                       const Shift& sh) {
   if constexpr (S::shifted) {
     a[idx] = from_f<typename S::pop>((v - weight<float>(k) * sh.ref) * sh.scale);
   } else {
@@ -98,123 +101,152 @@ __device__ __forceinline__ void st_pop(typename S::pop* __restrict__ a, int64_t 
   }
 }
 
+template <class R>
+__device__ __forceinline__ R nan_v() {
+  return __int_as_float(0x7fc00000);
+}
+template <>
+__device__ __forceinline__ double nan_v<double>() {
+  return __longlong_as_double(0x7ff8000000000000ll);
+}
+template <class R>
+__device__ __forceinline__ bool is_site(R v) {
+  return v == v;  // solid tile positions hold NaN
+}
+
 // ---------------------------------------------------------------------------
-// brick tile staging
+// brick shapes and tiles
 // ---------------------------------------------------------------------------
-constexpr int MAX_SEG = 4;      // distinct bricks a tile can touch per axis
-constexpr int MAX_T = 24;       // tile extent per axis
-constexpr int MAX_SLOTS = 512;  // nodes per brick
 constexpr int CTA = 256;
 
-struct TileShared {
-  uint8_t seg[3][MAX_T];        // tile coordinate -> neighbour-brick segment
-  uint8_t loc[3][MAX_T];        // tile coordinate -> local coordinate in that brick
-  int32_t ucoord[3][MAX_SEG];   // segment -> brick coordinate
-  int32_t nseg[3];
-  int32_t T[3];                 // tile extents
-  int32_t org[3];               // tile position of the brick's local (0,0,0)
-  int32_t nbr[MAX_SEG * MAX_SEG * MAX_SEG];
-  int32_t off1[Q], off2[Q];     // tile offsets of +e_k and +2 e_k
-  int32_t first, cnt, ntile;
-  uint16_t slot_of[MAX_SLOTS];
-  double red[CTA / 32][6];      // block reductions
-  float ff;                     // forcing factor of this step
-  double lambda;                // mass-correction lambda of this step
+template <int BX_, int BY_, int BZ_>
+struct BrickShape {
+  static constexpr int BX = BX_, BY = BY_, BZ = BZ_;
+  static constexpr int LBX = BX == 16 ? 4 : (BX == 8 ? 3 : (BX == 4 ? 2 : (BX == 2 ? 1 : 0)));
+  static constexpr int LBY = BY == 16 ? 4 : (BY == 8 ? 3 : (BY == 4 ? 2 : (BY == 2 ? 1 : 0)));
+  static constexpr int C = BX * BY * BZ;
+  static constexpr int W = (C + 63) / 64;
+  static constexpr int HZ = BZ > 1 ? 1 : 0;  // the z axis has a halo (3-D bricks)
+  static_assert((1 << LBX) == BX && (1 << LBY) == BY, "power-of-two brick");
+};
+using Shape3D = BrickShape<8, 8, 8>;
+using Shape2D = BrickShape<16, 16, 1>;
+
+template <class Sh, int H>
+struct Tile {
+  static constexpr int TX = Sh::BX + 2 * H, TY = Sh::BY + 2 * H, TZ = Sh::BZ + 2 * H * Sh::HZ;
+  static constexpr int N = TX * TY * TZ;
+  static constexpr int SY = TX, SZ = TX * TY;
+  // tile offset of +e_k and of the brick slot s
+  __device__ static constexpr int off(int k) { return lat_cx(k) + SY * lat_cy(k) + SZ * lat_cz(k) * Sh::HZ; }
+  __device__ static __forceinline__ int pos(int s) {
+    const int lx = s & (Sh::BX - 1), ly = (s >> Sh::LBX) & (Sh::BY - 1), lz = s >> (Sh::LBX + Sh::LBY);
+    return (lx + H) + SY * (ly + H) + SZ * (lz + H * Sh::HZ);
+  }
+};
+
+// Prologue state in shared memory (static part).
+template <class Sh>
+struct Pro {
+  BrickRec rec;
+  uint64_t nmask[64][Sh::W];
+  int32_t nbase[64][Sh::W];
+  uint16_t slot_of[Sh::C];
+  double red[CTA / 32][6];
+  double lambda;
+  float ff;
   int last;
 };
 
-__device__ __forceinline__ int mod_pos(int a, int n) {
-  int r = a % n;
-  return r < 0 ? r + n : r;
-}
-
-// Build the axis tables, neighbour-brick ids and the brick's slot list.
-// H = halo depth (1 or 2). Axes of extent 1 get no halo and no offsets.
-template <int H>
-__device__ void tile_setup(const LatDesc& D, int brick, TileShared& ts) {
+// Load the brick record and the neighbour bricks' occupancy into shared
+// memory, and list the brick's fluid slots in site order.
+template <class Sh>
+__device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s) {
   const int tid = threadIdx.x;
-  if (tid < 3) {
-    const int a = tid;
-    const int N = a == 0 ? D.nx : (a == 1 ? D.ny : D.nz);
-    const int lb = a == 0 ? D.lbx : (a == 1 ? D.lby : D.lbz);
-    const int B = 1 << lb;
-    const int h = N > 1 ? H : 0;
-    const int T = B + 2 * h;
-    const int origin = D.brick_xyz[brick * 3 + a] * B - h;
-    // A tile spans B + 2h <= 20 consecutive positions (mod N), which touch at
-    // most 4 distinct bricks per axis (two partial bricks across the wrap);
-    // the bound check below only guards against a layout the host never builds.
-    int nu = 0;
-    for (int t = 0; t < T && t < MAX_T; ++t) {
-      const int X = mod_pos(origin + t, N);
-      const int bc = X >> lb;
-      int s = 0;
-      while (s < nu && ts.ucoord[a][s] != bc) ++s;
-      if (s == nu) {
-        if (nu == MAX_SEG) { atomicOr(&D.ctl->status, 2); s = 0; }
-        else { ts.ucoord[a][nu] = bc; ++nu; }
-      }
-      ts.seg[a][t] = (uint8_t)s;
-      ts.loc[a][t] = (uint8_t)(X & (B - 1));
-    }
-    ts.nseg[a] = nu;
-    ts.T[a] = T;
-    ts.org[a] = h;
+  {
+    const int4* src = reinterpret_cast<const int4*>(D.rec + brick);
+    int4* dst = reinterpret_cast<int4*>(&s.rec);
+    constexpr int N4 = sizeof(BrickRec) / 16;
+    if (tid < N4) dst[tid] = __ldg(src + tid);
   }
   __syncthreads();
-  const int nsx = ts.nseg[0], nsy = ts.nseg[1], nsz = ts.nseg[2];
-  for (int q = tid; q < nsx * nsy * nsz; q += blockDim.x) {
-    const int sx = q % nsx, sy = (q / nsx) % nsy, sz = q / (nsx * nsy);
-    const int ux = ts.ucoord[0][sx], uy = ts.ucoord[1][sy], uz = ts.ucoord[2][sz];
-    ts.nbr[sx + MAX_SEG * (sy + MAX_SEG * sz)] = D.brick_grid[((int64_t)uz * D.nby + uy) * D.nbx + ux];
-  }
-  if (tid < Q) {
-    const int k = tid;
-    const int TX = ts.T[0], TY = ts.T[1];
-    const int ex = D.nx > 1 ? lat_cx(k) : 0, ey = D.ny > 1 ? lat_cy(k) : 0, ez = D.nz > 1 ? lat_cz(k) : 0;
-    ts.off1[k] = ex + TX * (ey + TY * ez);
-    ts.off2[k] = 2 * ts.off1[k];
-  }
-  // own slot list
-  const int W = D.words, C = W * 64;
-  const int first = D.base[(int64_t)brick * W];
-  for (int s = tid; s < C; s += blockDim.x) {
-    const int w = s >> 6, b = s & 63;
-    const uint64_t m = D.mask[(int64_t)brick * W + w];
-    if ((m >> b) & 1ull) {
-      const int r = D.base[(int64_t)brick * W + w] - first + __popcll(m & ((1ull << b) - 1ull));
-      ts.slot_of[r] = (uint16_t)s;
+  for (int q = tid; q < 64 * Sh::W; q += blockDim.x) {
+    const int slot = q / Sh::W, w = q - slot * Sh::W;
+    const int id = s.rec.nbr[slot];
+    if (id >= 0) {
+      s.nmask[slot][w] = __ldg(&D.mask[(int64_t)id * Sh::W + w]);
+      s.nbase[slot][w] = __ldg(&D.base[(int64_t)id * Sh::W + w]);
     }
   }
-  if (tid == 0) {
-    const uint64_t ml = D.mask[(int64_t)brick * W + W - 1];
-    ts.first = first;
-    ts.cnt = D.base[(int64_t)brick * W + W - 1] - first + __popcll(ml);
-    ts.ntile = ts.T[0] * ts.T[1] * ts.T[2];
-  }
   __syncthreads();
+  const int own = s.rec.seg[0][HMAX] + 4 * (s.rec.seg[1][HMAX] + 4 * s.rec.seg[2][Sh::HZ ? HMAX : 0]);
+  for (int q = tid; q < Sh::C; q += blockDim.x) {
+    const int w = q >> 6, b = q & 63;
+    const uint64_t m = s.nmask[own][w];
+    if ((m >> b) & 1ull) s.slot_of[s.nbase[own][w] - s.rec.first + __popcll(m & ((1ull << b) - 1ull))] = (uint16_t)q;
+  }
 }
 
-// Site index of every tile position (-1 = solid or outside any stored brick).
-__device__ __forceinline__ int tile_site(const LatDesc& D, const TileShared& ts, int t) {
-  const int TX = ts.T[0], TY = ts.T[1];
-  const int tx = t % TX, r = t / TX, ty = r % TY, tz = r / TY;
-  const int id = ts.nbr[ts.seg[0][tx] + MAX_SEG * (ts.seg[1][ty] + MAX_SEG * ts.seg[2][tz])];
-  if (id < 0) return -1;
-  const int slot = ts.loc[0][tx] | (ts.loc[1][ty] << D.lbx) | (ts.loc[2][tz] << (D.lbx + D.lby));
+// Site index of tile position t (halo H), -1 when solid.
+template <class Sh, int H>
+__device__ __forceinline__ int tile_site(const Pro<Sh>& s, int t) {
+  using T = Tile<Sh, H>;
+  const int tx = t % T::TX, r = t / T::TX, ty = r % T::TY, tz = r / T::TY;
+  const int ax = tx + (HMAX - H), ay = ty + (HMAX - H), az = Sh::HZ ? tz + (HMAX - H) : 0;
+  const int seg = s.rec.seg[0][ax] + 4 * (s.rec.seg[1][ay] + 4 * s.rec.seg[2][az]);
+  if (s.rec.nbr[seg] < 0) return -1;
+  const int slot = s.rec.loc[0][ax] | (s.rec.loc[1][ay] << Sh::LBX) | (s.rec.loc[2][az] << (Sh::LBX + Sh::LBY));
   const int w = slot >> 6, b = slot & 63;
-  const uint64_t m = __ldg(&D.mask[(int64_t)id * D.words + w]);
+  const uint64_t m = s.nmask[seg][w];
   if (!((m >> b) & 1ull)) return -1;
-  return __ldg(&D.base[(int64_t)id * D.words + w]) + __popcll(m & ((1ull << b) - 1ull));
+  return s.nbase[seg][w] + __popcll(m & ((1ull << b) - 1ull));
 }
 
-// tile position of the brick slot s
-__device__ __forceinline__ int slot_pos(const LatDesc& D, const TileShared& ts, int s) {
-  const int lx = s & ((1 << D.lbx) - 1);
-  const int ly = (s >> D.lbx) & ((1 << D.lby) - 1);
-  const int lz = s >> (D.lbx + D.lby);
-  return (lx + ts.org[0]) + ts.T[0] * ((ly + ts.org[1]) + ts.T[1] * (lz + ts.org[2]));
+// Site indices of a whole halo-H tile, built row by row: for each (y, z) row
+// and each neighbour brick it crosses, the row's occupancy bits and first site
+// index, then per position one popcount. Ends with a barrier.
+template <class Sh, int H>
+__device__ __forceinline__ void build_idx_tile(const Pro<Sh>& s, int32_t* __restrict__ s_idx,
+                                               uint32_t* __restrict__ s_rbits, int32_t* __restrict__ s_rbase) {
+  using T = Tile<Sh, H>;
+  constexpr int ROWS = T::TY * T::TZ;
+  for (int q = threadIdx.x; q < ROWS * 4; q += blockDim.x) {
+    const int row = q >> 2, sx = q & 3;
+    const int ty = row % T::TY, tz = row / T::TY;
+    const int ay = ty + (HMAX - H), az = Sh::HZ ? tz + (HMAX - H) : 0;
+    const int seg = sx + 4 * (s.rec.seg[1][ay] + 4 * s.rec.seg[2][az]);
+    uint32_t bits = 0;
+    int32_t base = 0;
+    if (s.rec.nbr[seg] >= 0) {
+      const int slot0 = (s.rec.loc[1][ay] << Sh::LBX) | (s.rec.loc[2][az] << (Sh::LBX + Sh::LBY));
+      const int w = slot0 >> 6, b0 = slot0 & 63;
+      const uint64_t m = s.nmask[seg][w];
+      bits = (uint32_t)((m >> b0) & ((1ull << Sh::BX) - 1ull));
+      base = s.nbase[seg][w] + __popcll(m & ((1ull << b0) - 1ull));
+    }
+    s_rbits[q] = bits;
+    s_rbase[q] = base;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < T::N; t += blockDim.x) {
+    const int row = t / T::TX, tx = t - row * T::TX;
+    const int ax = tx + (HMAX - H);
+    const int q = row * 4 + s.rec.seg[0][ax];
+    const uint32_t bits = s_rbits[q];
+    const int lx = s.rec.loc[0][ax];
+    s_idx[t] = ((bits >> lx) & 1u) ? s_rbase[q] + __popc(bits & ((1u << lx) - 1u)) : -1;
+  }
+  __syncthreads();
 }
+
+// Shared-memory arrays of a halo-H site-index tile.
+template <class Sh, int H>
+struct IdxTile {
+  using T = Tile<Sh, H>;
+  int32_t idx[T::N];
+  uint32_t rbits[T::TY * T::TZ * 4];
+  int32_t rbase[T::TY * T::TZ * 4];
+};
 
 // forcing_factor_at (reference felbm_gpu_main.cu:587-594)
 __device__ __forceinline__ double forcing_factor_dev(const DevPrm& P, const Ctl& C) {
@@ -228,39 +260,49 @@ __device__ __forceinline__ double forcing_factor_dev(const DevPrm& P, const Ctl&
   return 1.0;
 }
 
-// Block sum of NV doubles into ts.red[0][*] (thread 0 holds the result).
-template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], TileShared& ts, bool is_max_last = false) {
+template <class Sh>
+__device__ __forceinline__ void load_step_scalars(const LatDesc& D, Pro<Sh>& s) {
+  if (threadIdx.x == 0) {
+    const Ctl& C = *D.ctl;
+    s.ff = (float)forcing_factor_dev(D.prm, C);
+    s.lambda = C.lambda;
+  }
+}
+
+// Block reduction of NV doubles into thread 0 (the last one as a max when mx).
+template <int NV, class Sh>
+__device__ __forceinline__ void block_sum(double (&v)[NV], Pro<Sh>& s, bool mx_last = false) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double x = v[q];
-    const bool mx = is_max_last && q == NV - 1;
+    const bool mx = mx_last && q == NV - 1;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double y = __shfl_down_sync(0xffffffffu, x, o);
       x = mx ? fmax(x, y) : x + y;
     }
-    if (lane == 0) ts.red[wid][q] = x;
+    if (lane == 0) s.red[wid][q] = x;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     const int nw = blockDim.x >> 5;
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
-      double x = ts.red[0][q];
-      const bool mx = is_max_last && q == NV - 1;
-      for (int w = 1; w < nw; ++w) x = mx ? fmax(x, ts.red[w][q]) : x + ts.red[w][q];
+      double x = s.red[0][q];
+      const bool mx = mx_last && q == NV - 1;
+      for (int w = 1; w < nw; ++w) x = mx ? fmax(x, s.red[w][q]) : x + s.red[w][q];
       v[q] = x;
     }
   }
+  __syncthreads();
 }
 
-// Deterministic sum over `count` partial records of stride `stride` (one
-// CTA): each thread sums a fixed strided subset, then a fixed tree.
-template <int NV>
-__device__ void sum_partials(const double* __restrict__ part, int count, int stride, double (&out)[NV],
-                             TileShared& ts, bool is_max_last = false) {
+// Deterministic sum over `count` partial records (fixed strided subsets, then
+// a fixed tree), result in thread 0.
+template <int NV, class Sh>
+__device__ void sum_partials(const double* __restrict__ part, int count, int stride, double (&out)[NV], Pro<Sh>& s,
+                             bool mx_last = false) {
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
@@ -268,45 +310,57 @@ __device__ void sum_partials(const double* __restrict__ part, int count, int str
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       const double x = __ldcg(&part[(int64_t)r * stride + q]);
-      acc[q] = (is_max_last && q == NV - 1) ? fmax(acc[q], x) : acc[q] + x;
+      acc[q] = (mx_last && q == NV - 1) ? fmax(acc[q], x) : acc[q] + x;
     }
   }
-  block_sum<NV>(acc, ts, is_max_last);
+  block_sum<NV>(acc, s, mx_last);
 #pragma unroll
   for (int q = 0; q < NV; ++q) out[q] = acc[q];
 }
 
-// Returns true in every thread of the block that finished last (per lattice).
-__device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int total, TileShared& ts) {
+// True in every thread of the block that finished last (per lattice).
+template <class Sh>
+__device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int total, Pro<Sh>& s) {
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned int prev = atomicAdd(counter, 1u);
-    ts.last = (prev == total - 1) ? 1 : 0;
-  }
+  if (threadIdx.x == 0) s.last = (atomicAdd(counter, 1u) == total - 1) ? 1 : 0;
   __syncthreads();
-  return ts.last != 0;
+  return s.last != 0;
+}
+
+// lambda of the queued mass correction from the M, W sums (multiphase_gpu.cuh:689-700)
+__device__ __forceinline__ void finish_mass(Ctl* C, double M, double Wt) {
+  C->M = M;
+  C->W = Wt;
+  double lam = 0.0;
+  if (C->pending) {
+    const double drift = M - C->target_mass;
+    C->drift = drift;
+    if (Wt > 0.0 && drift != 0.0) lam = drift / Wt;
+  }
+  C->lambda = lam;
 }
 
 // ---------------------------------------------------------------------------
 // P1: pull streaming + moments (reference k_moments, device_engine.cuh:116-135,
-// with the streaming of the previous step's k_stream_gather, :882-889, fused
-// in as a pull, and k_mass_weight, :1109-1126, fused as block partials).
+// with the previous step's k_stream_gather, :882-889, fused in as a pull, and
+// k_mass_weight, :1109-1126, fused as block partials + last-block lambda).
 // ---------------------------------------------------------------------------
-template <class S>
+template <class S, class Sh>
 __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                  int parity) {
+                                                  int parity, int write_j) {
   using R = typename S::real;
   using P = typename S::pop;
   using F = typename S::fld;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  using T = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 1> it;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
-  tile_setup<1>(D, brick, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
+  prologue<Sh>(D, brick, s);
+  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  const int32_t* s_idx = it.idx;
   __syncthreads();
   const P* __restrict__ hin = static_cast<const P*>(D.pop[parity][0]);
   const P* __restrict__ gin = static_cast<const P*>(D.pop[parity][1]);
@@ -318,15 +372,15 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   double acc[2] = {0.0, 0.0};
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
+  const int first = s.rec.first, cnt = s.rec.cnt;
+  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+    const int64_t i = first + r;
+    const int pos = T::pos(s.slot_of[r]);
     R c = 0, p = 0, jx = 0, jy = 0, jz = 0;
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - ts.off1[k]];
+      const int up = s_idx[pos - T::off(k)];
       const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
       const int kk = up >= 0 ? k : lat_opp(k);
       const R hv = ld_pop<S>(hin, a, kk, shh);
@@ -340,41 +394,35 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
     }
     fc[i] = (F)c;
     fp[i] = (F)p;
-    fjx[i] = (F)jx;
-    fjy[i] = (F)jy;
-    fjz[i] = (F)jz;
+    if (write_j) {  // read only by P2's pressure correction (drho != 0), the
+      fjx[i] = (F)jx;  // open-boundary kernels and field downloads
+      fjy[i] = (F)jy;
+      fjz[i] = (F)jz;
+    }
     double phi = cd * (1.0 - cd);
     if (phi < 0.0) phi = 0.0;
     acc[0] += cd;
     acc[1] += phi;
   }
   if (!D.prm.correct_mass) return;
-  block_sum<2>(acc, ts);
+  block_sum<2>(acc, s);
   if (threadIdx.x == 0) {
     D.part1[(int64_t)brick * 2 + 0] = acc[0];
     D.part1[(int64_t)brick * 2 + 1] = acc[1];
   }
-  if (!last_block(&D.ctl->count1, (unsigned)D.nbricks, ts)) return;
+  if (!last_block(&D.ctl->count1, (unsigned)D.nbricks, s)) return;
   double tot[2];
-  sum_partials<2>(D.part1, D.nbricks, 2, tot, ts);
+  sum_partials<2>(D.part1, D.nbricks, 2, tot, s);
   if (threadIdx.x == 0) {
-    Ctl* C = D.ctl;
-    C->M = tot[0];
-    C->W = tot[1];
-    double lam = 0.0;
-    if (C->pending) {
-      const double drift = tot[0] - C->target_mass;
-      C->drift = drift;
-      if (tot[1] > 0.0 && drift != 0.0) lam = drift / tot[1];
-    }
-    C->lambda = lam;
-    C->count1 = 0;
+    finish_mass(D.ctl, tot[0], tot[1]);
+    D.ctl->count1 = 0;
   }
 }
 
-// corrected order parameter c' = c - lambda * max(c(1-c), 0) (the reference's
-// k_inject_mass, device_engine.cuh:1128-1139, applied to c instead of h; h is
-// never read by the collision, so this is the same state)
+// corrected order parameter c' = c - lambda * max(c(1-c), 0): the reference's
+// k_inject_mass (device_engine.cuh:1128-1139) applied to c instead of h; h is
+// never read by the collision (the h update is eq_h + force_h), so the next
+// step sees the same state.
 template <class R>
 __device__ __forceinline__ R corr_c(R c, double lambda) {
   if (lambda == 0.0) return c;
@@ -383,524 +431,197 @@ __device__ __forceinline__ R corr_c(R c, double lambda) {
   return phi > 0.0 ? (R)(cd - lambda * phi) : c;
 }
 
-template <class S>
-__device__ __forceinline__ void load_step_scalars(const LatDesc& D, TileShared& ts) {
-  if (threadIdx.x == 0) {
-    const Ctl& C = *D.ctl;
-    ts.ff = (float)forcing_factor_dev(D.prm, C);
-    ts.lambda = C.lambda;
-  }
-}
-
-// Stage c' (and the site indices) of the tile; returns nothing.
-template <class S>
-__device__ __forceinline__ void stage_field(const LatDesc& D, const TileShared& ts, const int32_t* s_idx,
-                                            typename S::real* s_v, const typename S::fld* __restrict__ f,
-                                            bool correct, double lambda) {
-  using R = typename S::real;
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) {
-    const int j = s_idx[t];
-    R v = R(0);
+// Stage a field over tile positions [t0, N) of halo H (NaN at solid positions);
+// optionally only the positions within distance `reach` of the brick.
+template <class Sh, int H, class R, class F>
+__device__ __forceinline__ void stage(const Pro<Sh>& s, const F* __restrict__ f, R* __restrict__ tile, bool correct,
+                                      double lambda, const int32_t* s_idx) {
+  using T = Tile<Sh, H>;
+  for (int t = threadIdx.x; t < T::N; t += blockDim.x) {
+    const int j = s_idx ? s_idx[t] : tile_site<Sh, H>(s, t);
+    R v = nan_v<R>();
     if (j >= 0) {
       v = (R)f[j];
       if (correct) v = corr_c<R>(v, lambda);
     }
-    s_v[t] = v;
+    tile[t] = v;
   }
+}
+
+// ---------------------------------------------------------------------------
+// near-wall stencil cases (table builders multiphase_gpu.cuh:93-193, helpers
+// device_engine.cuh:89-113,897-1010), from NaN-marked tile values
+// ---------------------------------------------------------------------------
+// central-difference value of direction k (cd_dir_val)
+template <class R>
+__device__ __forceinline__ R cd_val(R f0, R fm, R fp, bool hbb) {
+  const bool b1 = is_site(fm), f1 = is_site(fp);
+  if (hbb) return R(0.5) * ((f1 ? fp : f0) - (b1 ? fm : f0));
+  return (b1 && f1) ? R(0.5) * (fp - fm) : R(0);
+}
+// biased value of direction k (bd_dir_val): fp2 = f(x + 2e), fm2 = f(x - 2e)
+template <class R>
+__device__ __forceinline__ R bd_val(R f0, R fm, R fp, R fm2, R fp2, bool hbb) {
+  const bool b1 = is_site(fm), f1 = is_site(fp), f2 = is_site(fp2);
+  if (f1) {
+    if (f2) return R(-1.5) * f0 + R(2.0) * fp + R(-0.5) * fp2;
+    return hbb ? R(-1.5) * f0 + R(1.5) * fp : R(-2.0) * f0 + R(2.0) * fp;
+  }
+  if (hbb) return b1 ? R(0.5) * f0 + R(-0.5) * fm : R(0);
+  return (b1 && is_site(fm2)) ? R(-1.5) * f0 + R(2.0) * fm + R(-0.5) * fm2 : R(0);
+}
+// Laplacian term of direction k (k_lap_mf), boundary half `bnd`
+template <class R>
+__device__ __forceinline__ R lap_val(R f0, R fm, R fp, R bnd, bool hbb) {
+  const bool b1 = is_site(fm), f1 = is_site(fp);
+  if (b1 && f1) return fm - R(2) * f0 + fp;
+  if (!(b1 || f1)) return R(0);
+  const R f1v = b1 ? fm : fp;
+  return hbb ? (f1v - f0 - bnd) : (R(2) * f1v - R(2) * f0 - R(2) * bnd);
 }
 
 // ---------------------------------------------------------------------------
 // P2: grad_cd(c), Laplacian(c) with the wetting term, mu, velocity/pressure
 // correction (reference k_grad_cd_mf :897-913, k_pack_lap_c :159-165,
-// k_lap_mf :996-1010, k_mu_axpy :149-153, k_vel_press_corr :177-196; the
-// near-wall cases of the table builders multiphase_gpu.cuh:93-193).
+// k_lap_mf :996-1010, k_mu_axpy :149-153, k_vel_press_corr :177-196).
+// Open-boundary nodes were resolved by k_bc_final: their mu, p are final.
 // OUT != 0: also write c, rho, u, p, mu in the reference site order (download).
 // ---------------------------------------------------------------------------
 struct FieldOut {
   double *rho, *c, *ux, *uy, *uz, *p, *mu;
 };
 
-template <class S, int OUT>
+template <class S, class Sh, int OUT>
 __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                  FieldOut out) {
   using R = typename S::real;
   using F = typename S::fld;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  using T = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 1> it;
+  __shared__ R s_c[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  tile_setup<1>(D, wk.y, ts);
-  load_step_scalars<S>(D, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
-  __syncthreads();
-  R* s_c = reinterpret_cast<R*>(dsm + ((ts.ntile * 4 + 15) & ~15));
-  stage_field<S>(D, ts, s_idx, s_c, static_cast<const F*>(D.c), true, ts.lambda);
+  prologue<Sh>(D, wk.y, s);
+  load_step_scalars<Sh>(D, s);
+  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  stage<Sh, 1>(s, static_cast<const F*>(D.c), s_c, true, s.lambda, it.idx);
   __syncthreads();
   const DevPrm& Pm = D.prm;
   const R alpha = R(ALPHA), cs2 = R(CS2);
   const R rho1 = (R)Pm.rho1, drho = (R)Pm.drho, kappa = (R)Pm.kappa, four_beta = (R)Pm.four_beta;
-  const R bnd_coeff = (R)Pm.bnd_coeff, ff = (R)ts.ff;
+  const R bnd_coeff = (R)Pm.bnd_coeff, ff = (R)s.ff;
   const bool hbb = Pm.hbb != 0;
   const F* __restrict__ fjx = static_cast<const F*>(D.jx);
   const F* __restrict__ fjy = static_cast<const F*>(D.jy);
   const F* __restrict__ fjz = static_cast<const F*>(D.jz);
   F* __restrict__ fp = static_cast<F*>(D.p);
   F* __restrict__ fmu = static_cast<F*>(D.mu);
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
+  const int first = s.rec.first, cnt = s.rec.cnt;
+  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+    const int64_t i = first + r;
+    const int pos = T::pos(s.slot_of[r]);
     const R c0 = s_c[pos];
+    const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
+    if (flag & BC_SITE) {
+      if (OUT) {
+        const int64_t q = D.ref_of[i];
+        const F* ub = static_cast<const F*>(D.u_bc);
+        out.c[q] = (double)c0;
+        out.rho[q] = (double)(rho1 + drho * c0);
+        out.ux[q] = (double)ub[i]; out.uy[q] = (double)ub[D.n + i]; out.uz[q] = (double)ub[2 * D.n + i];
+        out.p[q] = (double)fp[i];
+        out.mu[q] = (double) static_cast<const F*>(D.mu)[i];
+      }
+      continue;  // fields resolved by the open-boundary kernels
+    }
     const R bnd = bnd_coeff * c0 * (R(1) - c0);
+    // opposite pairs: the central difference is antisymmetric and the
+    // Laplacian term symmetric, so each pair counts its leading direction twice
     R gx = 0, gy = 0, gz = 0, lap = 0;
 #pragma unroll
-    for (int k = 1; k < Q; ++k) {
-      const int o = ts.off1[k];
-      const bool b1 = s_idx[pos - o] >= 0, f1 = s_idx[pos + o] >= 0;
-      const R cm = s_c[pos - o], cp = s_c[pos + o];
-      R cdv = 0;
-      if (b1 && f1) cdv = R(0.5) * (cp - cm);
-      else if (hbb && b1) cdv = R(0.5) * (c0 - cm);
-      else if (hbb && f1) cdv = R(0.5) * (cp - c0);
-      const R aw = alpha * weight<R>(k);
-      if (lat_cx(k)) gx += aw * R(lat_cx(k)) * cdv;
-      if (lat_cy(k)) gy += aw * R(lat_cy(k)) * cdv;
-      if (lat_cz(k)) gz += aw * R(lat_cz(k)) * cdv;
-      R lv = 0;
-      if (b1 && f1) lv = cm - R(2) * c0 + cp;
-      else if (b1 || f1) {
-        const R f1v = b1 ? cm : cp;
-        lv = hbb ? (f1v - c0 - bnd) : (R(2) * f1v - R(2) * c0 - R(2) * bnd);
-      }
-      lap += aw * lv;
+    for (int k = 1; k < Q; k += 2) {
+      const R cm = s_c[pos - T::off(k)], cp = s_c[pos + T::off(k)];
+      const R aw2 = R(2) * alpha * weight<R>(k);
+      const R cdv = cd_val(c0, cm, cp, hbb);
+      if (lat_cx(k)) gx += aw2 * R(lat_cx(k)) * cdv;
+      if (lat_cy(k)) gy += aw2 * R(lat_cy(k)) * cdv;
+      if (lat_cz(k)) gz += aw2 * R(lat_cz(k)) * cdv;
+      lap += aw2 * lap_val(c0, cm, cp, bnd, hbb);
     }
-    uint8_t flag = 0;
-    if (Pm.open_bnd) flag = D.bcflag[i];
-    const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : c0;
     const R rho = rho1 + drho * c0;
-    const R mu = four_beta * (cm_ * (R(1) - cm_)) * (R(0.5) - cm_) + (-kappa * lap);
-    R ux, uy, uz;
-    F* ubc = static_cast<F*>(D.u_bc);
-    if (flag & BC_SITE) {
-      ux = (R)ubc[i]; uy = (R)ubc[D.n + i]; uz = (R)ubc[2 * D.n + i];
-    } else {
-      const R inv = R(1) / (cs2 * rho);
-      ux = (R)fjx[i] * inv; uy = (R)fjy[i] * inv; uz = (R)fjz[i] * inv;
-    }
-    R p = (R)fp[i];
-    if (!(flag & BC_PROC)) {
-      const R mor = mu / rho;
-      ux = ux + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff / rho + mor * gx);
-      uy = uy + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff / rho + mor * gy);
-      uz = uz + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
-      const R u_dot_drho = drho * (ux * gx + uy * gy + uz * gz);
-      p += R(0.5) * u_dot_drho * cs2;
-      fp[i] = (F)p;
-    }
+    const R mu = four_beta * (c0 * (R(1) - c0)) * (R(0.5) - c0) + (-kappa * lap);
     fmu[i] = (F)mu;
-    if (flag & BC_SITE) { ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz; }
-    if (OUT) {
-      const int64_t q = D.ref_of[i];
-      out.c[q] = (double)c0;
-      out.rho[q] = (double)rho;
-      out.ux[q] = (double)ux;
-      out.uy[q] = (double)uy;
-      out.uz[q] = (double)uz;
-      out.p[q] = (double)p;
-      out.mu[q] = (double)mu;
+    // the correction changes p only through drho (k_vel_press_corr :194-195);
+    // u is needed here only for that, or for output
+    if (Pm.drho != 0.0 || OUT) {
+      const R inv = R(1) / (cs2 * rho);
+      const R mor = mu / rho;
+      const R ux = (R)fjx[i] * inv + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff / rho + mor * gx);
+      const R uy = (R)fjy[i] * inv + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff / rho + mor * gy);
+      const R uz = (R)fjz[i] * inv + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
+      const R p = (R)fp[i] + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
+      if (Pm.drho != 0.0) fp[i] = (F)p;
+      if (OUT) {
+        const int64_t q = D.ref_of[i];
+        out.c[q] = (double)c0;
+        out.rho[q] = (double)rho;
+        out.ux[q] = (double)ux;
+        out.uy[q] = (double)uy;
+        out.uz[q] = (double)uz;
+        out.p[q] = (double)p;
+        out.mu[q] = (double)mu;
+      }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
 // P3: Laplacian of mu, boundary half zero (reference k_pack_lap_zero :168-173
-// + k_lap_mf).
+// + k_lap_mf); symmetric within an opposite pair.
 // ---------------------------------------------------------------------------
-template <class S>
+template <class S, class Sh>
 __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
   using R = typename S::real;
   using F = typename S::fld;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  using T = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 1> it;
+  __shared__ R s_m[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  tile_setup<1>(D, wk.y, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
-  __syncthreads();
-  R* s_m = reinterpret_cast<R*>(dsm + ((ts.ntile * 4 + 15) & ~15));
-  stage_field<S>(D, ts, s_idx, s_m, static_cast<const F*>(D.mu), false, 0.0);
+  prologue<Sh>(D, wk.y, s);
+  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  stage<Sh, 1>(s, static_cast<const F*>(D.mu), s_m, false, 0.0, it.idx);
   __syncthreads();
   const bool hbb = D.prm.hbb != 0;
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
+  const int first = s.rec.first, cnt = s.rec.cnt;
+  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+    const int pos = T::pos(s.slot_of[r]);
     const R m0 = s_m[pos];
     R lap = 0;
 #pragma unroll
-    for (int k = 1; k < Q; ++k) {
-      const int o = ts.off1[k];
-      const bool b1 = s_idx[pos - o] >= 0, f1 = s_idx[pos + o] >= 0;
-      R lv = 0;
-      if (b1 && f1) lv = s_m[pos - o] - R(2) * m0 + s_m[pos + o];
-      else if (b1 || f1) {
-        const R f1v = b1 ? s_m[pos - o] : s_m[pos + o];
-        lv = hbb ? (f1v - m0) : (R(2) * f1v - R(2) * m0);
-      }
-      lap += alpha * weight<R>(k) * lv;
-    }
-    flm[i] = (F)lap;
+    for (int k = 1; k < Q; k += 2)
+      lap += R(2) * alpha * weight<R>(k) * lap_val(m0, s_m[pos - T::off(k)], s_m[pos + T::off(k)], R(0), hbb);
+    flm[first + r] = (F)lap;
   }
 }
+
+// P4 (k_collide) lives in collide.cuh.
 
 // ---------------------------------------------------------------------------
-// P4: fused equilibria + Guo force + BGK/MRT collision (reference
-// k_collide_fused_mrt :547-651 and k_collide_fused_bgk :459-545, with the
-// directional helpers cd_dir_val/bd_dir_val/avg_dir_val :89-113 evaluated
-// from the staged tiles, and the open-boundary overwrite of g,
-// k_open_bnd/k_open_bnd_buf :761-798,826-846, folded in). The corrected
-// velocity is rebuilt from the pulled g (same g as P1) instead of being
-// stored. Writes post-collision h, g to the other buffer.
-// ---------------------------------------------------------------------------
-template <class R>
-struct DirVals {
-  R cdc, cdp, bdc, bdp;
-};
-
-template <class R>
-__device__ __forceinline__ DirVals<R> dir_vals(const int32_t* s_idx, const R* s_c, const R* s_p, int pos, int o1,
-                                               int o2, R c0, R p0, bool hbb) {
-  const bool b1 = s_idx[pos - o1] >= 0, f1 = s_idx[pos + o1] >= 0;
-  DirVals<R> v;
-  // central-difference pair (multiphase_gpu.cuh:118-120)
-  if (b1 && f1) { v.cdc = R(0.5) * (s_c[pos + o1] - s_c[pos - o1]); v.cdp = R(0.5) * (s_p[pos + o1] - s_p[pos - o1]); }
-  else if (hbb && b1) { v.cdc = R(0.5) * (c0 - s_c[pos - o1]); v.cdp = R(0.5) * (p0 - s_p[pos - o1]); }
-  else if (hbb && f1) { v.cdc = R(0.5) * (s_c[pos + o1] - c0); v.cdp = R(0.5) * (s_p[pos + o1] - p0); }
-  else { v.cdc = 0; v.cdp = 0; }
-  // biased cases (multiphase_gpu.cuh:142-152, device_engine.cuh:96-107)
-  if (f1) {
-    const bool f2 = s_idx[pos + o2] >= 0;
-    const R c1 = s_c[pos + o1], p1 = s_p[pos + o1];
-    if (f2) {
-      v.bdc = R(-1.5) * c0 + R(2.0) * c1 + R(-0.5) * s_c[pos + o2];
-      v.bdp = R(-1.5) * p0 + R(2.0) * p1 + R(-0.5) * s_p[pos + o2];
-    } else if (!hbb) {
-      v.bdc = R(-2.0) * c0 + R(2.0) * c1;
-      v.bdp = R(-2.0) * p0 + R(2.0) * p1;
-    } else {
-      v.bdc = R(-1.5) * c0 + R(1.5) * c1;
-      v.bdp = R(-1.5) * p0 + R(1.5) * p1;
-    }
-  } else if (!hbb) {
-    v.bdc = 0; v.bdp = 0;
-    if (b1 && s_idx[pos - o2] >= 0) {
-      v.bdc = R(-1.5) * c0 + R(2.0) * s_c[pos - o1] + R(-0.5) * s_c[pos - o2];
-      v.bdp = R(-1.5) * p0 + R(2.0) * s_p[pos - o1] + R(-0.5) * s_p[pos - o2];
-    }
-  } else if (b1) {
-    v.bdc = R(0.5) * c0 + R(-0.5) * s_c[pos - o1];
-    v.bdp = R(0.5) * p0 + R(-0.5) * s_p[pos - o1];
-  } else {
-    v.bdc = 0; v.bdp = 0;
-  }
-  return v;
-}
-
-// M^-1 S M applied to x (S diagonal, conserved rows zero), with the moment
-// matrix folded at compile time. srate[kind] = rate of that moment kind.
-template <class R>
-__device__ __forceinline__ void mrt_apply(R (&x)[Q], const R (&srate)[7]) {
-  R m[Q];
-#pragma unroll
-  for (int j = 0; j < Q; ++j) {
-    if (mrt_kind(j) == MK_CONS) { m[j] = R(0); continue; }
-    R acc = R(0);
-#pragma unroll
-    for (int k = 0; k < Q; ++k) {
-      const int mk = mrt_M(j, k);
-      if (mk == 1) acc += x[k];
-      else if (mk == -1) acc -= x[k];
-      else if (mk != 0) acc += R(mk) * x[k];
-    }
-    m[j] = acc * (srate[mrt_kind(j)] * (R(1) / R(mrt_norm2(j))));
-  }
-#pragma unroll
-  for (int k = 0; k < Q; ++k) {
-    R acc = R(0);
-#pragma unroll
-    for (int j = 0; j < Q; ++j) {
-      if (mrt_kind(j) == MK_CONS) continue;
-      const int mk = mrt_M(j, k);
-      if (mk == 1) acc += m[j];
-      else if (mk == -1) acc -= m[j];
-      else if (mk != 0) acc += R(mk) * m[j];
-    }
-    x[k] = acc;
-  }
-}
-
-template <class S, int MRT>
-__global__ void __launch_bounds__(CTA) k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                  int parity) {
-  using R = typename S::real;
-  using P = typename S::pop;
-  using F = typename S::fld;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
-  const int2 wk = work[blockIdx.x];
-  const LatDesc& D = descs[wk.x];
-  const int brick = wk.y;
-  tile_setup<2>(D, brick, ts);
-  load_step_scalars<S>(D, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
-  __syncthreads();
-  const int nt16 = (ts.ntile * 4 + 15) & ~15;
-  const int ntr = (ts.ntile * (int)sizeof(R) + 15) & ~15;
-  R* s_c = reinterpret_cast<R*>(dsm + nt16);
-  R* s_p = reinterpret_cast<R*>(dsm + nt16 + ntr);
-  R* s_l = reinterpret_cast<R*>(dsm + nt16 + 2 * ntr);
-  stage_field<S>(D, ts, s_idx, s_c, static_cast<const F*>(D.c), true, ts.lambda);
-  stage_field<S>(D, ts, s_idx, s_p, static_cast<const F*>(D.p), false, 0.0);
-  stage_field<S>(D, ts, s_idx, s_l, static_cast<const F*>(D.lapmu), false, 0.0);
-  __syncthreads();
-
-  const DevPrm& Pm = D.prm;
-  const bool hbb = Pm.hbb != 0;
-  const R cs2 = R(CS2), alpha = R(ALPHA), beta_c = R(BETA), gamma_c = R(GAMMA);
-  const R rho1 = (R)Pm.rho1, drho = (R)Pm.drho, mobility = (R)Pm.mobility;
-  const R tau0 = (R)Pm.tau0, tau1 = (R)Pm.tau1, ffac = (R)ts.ff;
-  const R gxa = (R)Pm.gx, gya = (R)Pm.gy, gza = (R)Pm.gz;
-  const R fxa = (R)Pm.fx * ffac, fya = (R)Pm.fy * ffac, fza = (R)Pm.fz * ffac;
-  const P* __restrict__ gin = static_cast<const P*>(D.pop[parity][1]);
-  P* __restrict__ hout = static_cast<P*>(D.pop[parity ^ 1][0]);
-  P* __restrict__ gout = static_cast<P*>(D.pop[parity ^ 1][1]);
-  const F* __restrict__ fmu = static_cast<const F*>(D.mu);
-  const Shift shh{(float)Pm.c_ref, (float)(1.0 / Pm.h_scale), (float)Pm.h_scale};
-  const Shift shg{(float)Pm.p_ref, (float)(1.0 / Pm.g_scale), (float)Pm.g_scale};
-  double st[6] = {0, 0, 0, 0, 0, 0};
-  int bad = 0;
-
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
-    const R c = s_c[pos], p = s_p[pos], lmu = s_l[pos];
-    const R mu = (R)fmu[i];
-    // pulled g (identical to what P1 read)
-    R g[Q];
-#pragma unroll
-    for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - ts.off1[k]];
-      const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
-      g[k] = ld_pop<S>(gin, a, up >= 0 ? k : lat_opp(k), shg);
-    }
-    // gradients of c and p: central (eq) and biased (force) from the tiles
-    R e_dcx = 0, e_dcy = 0, e_dcz = 0, e_dpx = 0, e_dpy = 0, e_dpz = 0;
-    R b_dcx = 0, b_dcy = 0, b_dcz = 0, b_dpx = 0, b_dpy = 0, b_dpz = 0;
-#pragma unroll
-    for (int k = 1; k < Q; ++k) {
-      const DirVals<R> v = dir_vals<R>(s_idx, s_c, s_p, pos, ts.off1[k], ts.off2[k], c, p, hbb);
-      const R aw = alpha * weight<R>(k);
-      if (lat_cx(k)) {
-        const R e = aw * R(lat_cx(k));
-        e_dcx += e * v.cdc; e_dpx += e * v.cdp; b_dcx += e * v.bdc; b_dpx += e * v.bdp;
-      }
-      if (lat_cy(k)) {
-        const R e = aw * R(lat_cy(k));
-        e_dcy += e * v.cdc; e_dpy += e * v.cdp; b_dcy += e * v.bdc; b_dpy += e * v.bdp;
-      }
-      if (lat_cz(k)) {
-        const R e = aw * R(lat_cz(k));
-        e_dcz += e * v.cdc; e_dpz += e * v.cdp; b_dcz += e * v.bdc; b_dpz += e * v.bdp;
-      }
-    }
-    const R f_dcx = R(0.5) * (e_dcx + b_dcx), f_dcy = R(0.5) * (e_dcy + b_dcy), f_dcz = R(0.5) * (e_dcz + b_dcz);
-    const R f_dpx = R(0.5) * (e_dpx + b_dpx), f_dpy = R(0.5) * (e_dpy + b_dpy), f_dpz = R(0.5) * (e_dpz + b_dpz);
-
-    const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
-    const R rho = rho1 + drho * c;
-    const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : c;
-    // relaxation rate (reference k_moments :130-132)
-    const R cpc = cm_ < R(0) ? R(0) : (cm_ > R(1) ? R(1) : cm_);
-    const R tau = R(1) / (cpc / tau0 + (R(1) - cpc) / tau1);
-    const R s0 = R(1) / (tau + R(0.5));
-    // corrected velocity (k_moments + k_vel_press_corr)
-    R ux, uy, uz;
-    if (flag & BC_SITE) {
-      const F* ubc = static_cast<const F*>(D.u_bc);
-      ux = (R)ubc[i]; uy = (R)ubc[D.n + i]; uz = (R)ubc[2 * D.n + i];
-    } else {
-      R jx = 0, jy = 0, jz = 0;
-#pragma unroll
-      for (int k = 0; k < Q; ++k) {
-        if (lat_cx(k)) jx += R(lat_cx(k)) * g[k];
-        if (lat_cy(k)) jy += R(lat_cy(k)) * g[k];
-        if (lat_cz(k)) jz += R(lat_cz(k)) * g[k];
-      }
-      const R inv = R(1) / (cs2 * rho);
-      const R mor = mu / rho;
-      ux = jx * inv + R(0.5) * (gxa + fxa / rho + mor * e_dcx);
-      uy = jy * inv + R(0.5) * (gya + fya / rho + mor * e_dcy);
-      uz = jz * inv + R(0.5) * (gza + fza / rho + mor * e_dcz);
-    }
-    // open-boundary overwrite of g by the plain equilibrium (apply_open_bnd)
-    if (flag & BC_G_OVER) {
-      const int64_t sb = D.bcsrc[i];
-      const F* ubc = static_cast<const F*>(D.u_bc);
-      const R bux = (R)ubc[sb], buy = (R)ubc[D.n + sb], buz = (R)ubc[2 * D.n + sb];
-      const R bp = (R) static_cast<const F*>(D.p)[sb];
-      const R bc = (R) static_cast<const F*>(D.c)[sb];
-      const R brho = rho1 + drho * bc;
-      const R bu_sq = bux * bux + buy * buy + buz * buz;
-#pragma unroll
-      for (int k = 0; k < Q; ++k) {
-        const R uk = bux * R(lat_cx(k)) + buy * R(lat_cy(k)) + buz * R(lat_cz(k));
-        const R u_term = uk * (alpha + beta_c * uk) - gamma_c * bu_sq;
-        g[k] = weight<R>(k) * (bp + brho * cs2 * u_term);
-      }
-    }
-    const R bfx = rho * gxa + fxa, bfy = rho * gya + fya, bfz = rho * gza + fza;
-    const R u2 = ux * ux + uy * uy + uz * uz;
-    st[0] += (double)ux; st[1] += (double)uy; st[2] += (double)uz; st[3] += (double)u2; st[4] += (double)c;
-    st[5] = fmax(st[5], (double)u2);
-    bad |= !(u2 < R(1e30));
-
-    R x[Q];   // MRT: raw collision term eq_g - g;  BGK: unused
-    R gpf[Q]; // g + force_g (MRT) or the new g (BGK)
-    if (MRT) {
-      const R drho_cs2 = drho * cs2, rho_cs2 = rho * cs2, c_over = c / rho_cs2;
-      const R drcx = drho_cs2 * e_dcx, drcy = drho_cs2 * e_dcy, drcz = drho_cs2 * e_dcz;
-      const R e_fgx = mu * e_dcx + bfx, e_fgy = mu * e_dcy + bfy, e_fgz = mu * e_dcz + bfz;
-      const R e_fhx = e_dcx - c_over * (e_dpx - e_fgx), e_fhy = e_dcy - c_over * (e_dpy - e_fgy),
-              e_fhz = e_dcz - c_over * (e_dpz - e_fgz);
-      const R gamma_u_sq = gamma_c * u2;
-      const R u_term_h = ux * e_fhx + uy * e_fhy + uz * e_fhz;
-      const R u_force_g = ux * e_fgx + uy * e_fgy + uz * e_fgz;
-      const R u_drho = ux * drcx + uy * drcy + uz * drcz;
-      const R drmx = drho_cs2 * f_dcx, drmy = drho_cs2 * f_dcy, drmz = drho_cs2 * f_dcz;
-      const R f_fgx = mu * f_dcx + bfx, f_fgy = mu * f_dcy + bfy, f_fgz = mu * f_dcz + bfz;
-      const R f_fhx = f_dcx - c_over * (f_dpx - f_fgx), f_fhy = f_dcy - c_over * (f_dpy - f_fgy),
-              f_fhz = f_dcz - c_over * (f_dpz - f_fgz);
-      const R u_fh_f = ux * f_fhx + uy * f_fhy + uz * f_fhz;
-      const R u_drm = ux * drmx + uy * drmy + uz * drmz;
-      const R u_fg_f = ux * f_fgx + uy * f_fgy + uz * f_fgz;
-#pragma unroll
-      for (int k = 0; k < Q; ++k) {
-        const R w = weight<R>(k);
-        const R uk = ux * R(lat_cx(k)) + uy * R(lat_cy(k)) + uz * R(lat_cz(k));
-        const R u_term = uk * (alpha + beta_c * uk) - gamma_u_sq;
-        const R G = w * (R(1) + u_term);
-        const R w_u_term = G - w;
-        const R f_proj = bfx * R(lat_cx(k)) + bfy * R(lat_cy(k)) + bfz * R(lat_cz(k));
-        DirVals<R> v{0, 0, 0, 0};
-        R avgk = lmu;
-        if (k > 0) {
-          v = dir_vals<R>(s_idx, s_c, s_p, pos, ts.off1[k], ts.off2[k], c, p, hbb);
-          if (s_idx[pos + ts.off1[k]] >= 0) avgk = R(0.5) * (lmu + s_l[pos + ts.off1[k]]);
-        }
-        const R drho_dk = drho_cs2 * v.cdc;
-        const R eh = c * G + R(0.5) * G * (u_term_h - v.cdc + c_over * (v.cdp - mu * v.cdc - f_proj));
-        const R eg = w * p + rho_cs2 * w_u_term +
-                     R(0.5) * ((u_drho - drho_dk) * w_u_term + (u_force_g + mu * v.cdc + f_proj) * G);
-        const R dc_dk = R(0.5) * (v.cdc + v.bdc), dp_dk = R(0.5) * (v.cdp + v.bdp);
-        const R drho_dk2 = drho_cs2 * dc_dk;
-        const R ffk = mu * dc_dk + f_proj;
-        const R fh = G * (dc_dk - c_over * (dp_dk - ffk) - u_fh_f + mobility * avgk);
-        const R fg = (drho_dk2 - u_drm) * w_u_term + (ffk - u_fg_f) * G;
-        st_pop<S>(hout, pidx(i, k), k, eh + fh, shh);
-        x[k] = eg - g[k];
-        gpf[k] = g[k] + fg;
-      }
-      // rates (reference device_engine.cuh:623-625 with per-kind modes)
-      const R taus = R(1) / s0 - R(0.5);
-      const R s1 = R(2) * taus / (R(2) * (R)Pm.mrt_lambda + taus);
-      R srate[7];
-#pragma unroll
-      for (int q = 0; q < 7; ++q)
-        srate[q] = Pm.rate_mode[q] == RATE_S0 ? s0 : (Pm.rate_mode[q] == RATE_MAGIC ? s1 : (R)Pm.rate_value[q]);
-      mrt_apply<R>(x, srate);
-#pragma unroll
-      for (int k = 0; k < Q; ++k) st_pop<S>(gout, pidx(i, k), k, gpf[k] + x[k], shg);
-    } else {
-      const R relax = s0;
-      const R drcx = drho * e_dcx * cs2, drcy = drho * e_dcy * cs2, drcz = drho * e_dcz * cs2;
-      const R e_fgx = mu * e_dcx + bfx, e_fgy = mu * e_dcy + bfy, e_fgz = mu * e_dcz + bfz;
-      const R a_over_rho = alpha / rho;
-      const R e_fhx = e_dcx - c * a_over_rho * (e_dpx - e_fgx), e_fhy = e_dcy - c * a_over_rho * (e_dpy - e_fgy),
-              e_fhz = e_dcz - c * a_over_rho * (e_dpz - e_fgz);
-      const R u_fh_e = ux * e_fhx + uy * e_fhy + uz * e_fhz;
-      const R u_drhocd = ux * drcx + uy * drcy + uz * drcz;
-      const R u_fg_e = ux * e_fgx + uy * e_fgy + uz * e_fgz;
-      const R drho_cs2 = drho * cs2;
-      const R drmx = drho_cs2 * f_dcx, drmy = drho_cs2 * f_dcy, drmz = drho_cs2 * f_dcz;
-      const R c_over = c / cs2 / rho;
-      const R f_fgx = mu * f_dcx + bfx, f_fgy = mu * f_dcy + bfy, f_fgz = mu * f_dcz + bfz;
-      const R f_fhx = f_dcx - c_over * (f_dpx - f_fgx), f_fhy = f_dcy - c_over * (f_dpy - f_fgy),
-              f_fhz = f_dcz - c_over * (f_dpz - f_fgz);
-      const R u_fh_f = ux * f_fhx + uy * f_fhy + uz * f_fhz;
-      const R u_drm = ux * drmx + uy * drmy + uz * drmz;
-      const R u_fg_f = ux * f_fgx + uy * f_fgy + uz * f_fgz;
-#pragma unroll
-      for (int k = 0; k < Q; ++k) {
-        const R w = weight<R>(k);
-        const R uk = ux * R(lat_cx(k)) + uy * R(lat_cy(k)) + uz * R(lat_cz(k));
-        const R u_term = uk * (alpha + beta_c * uk) - gamma_c * u2;
-        const R G = w * (R(1) + u_term);
-        const R f_proj = bfx * R(lat_cx(k)) + bfy * R(lat_cy(k)) + bfz * R(lat_cz(k));
-        DirVals<R> v{0, 0, 0, 0};
-        R avgk = lmu;
-        if (k > 0) {
-          v = dir_vals<R>(s_idx, s_c, s_p, pos, ts.off1[k], ts.off2[k], c, p, hbb);
-          if (s_idx[pos + ts.off1[k]] >= 0) avgk = R(0.5) * (lmu + s_l[pos + ts.off1[k]]);
-        }
-        const R drho_dk = drho * v.cdc * cs2;
-        R eh = c * G;
-        eh -= R(0.5) * G * (v.cdc - c * a_over_rho * (v.cdp - mu * v.cdc - f_proj));
-        eh += R(0.5) * G * u_fh_e;
-        R eg = w * (p + rho * cs2 * u_term);
-        eg -= R(0.5) * (drho_dk * (G - w) + (mu * v.cdc + f_proj) * G);
-        eg += R(0.5) * ((G - w) * u_drhocd + G * u_fg_e);
-        const R dGk = G - w;
-        const R dc_dk = R(0.5) * (v.cdc + v.bdc), dp_dk = R(0.5) * (v.cdp + v.bdp);
-        const R drho_dk2 = drho_cs2 * dc_dk;
-        const R ffk = mu * dc_dk + f_proj;
-        const R fh = G * (dc_dk - c_over * (dp_dk - ffk) - u_fh_f + mobility * avgk);
-        const R fg = (drho_dk2 - u_drm) * dGk + (ffk - u_fg_f) * G;
-        st_pop<S>(hout, pidx(i, k), k, eh + fh, shh);
-        st_pop<S>(gout, pidx(i, k), k, g[k] + relax * (eg - g[k]) + fg, shg);
-      }
-      (void)x; (void)gpf;
-    }
-  }
-  // flow-statistics partials (reference k_flow_stats :660-683, summed on demand)
-  block_sum<6>(st, ts, true);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int q = 0; q < 6; ++q) D.part4[(int64_t)brick * 6 + q] = st[q];
-    if (bad) atomicOr(&D.ctl->status, 1);
-  }
-  if (!last_block(&D.ctl->count4, (unsigned)D.nbricks, ts)) return;
-  if (threadIdx.x == 0) {
-    Ctl* C = D.ctl;
-    C->t += 1;
-    if (Pm.open_bnd) C->open_step += 1;
-    C->pending = (C->auto_correct && Pm.correct_mass) ? 1 : 0;
-    C->lambda = 0.0;
-    C->count4 = 0;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// open-boundary field enforcement (reference enforce_open_bnd_fields,
-// multiphase_gpu.cuh:404-418: k_open_bnd_fields :738-759 and the injection
-// gate d_inlet_gate :699-728), run between P1 and P2. Saves each boundary
-// site's moment value of c (for mu and tau, which the reference keeps from
-// the moments) and its velocity, then imposes the prescribed fields.
+// open boundaries, run between P1 and P2 (reference enforce_open_bnd_fields,
+// multiphase_gpu.cuh:404-418, and the velocity/pressure correction of the
+// boundary nodes). Three small kernels over the boundary node lists:
+//  k_bc_fields  (inlet, outlet) save the moment value of c (mu and tau keep
+//               it, as in the reference), form u from j, impose u/p/c
+//               (k_open_bnd_fields :738-759, gate d_inlet_gate :699-728);
+//  k_bc_buffers (buffers) copy the reference vertex's fields
+//               (k_open_bnd_buf_fields :807-815);
+//  k_bc_final   (all) mu, and the correction of u and p where the node is
+//               not imposed, so that P2 and P4 only read final values.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double inlet_gate(const DevPrm& P, unsigned step, double coord) {
   const double w = P.inlet_ramp;
@@ -964,7 +685,6 @@ __global__ void k_bc_fields(const LatDesc* __restrict__ descs, int lat) {
   ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz;
 }
 
-// copy_to_buffers field copy (k_open_bnd_buf_fields :807-815)
 template <class S>
 __global__ void k_bc_buffers(const LatDesc* __restrict__ descs, int lat) {
   using F = typename S::fld;
@@ -981,24 +701,86 @@ __global__ void k_bc_buffers(const LatDesc* __restrict__ descs, int lat) {
   ubc[b] = ubc[r]; ubc[D.n + b] = ubc[D.n + r]; ubc[2 * D.n + b] = ubc[2 * D.n + r];
 }
 
+// Site index of node (x, y, z) (periodic), -1 if solid: brick grid + occupancy.
+__device__ __forceinline__ int64_t site_at(const LatDesc& D, int x, int y, int z) {
+  x = (x % D.nx + D.nx) % D.nx;
+  y = (y % D.ny + D.ny) % D.ny;
+  z = (z % D.nz + D.nz) % D.nz;
+  const int bx = x >> D.lbx, by = y >> D.lby, bz = z >> D.lbz;
+  const int id = D.brick_grid[((int64_t)bz * D.nby + by) * D.nbx + bx];
+  if (id < 0) return -1;
+  const int slot = (x & ((1 << D.lbx) - 1)) | ((y & ((1 << D.lby) - 1)) << D.lbx) |
+                   ((z & ((1 << D.lbz) - 1)) << (D.lbx + D.lby));
+  const int w = slot >> 6, b = slot & 63;
+  const uint64_t m = D.mask[(int64_t)id * D.words + w];
+  if (!((m >> b) & 1ull)) return -1;
+  return D.base[(int64_t)id * D.words + w] + __popcll(m & ((1ull << b) - 1ull));
+}
+
+// mu and the velocity/pressure correction of every boundary node, exactly as
+// P2 computes them for interior sites (the node's own c enters the wetting
+// term and the chemical potential keeps the moment value of c).
+template <class S>
+__global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
+  using R = typename S::real;
+  using F = typename S::fld;
+  const LatDesc& D = descs[lat];
+  const DevPrm& Pm = D.prm;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= D.n_inlet + D.n_outlet + D.n_buf) return;
+  const int64_t i = j < D.n_inlet + D.n_outlet ? D.bc_list[j] : D.buf_verts[j - D.n_inlet - D.n_outlet];
+  F* fc = static_cast<F*>(D.c);
+  F* fp = static_cast<F*>(D.p);
+  F* ubc = static_cast<F*>(D.u_bc);
+  const int x = D.bc_xyz[3 * j], y = D.bc_xyz[3 * j + 1], z = D.bc_xyz[3 * j + 2];
+  const R c0 = (R)fc[i];
+  const R bnd = (R)Pm.bnd_coeff * c0 * (R(1) - c0);
+  const bool hbb = Pm.hbb != 0;
+  R gx = 0, gy = 0, gz = 0, lap = 0;
+  for (int k = 1; k < Q; ++k) {
+    const int ex = D.nx > 1 ? lat_cx(k) : 0, ey = D.ny > 1 ? lat_cy(k) : 0, ez = D.nz > 1 ? lat_cz(k) : 0;
+    const int64_t im = site_at(D, x - ex, y - ey, z - ez), ip = site_at(D, x + ex, y + ey, z + ez);
+    const R cm = im >= 0 ? (R)fc[im] : nan_v<R>(), cp = ip >= 0 ? (R)fc[ip] : nan_v<R>();
+    const R aw = R(ALPHA) * weight<R>(k);
+    const R cdv = cd_val(c0, cm, cp, hbb);
+    gx += aw * R(lat_cx(k)) * cdv;
+    gy += aw * R(lat_cy(k)) * cdv;
+    gz += aw * R(lat_cz(k)) * cdv;
+    lap += aw * lap_val(c0, cm, cp, bnd, hbb);
+  }
+  const R craw = (R) static_cast<const F*>(D.c_raw_bc)[i];
+  const R mu = (R)Pm.four_beta * (craw * (R(1) - craw)) * (R(0.5) - craw) + (-(R)Pm.kappa * lap);
+  static_cast<F*>(D.mu)[i] = (F)mu;
+  if (D.bcflag[i] & BC_PROC) return;
+  const R rho = (R)Pm.rho1 + (R)Pm.drho * c0;
+  const R ff = (R)forcing_factor_dev(Pm, *D.ctl);
+  const R mor = mu / rho;
+  const R ux = (R)ubc[i] + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff / rho + mor * gx);
+  const R uy = (R)ubc[D.n + i] + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff / rho + mor * gy);
+  const R uz = (R)ubc[2 * D.n + i] + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
+  ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz;
+  fp[i] = (F)((R)fp[i] + R(0.5) * ((R)Pm.drho * (ux * gx + uy * gy + uz * gz)) * R(CS2));
+}
+
 // ---------------------------------------------------------------------------
 // state transfer and reductions
 // ---------------------------------------------------------------------------
 // Post-stream state in the reference layout f[k*n + ref(i)] (double), with a
 // queued mass correction injected as the reference's k_inject_mass does.
-template <class S>
+template <class S, class Sh>
 __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                          int parity, double* __restrict__ h_out,
                                                          double* __restrict__ g_out, int apply_lambda) {
   using R = typename S::real;
   using P = typename S::pop;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  using T = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 1> it;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  tile_setup<1>(D, wk.y, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
+  prologue<Sh>(D, wk.y, s);
+  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  const int32_t* s_idx = it.idx;
   __syncthreads();
   const P* hin = static_cast<const P*>(D.pop[parity][0]);
   const P* gin = static_cast<const P*>(D.pop[parity][1]);
@@ -1006,16 +788,15 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   const double lambda = apply_lambda ? D.ctl->lambda : 0.0;
   const int64_t n = D.n;
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
+  for (int r = threadIdx.x; r < s.rec.cnt; r += blockDim.x) {
+    const int64_t i = s.rec.first + r;
+    const int pos = T::pos(s.slot_of[r]);
     const int64_t q = D.ref_of[i];
     R hv[Q];
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - ts.off1[k]];
+      const int up = s_idx[pos - T::off(k)];
       const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
       const int kk = up >= 0 ? k : lat_opp(k);
       hv[k] = ld_pop<S>(hin, a, kk, shh);
@@ -1035,32 +816,32 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
 
 // Inverse of the pull: place post-stream values so that the next P1 pulls
 // them back (reference upload_state, multiphase_gpu.cuh:354-359).
-template <class S>
+template <class S, class Sh>
 __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                        int parity, const double* __restrict__ h_in,
                                                        const double* __restrict__ g_in) {
   using P = typename S::pop;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  using T = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 1> it;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  tile_setup<1>(D, wk.y, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
+  prologue<Sh>(D, wk.y, s);
+  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  const int32_t* s_idx = it.idx;
   __syncthreads();
   P* hb = static_cast<P*>(D.pop[parity][0]);
   P* gb = static_cast<P*>(D.pop[parity][1]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   const int64_t n = D.n;
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
+  for (int r = threadIdx.x; r < s.rec.cnt; r += blockDim.x) {
+    const int64_t i = s.rec.first + r;
+    const int pos = T::pos(s.slot_of[r]);
     const int64_t q = D.ref_of[i];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - ts.off1[k]];
+      const int up = s_idx[pos - T::off(k)];
       const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
       const int kk = up >= 0 ? k : lat_opp(k);
       st_pop<S>(hb, a, kk, (typename S::real)h_in[k * n + q], shh);
@@ -1070,33 +851,32 @@ __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict_
 }
 
 // M = sum c, W = sum c(1-c)^+ of the post-stream state (reference
-// k_mass_weight :1109-1126) into ctl->M, ctl->W; with `queue` the lambda of a
-// queued correction is formed as in P1.
-template <class S>
+// k_mass_weight :1109-1126) into ctl->M, ctl->W, and the lambda of a queued
+// correction as P1 forms it.
+template <class S, class Sh>
 __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                int parity, double* __restrict__ part) {
-  using R = typename S::real;
   using P = typename S::pop;
-  __shared__ TileShared ts;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  using T = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 1> it;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
-  tile_setup<1>(D, brick, ts);
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  for (int t = threadIdx.x; t < ts.ntile; t += blockDim.x) s_idx[t] = tile_site(D, ts, t);
+  prologue<Sh>(D, brick, s);
+  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  const int32_t* s_idx = it.idx;
   __syncthreads();
   const P* hin = static_cast<const P*>(D.pop[parity][0]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   double acc[2] = {0.0, 0.0};
-  for (int r = threadIdx.x; r < ts.cnt; r += blockDim.x) {
-    const int s = ts.slot_of[r];
-    const int64_t i = ts.first + r;
-    const int pos = slot_pos(D, ts, s);
+  for (int r = threadIdx.x; r < s.rec.cnt; r += blockDim.x) {
+    const int64_t i = s.rec.first + r;
+    const int pos = T::pos(s.slot_of[r]);
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - ts.off1[k]];
+      const int up = s_idx[pos - T::off(k)];
       const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
       cd += (double)ld_pop<S>(hin, a, up >= 0 ? k : lat_opp(k), shh);
     }
@@ -1105,35 +885,27 @@ __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs,
     acc[0] += cd;
     acc[1] += phi;
   }
-  block_sum<2>(acc, ts);
+  block_sum<2>(acc, s);
   if (threadIdx.x == 0) {
     part[(int64_t)brick * 2 + 0] = acc[0];
     part[(int64_t)brick * 2 + 1] = acc[1];
   }
-  if (!last_block(&D.ctl->countm, (unsigned)D.nbricks, ts)) return;
+  if (!last_block(&D.ctl->countm, (unsigned)D.nbricks, s)) return;
   double tot[2];
-  sum_partials<2>(part, D.nbricks, 2, tot, ts);
+  sum_partials<2>(part, D.nbricks, 2, tot, s);
   if (threadIdx.x == 0) {
-    Ctl* C = D.ctl;
-    C->M = tot[0];
-    C->W = tot[1];
-    double lam = 0.0;
-    if (C->pending) {
-      const double drift = tot[0] - C->target_mass;
-      C->drift = drift;
-      if (tot[1] > 0.0 && drift != 0.0) lam = drift / tot[1];
-    }
-    C->lambda = lam;
-    C->countm = 0;
+    finish_mass(D.ctl, tot[0], tot[1]);
+    D.ctl->countm = 0;
   }
 }
 
 // Sum the flow-statistics partials of the last collision pass into ctl->stats.
+template <class Sh>
 __global__ void __launch_bounds__(CTA) k_stats_finalize(const LatDesc* __restrict__ descs, int lat) {
-  __shared__ TileShared ts;
+  __shared__ Pro<Sh> s;
   const LatDesc& D = descs[lat];
   double tot[6];
-  sum_partials<6>(D.part4, D.nbricks, 6, tot, ts, true);
+  sum_partials<6>(D.part4, D.nbricks * (CTA / 32), 6, tot, s, true);  // one record per warp
   if (threadIdx.x == 0)
     for (int q = 0; q < 6; ++q) D.ctl->stats[q] = tot[q];
 }

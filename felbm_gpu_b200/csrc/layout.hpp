@@ -22,6 +22,22 @@
 namespace fe {
 
 constexpr int AOSOA = 32;
+constexpr int HMAX = 3;  // deepest halo the per-brick tile tables cover
+
+// Per-brick record, built on the host. A kernel's tile with halo H <= HMAX
+// covers brick coordinates [-H, B + H) per axis; tile coordinate t maps to
+// table index t + HMAX - H. seg[a][.] names which distinct neighbour brick the
+// (periodically wrapped) coordinate falls in along axis a (at most 4, see
+// the host builder) and loc[a][.] the local coordinate inside it; nbr holds
+// the brick id of each segment combination sx + 4*(sy + 4*sz) (-1: no fluid).
+struct alignas(16) BrickRec {
+  int32_t nbr[64];
+  uint8_t seg[3][24];
+  uint8_t loc[3][24];
+  int32_t first, cnt;  // the brick's site range
+  int32_t pad[2];
+};
+static_assert(sizeof(BrickRec) % 16 == 0, "BrickRec is copied as int4");
 
 // Per-lattice control block in device memory. Written by the kernels' last
 // block and by small host copies; read by every CTA at start.
@@ -86,6 +102,7 @@ struct LatDesc {
   const uint64_t* mask;        // [nbricks][words]
   const int32_t* base;         // [nbricks][words]
   const int32_t* brick_xyz;    // [nbricks][3]
+  const BrickRec* rec;         // [nbricks]
   const int32_t* ref_of;       // site -> reference-order index
   // state: pop[buffer][0 = h, 1 = g]
   void* pop[2][2];
@@ -97,6 +114,7 @@ struct LatDesc {
   void* c_raw_bc;
   void* u_bc;                  // [3][n]
   const int32_t* bc_list;      // inlet sites, then outlet sites
+  const int32_t* bc_xyz;       // node coordinates of inlet, outlet, buffer sites [3 each]
   const double* bc_coord;      // inlet coordinate along the split axis
   int n_inlet, n_outlet, n_buf;
   const int32_t* buf_verts;

@@ -33,16 +33,19 @@ def test_fp64_100_steps(require_gpu, name):
 
 @pytest.mark.parametrize("name", CASES)
 def test_fp32_20_steps(require_gpu, name):
-    """The reference's single-precision validation criterion: ~1e-6 after 20
-    steps (scripts/validate.sh:12-14). Longer runs are bounded against the
-    reference's own FP32 kernels in test_gpu_ref_kernels.py."""
+    """The reference's single-precision validation criterion: max|d| ~1e-6 on
+    h and g after 20 steps (scripts/validate.sh:12-14; the metric is the
+    max|delta| that compare_cpu_gpu prints, src/compare_cpu_gpu.cu:57-79).
+    Longer runs are bounded against the reference's own FP32 kernels in
+    test_gpu_ref_kernels.py."""
     case = make_case(name)
     h, g, f, _, _ = run_engine(case, 20, "f32")
     ho, go, fo, _ = run_oracle(case, 20)
-    assert reldiff(h, ho) <= TOL32, reldiff(h, ho)
-    assert reldiff(g, go) <= TOL32, reldiff(g, go)
+    assert maxdiff(h, ho) <= TOL32, maxdiff(h, ho)
+    assert maxdiff(g, go) <= TOL32, maxdiff(g, go)
+    # macroscopic fields: the FP32 bound the workload states, max|dc| <= 1e-5
     for k in ("c", "rho", "p"):
-        assert reldiff(f[k], fo[k]) <= TOL32, (k, reldiff(f[k], fo[k]))
+        assert maxdiff(f[k], fo[k]) <= 1e-5, (k, maxdiff(f[k], fo[k]))
 
 
 @pytest.mark.parametrize("name", ["spheres_mrt", "grf_mrt_mass", "openbnd_bgk"])
