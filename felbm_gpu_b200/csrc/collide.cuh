@@ -1,5 +1,5 @@
 // P4: fused equilibria + Guo force + BGK/MRT collision of the Lee–Liu step,
-// pull-streamed (reference k_collide_fused_mrt, device_engine.cuh:547-651, and
+// push-streamed (reference k_collide_fused_mrt, device_engine.cuh:547-651, and
 // k_collide_fused_bgk, :459-545, with cd_dir_val / bd_dir_val / avg_dir_val,
 // :89-113, evaluated from shared-memory tiles, and the open-boundary overwrite
 // of g, k_open_bnd / k_open_bnd_buf, :761-798,826-846, folded in).
@@ -131,14 +131,17 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
     const R lmu = s_l[pos];
     q.mu = (R)fmu[i];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
-    // pulled g (identical to what P1 read)
+    // post-stream g of the site (what P1 read)
+    const int64_t a0 = pbase(i);
     R g[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - T::off(k)];
-      const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
-      g[k] = ld_pop<S>(gin, a, up >= 0 ? k : lat_opp(k), shg);
-    }
+    for (int k = 0; k < Q; ++k) g[k] = ld_pop<S>(gin, a0 + k * AOSOA, k, shg);
+    // push target of direction k: slot k of x + e_k, or slot opp(k) of x
+    // (halfway bounce-back) when x + e_k is solid
+    auto dst = [&](int k) -> int64_t {
+      const int dn = s_idx[pos + T::off(k)];
+      return dn >= 0 ? pidx(dn, k) : a0 + lat_opp(k) * AOSOA;
+    };
     // ---- pre-pass: near-wall cases once, the four gradients, stash -----------
     R ecx = 0, ecy = 0, ecz = 0, epx = 0, epy = 0, epz = 0;
     R bcx = 0, bcy = 0, bcz = 0, bpx = 0, bpy = 0, bpz = 0;
@@ -244,13 +247,13 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
     {  // rest direction: no derivatives, avg = lap(mu) of the site
       R h0, x0;
       dir_terms<R, MRT>(q, weight<R>(0), R(0), R(0), R(0), R(0), R(0), R(0), lmu, g[0], h0, x0, Z[0]);
-      st_pop<S>(hout, pidx(i, 0), 0, h0, shh);
+      st_pop<S>(hout, a0, 0, h0, shh);
       if (MRT) {
 #pragma unroll
         for (int j = 0; j < Q; ++j)
           if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) mom[j] += R(mrt_M(j, 0)) * x0;
       } else {
-        st_pop<S>(gout, pidx(i, 0), 0, Z[0] + s0 * x0, shg);
+        st_pop<S>(gout, a0, 0, Z[0] + s0 * x0, shg);
       }
     }
 #pragma unroll
@@ -268,8 +271,8 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
       R ha, hb, xa, xb;
       dir_terms<R, MRT>(q, w, uk, fproj, cdc, cdp, bca, bpa, avg_a, g[k], ha, xa, Z[k]);
       dir_terms<R, MRT>(q, w, -uk, -fproj, -cdc, -cdp, bcb, bpb, avg_b, g[k + 1], hb, xb, Z[k + 1]);
-      st_pop<S>(hout, pidx(i, k), k, ha, shh);
-      st_pop<S>(hout, pidx(i, k + 1), k + 1, hb, shh);
+      st_pop<S>(hout, dst(k), k, ha, shh);
+      st_pop<S>(hout, dst(k + 1), k + 1, hb, shh);
       if (MRT) {
         const R sx = xa + xb, dx = xa - xb;
 #pragma unroll
@@ -283,8 +286,8 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
           else if (mjk != 0) mom[j] += R(mjk) * vv;
         }
       } else {
-        st_pop<S>(gout, pidx(i, k), k, Z[k] + s0 * xa, shg);
-        st_pop<S>(gout, pidx(i, k + 1), k + 1, Z[k + 1] + s0 * xb, shg);
+        st_pop<S>(gout, dst(k), k, Z[k] + s0 * xa, shg);
+        st_pop<S>(gout, dst(k + 1), k + 1, Z[k + 1] + s0 * xb, shg);
       }
     }
     if (MRT) {
@@ -302,7 +305,7 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
 #pragma unroll
       for (int j = 0; j < Q; ++j)
         if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) back0 += R(mrt_M(j, 0)) * mom[j];
-      st_pop<S>(gout, pidx(i, 0), 0, Z[0] + back0, shg);
+      st_pop<S>(gout, a0, 0, Z[0] + back0, shg);
 #pragma unroll
       for (int k = 1; k < Q; k += 2) {
         R E = 0, O = 0;
@@ -316,8 +319,8 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
           else if (mjk == -1) acc -= mom[j];
           else if (mjk != 0) acc += R(mjk) * mom[j];
         }
-        st_pop<S>(gout, pidx(i, k), k, Z[k] + (E + O), shg);
-        st_pop<S>(gout, pidx(i, k + 1), k + 1, Z[k + 1] + (E - O), shg);
+        st_pop<S>(gout, dst(k), k, Z[k] + (E + O), shg);
+        st_pop<S>(gout, dst(k + 1), k + 1, Z[k + 1] + (E - O), shg);
       }
     }
   }

@@ -191,7 +191,8 @@ struct Engine {
   HostLayout L;
   LatDesc hd{};               // host copy of the descriptor
   LatDesc* d_desc = nullptr;
-  int2* d_work = nullptr;
+  int2* d_work = nullptr;   // (lattice, brick) of the stencil passes
+  int2* d_cwork = nullptr;  // (lattice, chunk) of the flat passes
   Ctl* d_ctl = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
@@ -300,6 +301,7 @@ struct Engine {
     D.words = L.words;
     D.nbricks = nbk;
     D.n = L.n;
+    D.nchunks = (int)((L.n + CHUNK - 1) / CHUNK);
     D.n_pad = (L.n + AOSOA - 1) / AOSOA * AOSOA;
     int32_t *bg, *bs, *bx, *rf;
     uint64_t* mk;
@@ -326,10 +328,10 @@ struct Engine {
       FE_CUDA(cudaMemset(q, 0, (size_t)D.n * fld_size()));
       *f = q;
     }
-    if ((rc = alloc(&D.part1, (size_t)nbk * 2))) return rc;
+    if ((rc = alloc(&D.part1, (size_t)D.nchunks * 2))) return rc;
     if ((rc = alloc(&D.part4, (size_t)nbk * WARPS * 6))) return rc;
     FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * WARPS * 6 * 8));
-    if ((rc = alloc(&d_partm, (size_t)nbk * 2))) return rc;
+    if ((rc = alloc(&d_partm, (size_t)D.nchunks * 2))) return rc;
     if ((rc = alloc(&d_ctl, 1))) return rc;
     Ctl c0{};
     c0.ff_manual = 1.0;
@@ -340,6 +342,9 @@ struct Engine {
     std::vector<int2> work(nbk);
     for (int b = 0; b < nbk; ++b) work[b] = make_int2(0, b);
     if ((rc = upload_vec(&d_work, work))) return rc;
+    std::vector<int2> cwork(D.nchunks);
+    for (int b = 0; b < D.nchunks; ++b) cwork[b] = make_int2(0, b);
+    if ((rc = upload_vec(&d_cwork, cwork))) return rc;
     FE_DISPATCH(*this, rc = set_attrs<S FE_COMMA Sh>());
     if (rc) return rc;
     FE_CUDA(cudaMallocHost(&h_stats, 6 * sizeof(double)));
@@ -374,7 +379,7 @@ struct Engine {
     const int nb = hd.nbricks;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
     rec(0);
-    k_moments<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work, par, need_j() ? 1 : 0);
+    k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, need_j() ? 1 : 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
     rec(2);
@@ -487,7 +492,7 @@ struct Engine {
   }
 
   int mass_pass() {
-    FE_DISPATCH(*this, (k_mass<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, d_partm)));
+    FE_DISPATCH(*this, (k_mass<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_partm)));
     ++launches;
     FE_CUDA(cudaGetLastError());
     return FE_OK;
@@ -515,7 +520,7 @@ struct Engine {
       if ((rc = mass_pass())) return rc;
       apply = 1;
     }
-    FE_DISPATCH(*this, (k_download_state<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, d_tmp,
+    FE_DISPATCH(*this, (k_download_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
                                                                                   d_tmp + Vn, apply)));
     ++launches;
     FE_CUDA(cudaGetLastError());
@@ -531,7 +536,7 @@ struct Engine {
     if ((rc = ensure_tmp(2 * Vn))) return rc;
     FE_CUDA(cudaMemcpyAsync(d_tmp, h, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
     FE_CUDA(cudaMemcpyAsync(d_tmp + Vn, g, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
-    FE_DISPATCH(*this, (k_upload_state<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, d_tmp,
+    FE_DISPATCH(*this, (k_upload_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
                                                                                 d_tmp + Vn)));
     ++launches;
     FE_CUDA(cudaGetLastError());
@@ -544,7 +549,7 @@ struct Engine {
   // download()/download_raw(): P1 (+BC) and P2 in output mode, no step.
   template <class S, class Sh>
   void fields_launch(FieldOut o) {
-    k_moments<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, 1);
+    k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
     k_cfield<S, Sh, 1><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     launches += 2;

@@ -3,27 +3,29 @@
 // One step is four brick-parallel passes, separated by the grid-wide
 // dependencies of the scheme (reference MultiPhaseGPU::step,
 // multiphase_gpu.cuh:522-631):
-//   P1 k_moments  pull-stream h,g (19+19 loads), write c, p, j; M,W partials
+//   P1 k_moments  own-site h,g (19+19 loads), write c, p, j; M,W partials
 //                 of the order-parameter mass (and, last block, lambda)
 //   P2 k_cfield   c stencil (grad_cd, Laplacian + wetting BC) -> mu, p
 //                 (velocity/pressure correction)
 //   P3 k_lapmu    mu stencil -> Laplacian of mu
-//   P4 k_collide  c, p stencils to distance 2, lap(mu) to distance 1, pull g:
-//                 equilibria + Guo force + BGK/MRT relaxation, write h, g
-// Every CTA owns one brick. Its prologue reads the brick's precomputed record
-// (neighbour-brick ids and per-axis tile tables, built on the host) and the
-// occupancy words of the neighbour bricks into shared memory; from those it
-// resolves the site index of every tile position (brick + halo) without
-// further global traffic, stages the stencil fields into shared-memory tiles
-// (solid positions hold NaN, so one load gives value and occupancy), then runs
-// one thread per fluid site of the brick. All stencil case logic (central /
-// one-sided / biased, halfway bounce-back, wetting) is derived from tile
-// occupancy with selects, so no per-site tables are read from HBM.
+//   P4 k_collide  c, p stencils to distance 2, lap(mu) to distance 1, own g:
+//                 equilibria + Guo force + BGK/MRT relaxation, push h, g
+// The stencil passes (P2, P3, P4) run one CTA per brick. Its prologue reads
+// the brick's precomputed record (neighbour-brick ids and per-axis tile
+// tables, built on the host) and the occupancy words of the neighbour bricks
+// into shared memory; from those it resolves the site index of every tile
+// position (brick + halo) without further global traffic, stages the stencil
+// fields into shared-memory tiles (solid positions hold NaN, so one load gives
+// value and occupancy), then runs one thread per fluid site of the brick. All
+// stencil case logic (central / one-sided / biased, halfway bounce-back,
+// wetting) is derived from tile occupancy with selects, so no per-site tables
+// are read from HBM. P1 and the state transfers touch only a site's own
+// populations and run over flat chunks of CHUNK sites.
 //
-// Streaming is pull, fused into P1 and P4: the post-collision value f*_k at
-// x - e_k moves to site x, or f*_opp(k)(x) when x - e_k is solid (halfway
-// bounce-back). The state between steps is therefore post-collision; uploads
-// and downloads apply the (bijective) pull permutation.
+// Streaming is push, fused into P4: the post-collision value f*_k of site x
+// is written to slot k of x + e_k, or to slot opp(k) of x itself when x + e_k
+// is solid (halfway bounce-back). The state between steps is therefore the
+// post-stream state of the reference, and P1 reads it coalesced.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -269,9 +271,17 @@ __device__ __forceinline__ void load_step_scalars(const LatDesc& D, Pro<Sh>& s) 
   }
 }
 
+// Shared state of the reductions of the flat (chunk) kernels; Pro<Sh> has the
+// same two members.
+struct Red {
+  double red[CTA / 32][6];
+  int last;
+};
+
 // Block reduction of NV doubles into thread 0 (the last one as a max when mx).
-template <int NV, class Sh>
-__device__ __forceinline__ void block_sum(double (&v)[NV], Pro<Sh>& s, bool mx_last = false) {
+// SMem is Pro<Sh> or Red.
+template <int NV, class SMem>
+__device__ __forceinline__ void block_sum(double (&v)[NV], SMem& s, bool mx_last = false) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
@@ -300,8 +310,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], Pro<Sh>& s, bool mx_l
 
 // Deterministic sum over `count` partial records (fixed strided subsets, then
 // a fixed tree), result in thread 0.
-template <int NV, class Sh>
-__device__ void sum_partials(const double* __restrict__ part, int count, int stride, double (&out)[NV], Pro<Sh>& s,
+template <int NV, class SMem>
+__device__ void sum_partials(const double* __restrict__ part, int count, int stride, double (&out)[NV], SMem& s,
                              bool mx_last = false) {
   double acc[NV];
 #pragma unroll
@@ -319,8 +329,8 @@ __device__ void sum_partials(const double* __restrict__ part, int count, int str
 }
 
 // True in every thread of the block that finished last (per lattice).
-template <class Sh>
-__device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int total, Pro<Sh>& s) {
+template <class SMem>
+__device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int total, SMem& s) {
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) s.last = (atomicAdd(counter, 1u) == total - 1) ? 1 : 0;
@@ -342,26 +352,27 @@ __device__ __forceinline__ void finish_mass(Ctl* C, double M, double Wt) {
 }
 
 // ---------------------------------------------------------------------------
-// P1: pull streaming + moments (reference k_moments, device_engine.cuh:116-135,
-// with the previous step's k_stream_gather, :882-889, fused in as a pull, and
-// k_mass_weight, :1109-1126, fused as block partials + last-block lambda).
+// P1: moments of the post-stream state (reference k_moments,
+// device_engine.cuh:116-135, with k_mass_weight, :1109-1126, fused as chunk
+// partials + last-block lambda). One CTA per chunk of CHUNK sites; a site's 38
+// populations sit at one AoSoA base with constant offsets, so each warp reads
+// 38 full 128-byte lines (FP32) and issues them back to back.
 // ---------------------------------------------------------------------------
-template <class S, class Sh>
+constexpr int CHUNK = 2 * CTA;
+
+// AoSoA index of (site i, direction 0); direction k adds k * AOSOA.
+__device__ __forceinline__ int64_t pbase(int64_t i) { return (i >> 5) * (int64_t)(Q * AOSOA) + (i & (AOSOA - 1)); }
+
+template <class S>
 __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                   int parity, int write_j) {
   using R = typename S::real;
   using P = typename S::pop;
   using F = typename S::fld;
-  using T = Tile<Sh, 1>;
-  __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 1> it;
+  __shared__ Red s;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  const int brick = wk.y;
-  prologue<Sh>(D, brick, s);
-  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
-  const int32_t* s_idx = it.idx;
-  __syncthreads();
+  const int chunk = wk.y;
   const P* __restrict__ hin = static_cast<const P*>(D.pop[parity][0]);
   const P* __restrict__ gin = static_cast<const P*>(D.pop[parity][1]);
   F* __restrict__ fc = static_cast<F*>(D.c);
@@ -372,25 +383,26 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   double acc[2] = {0.0, 0.0};
-  const int first = s.rec.first, cnt = s.rec.cnt;
-  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
-    const int64_t i = first + r;
-    const int pos = T::pos(s.slot_of[r]);
+  const int64_t i0 = (int64_t)chunk * CHUNK;
+  const int64_t iend = i0 + CHUNK < D.n ? i0 + CHUNK : D.n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
+    const int64_t a = pbase(i);
+    R hv[Q], gv[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      hv[k] = ld_pop<S>(hin, a + k * AOSOA, k, shh);
+      gv[k] = ld_pop<S>(gin, a + k * AOSOA, k, shg);
+    }
     R c = 0, p = 0, jx = 0, jy = 0, jz = 0;
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - T::off(k)];
-      const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
-      const int kk = up >= 0 ? k : lat_opp(k);
-      const R hv = ld_pop<S>(hin, a, kk, shh);
-      const R gv = ld_pop<S>(gin, a, kk, shg);
-      c += hv;
-      cd += (double)hv;
-      p += gv;
-      if (lat_cx(k)) jx += R(lat_cx(k)) * gv;
-      if (lat_cy(k)) jy += R(lat_cy(k)) * gv;
-      if (lat_cz(k)) jz += R(lat_cz(k)) * gv;
+      c += hv[k];
+      cd += (double)hv[k];
+      p += gv[k];
+      if (lat_cx(k)) jx += R(lat_cx(k)) * gv[k];
+      if (lat_cy(k)) jy += R(lat_cy(k)) * gv[k];
+      if (lat_cz(k)) jz += R(lat_cz(k)) * gv[k];
     }
     fc[i] = (F)c;
     fp[i] = (F)p;
@@ -407,12 +419,12 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   if (!D.prm.correct_mass) return;
   block_sum<2>(acc, s);
   if (threadIdx.x == 0) {
-    D.part1[(int64_t)brick * 2 + 0] = acc[0];
-    D.part1[(int64_t)brick * 2 + 1] = acc[1];
+    D.part1[(int64_t)chunk * 2 + 0] = acc[0];
+    D.part1[(int64_t)chunk * 2 + 1] = acc[1];
   }
-  if (!last_block(&D.ctl->count1, (unsigned)D.nbricks, s)) return;
+  if (!last_block(&D.ctl->count1, (unsigned)D.nchunks, s)) return;
   double tot[2];
-  sum_partials<2>(D.part1, D.nbricks, 2, tot, s);
+  sum_partials<2>(D.part1, D.nchunks, 2, tot, s);
   if (threadIdx.x == 0) {
     finish_mass(D.ctl, tot[0], tot[1]);
     D.ctl->count1 = 0;
@@ -767,41 +779,30 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
 // ---------------------------------------------------------------------------
 // Post-stream state in the reference layout f[k*n + ref(i)] (double), with a
 // queued mass correction injected as the reference's k_inject_mass does.
-template <class S, class Sh>
+template <class S>
 __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                          int parity, double* __restrict__ h_out,
                                                          double* __restrict__ g_out, int apply_lambda) {
   using R = typename S::real;
   using P = typename S::pop;
-  using T = Tile<Sh, 1>;
-  __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 1> it;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  prologue<Sh>(D, wk.y, s);
-  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
-  const int32_t* s_idx = it.idx;
-  __syncthreads();
   const P* hin = static_cast<const P*>(D.pop[parity][0]);
   const P* gin = static_cast<const P*>(D.pop[parity][1]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   const double lambda = apply_lambda ? D.ctl->lambda : 0.0;
-  const int64_t n = D.n;
-  for (int r = threadIdx.x; r < s.rec.cnt; r += blockDim.x) {
-    const int64_t i = s.rec.first + r;
-    const int pos = T::pos(s.slot_of[r]);
-    const int64_t q = D.ref_of[i];
+  const int64_t n = D.n, i0 = (int64_t)wk.y * CHUNK;
+  const int64_t iend = i0 + CHUNK < n ? i0 + CHUNK : n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
+    const int64_t a = pbase(i), q = D.ref_of[i];
     R hv[Q];
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - T::off(k)];
-      const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
-      const int kk = up >= 0 ? k : lat_opp(k);
-      hv[k] = ld_pop<S>(hin, a, kk, shh);
+      hv[k] = ld_pop<S>(hin, a + k * AOSOA, k, shh);
       cd += (double)hv[k];
-      g_out[k * n + q] = (double)ld_pop<S>(gin, a, kk, shg);
+      g_out[k * n + q] = (double)ld_pop<S>(gin, a + k * AOSOA, k, shg);
     }
     const double phi = cd * (1.0 - cd);
     const bool inj = lambda != 0.0 && phi > 0.0;
@@ -814,38 +815,27 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
   }
 }
 
-// Inverse of the pull: place post-stream values so that the next P1 pulls
-// them back (reference upload_state, multiphase_gpu.cuh:354-359).
-template <class S, class Sh>
+// Post-stream state from the reference layout (reference upload_state,
+// multiphase_gpu.cuh:354-359).
+template <class S>
 __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                        int parity, const double* __restrict__ h_in,
                                                        const double* __restrict__ g_in) {
   using P = typename S::pop;
-  using T = Tile<Sh, 1>;
-  __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 1> it;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  prologue<Sh>(D, wk.y, s);
-  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
-  const int32_t* s_idx = it.idx;
-  __syncthreads();
   P* hb = static_cast<P*>(D.pop[parity][0]);
   P* gb = static_cast<P*>(D.pop[parity][1]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
-  const int64_t n = D.n;
-  for (int r = threadIdx.x; r < s.rec.cnt; r += blockDim.x) {
-    const int64_t i = s.rec.first + r;
-    const int pos = T::pos(s.slot_of[r]);
-    const int64_t q = D.ref_of[i];
+  const int64_t n = D.n, i0 = (int64_t)wk.y * CHUNK;
+  const int64_t iend = i0 + CHUNK < n ? i0 + CHUNK : n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
+    const int64_t a = pbase(i), q = D.ref_of[i];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - T::off(k)];
-      const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
-      const int kk = up >= 0 ? k : lat_opp(k);
-      st_pop<S>(hb, a, kk, (typename S::real)h_in[k * n + q], shh);
-      st_pop<S>(gb, a, kk, (typename S::real)g_in[k * n + q], shg);
+      st_pop<S>(hb, a + k * AOSOA, k, (typename S::real)h_in[k * n + q], shh);
+      st_pop<S>(gb, a + k * AOSOA, k, (typename S::real)g_in[k * n + q], shg);
     }
   }
 }
@@ -853,33 +843,24 @@ __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict_
 // M = sum c, W = sum c(1-c)^+ of the post-stream state (reference
 // k_mass_weight :1109-1126) into ctl->M, ctl->W, and the lambda of a queued
 // correction as P1 forms it.
-template <class S, class Sh>
+template <class S>
 __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                int parity, double* __restrict__ part) {
   using P = typename S::pop;
-  using T = Tile<Sh, 1>;
-  __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 1> it;
+  __shared__ Red s;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  const int brick = wk.y;
-  prologue<Sh>(D, brick, s);
-  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
-  const int32_t* s_idx = it.idx;
-  __syncthreads();
+  const int chunk = wk.y;
   const P* hin = static_cast<const P*>(D.pop[parity][0]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   double acc[2] = {0.0, 0.0};
-  for (int r = threadIdx.x; r < s.rec.cnt; r += blockDim.x) {
-    const int64_t i = s.rec.first + r;
-    const int pos = T::pos(s.slot_of[r]);
+  const int64_t i0 = (int64_t)chunk * CHUNK;
+  const int64_t iend = i0 + CHUNK < D.n ? i0 + CHUNK : D.n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
+    const int64_t a = pbase(i);
     double cd = 0.0;
 #pragma unroll
-    for (int k = 0; k < Q; ++k) {
-      const int up = s_idx[pos - T::off(k)];
-      const int64_t a = up >= 0 ? pidx(up, k) : pidx(i, lat_opp(k));
-      cd += (double)ld_pop<S>(hin, a, up >= 0 ? k : lat_opp(k), shh);
-    }
+    for (int k = 0; k < Q; ++k) cd += (double)ld_pop<S>(hin, a + k * AOSOA, k, shh);
     double phi = cd * (1.0 - cd);
     if (phi < 0.0) phi = 0.0;
     acc[0] += cd;
@@ -887,12 +868,12 @@ __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs,
   }
   block_sum<2>(acc, s);
   if (threadIdx.x == 0) {
-    part[(int64_t)brick * 2 + 0] = acc[0];
-    part[(int64_t)brick * 2 + 1] = acc[1];
+    part[(int64_t)chunk * 2 + 0] = acc[0];
+    part[(int64_t)chunk * 2 + 1] = acc[1];
   }
-  if (!last_block(&D.ctl->countm, (unsigned)D.nbricks, s)) return;
+  if (!last_block(&D.ctl->countm, (unsigned)D.nchunks, s)) return;
   double tot[2];
-  sum_partials<2>(part, D.nbricks, 2, tot, s);
+  sum_partials<2>(part, D.nchunks, 2, tot, s);
   if (threadIdx.x == 0) {
     finish_mass(D.ctl, tot[0], tot[1]);
     D.ctl->countm = 0;
@@ -902,7 +883,7 @@ __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs,
 // Sum the flow-statistics partials of the last collision pass into ctl->stats.
 template <class Sh>
 __global__ void __launch_bounds__(CTA) k_stats_finalize(const LatDesc* __restrict__ descs, int lat) {
-  __shared__ Pro<Sh> s;
+  __shared__ Red s;
   const LatDesc& D = descs[lat];
   double tot[6];
   sum_partials<6>(D.part4, D.nbricks * (CTA / 32), 6, tot, s, true);  // one record per warp

@@ -96,6 +96,7 @@ struct LatDesc {
   int nbx, nby, nbz;     // brick grid
   int words;             // 64-bit occupancy words per brick
   int nbricks;
+  int nchunks;           // flat chunks of CHUNK sites (P1, transfers)
   int64_t n;             // sites
   int64_t n_pad;         // rounded up to AOSOA
   const int32_t* brick_grid;   // [nbz][nby][nbx] -> brick or -1
@@ -120,7 +121,7 @@ struct LatDesc {
   const int32_t* buf_verts;
   const int32_t* buf_refs;
   // reductions
-  double* part1;               // [nbricks][2] M, W partials of the moment pass
+  double* part1;               // [nchunks][2] M, W partials of the moment pass
   double* part4;               // [nbricks][6] flow-statistics partials
   Ctl* ctl;
   DevPrm prm;
