@@ -100,9 +100,12 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
   __syncthreads();
   build_idx_tile<Sh, 2>(s, s_idx, s_rbits, s_rbase);
   __syncthreads();
-  stage<Sh, 2>(s, static_cast<const F*>(D.c), s_c, true, s.lambda, s_idx);
-  stage<Sh, 2>(s, static_cast<const F*>(D.p), s_p, false, 0.0, s_idx);
-  stage<Sh, 2>(s, static_cast<const F*>(D.lapmu), s_l, false, 0.0, s_idx);
+  {
+    const F* const src[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
+                             static_cast<const F*>(D.lapmu)};
+    R* const dst[3] = {s_c, s_p, s_l};
+    stage<Sh, 2, 3>(src, dst, true, s.lambda, s_idx);
+  }
   __syncthreads();
 
   const DevPrm& Pm = D.prm;
@@ -122,7 +125,7 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
   int bad = 0;
   const int first = s.rec.first, cnt = s.rec.cnt;
 
-  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+  for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int64_t i = first + r;
     const int pos = T::pos(s.slot_of[r]);
     SiteScal<R> q;

@@ -172,7 +172,7 @@ __device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s
     if (tid < N4) dst[tid] = __ldg(src + tid);
   }
   __syncthreads();
-  for (int q = tid; q < 64 * Sh::W; q += blockDim.x) {
+  for (int q = tid; q < 64 * Sh::W; q += CTA) {
     const int slot = q / Sh::W, w = q - slot * Sh::W;
     const int id = s.rec.nbr[slot];
     if (id >= 0) {
@@ -182,26 +182,11 @@ __device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s
   }
   __syncthreads();
   const int own = s.rec.seg[0][HMAX] + 4 * (s.rec.seg[1][HMAX] + 4 * s.rec.seg[2][Sh::HZ ? HMAX : 0]);
-  for (int q = tid; q < Sh::C; q += blockDim.x) {
+  for (int q = tid; q < Sh::C; q += CTA) {
     const int w = q >> 6, b = q & 63;
     const uint64_t m = s.nmask[own][w];
     if ((m >> b) & 1ull) s.slot_of[s.nbase[own][w] - s.rec.first + __popcll(m & ((1ull << b) - 1ull))] = (uint16_t)q;
   }
-}
-
-// Site index of tile position t (halo H), -1 when solid.
-template <class Sh, int H>
-__device__ __forceinline__ int tile_site(const Pro<Sh>& s, int t) {
-  using T = Tile<Sh, H>;
-  const int tx = t % T::TX, r = t / T::TX, ty = r % T::TY, tz = r / T::TY;
-  const int ax = tx + (HMAX - H), ay = ty + (HMAX - H), az = Sh::HZ ? tz + (HMAX - H) : 0;
-  const int seg = s.rec.seg[0][ax] + 4 * (s.rec.seg[1][ay] + 4 * s.rec.seg[2][az]);
-  if (s.rec.nbr[seg] < 0) return -1;
-  const int slot = s.rec.loc[0][ax] | (s.rec.loc[1][ay] << Sh::LBX) | (s.rec.loc[2][az] << (Sh::LBX + Sh::LBY));
-  const int w = slot >> 6, b = slot & 63;
-  const uint64_t m = s.nmask[seg][w];
-  if (!((m >> b) & 1ull)) return -1;
-  return s.nbase[seg][w] + __popcll(m & ((1ull << b) - 1ull));
 }
 
 // Site indices of a whole halo-H tile, built row by row: for each (y, z) row
@@ -212,7 +197,7 @@ __device__ __forceinline__ void build_idx_tile(const Pro<Sh>& s, int32_t* __rest
                                                uint32_t* __restrict__ s_rbits, int32_t* __restrict__ s_rbase) {
   using T = Tile<Sh, H>;
   constexpr int ROWS = T::TY * T::TZ;
-  for (int q = threadIdx.x; q < ROWS * 4; q += blockDim.x) {
+  for (int q = threadIdx.x; q < ROWS * 4; q += CTA) {
     const int row = q >> 2, sx = q & 3;
     const int ty = row % T::TY, tz = row / T::TY;
     const int ay = ty + (HMAX - H), az = Sh::HZ ? tz + (HMAX - H) : 0;
@@ -230,7 +215,7 @@ __device__ __forceinline__ void build_idx_tile(const Pro<Sh>& s, int32_t* __rest
     s_rbase[q] = base;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < T::N; t += blockDim.x) {
+  for (int t = threadIdx.x; t < T::N; t += CTA) {
     const int row = t / T::TX, tx = t - row * T::TX;
     const int ax = tx + (HMAX - H);
     const int q = row * 4 + s.rec.seg[0][ax];
@@ -296,7 +281,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], SMem& s, bool mx_last
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const int nw = blockDim.x >> 5;
+    const int nw = CTA / 32;
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double x = s.red[0][q];
@@ -316,7 +301,7 @@ __device__ void sum_partials(const double* __restrict__ part, int count, int str
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-  for (int r = threadIdx.x; r < count; r += blockDim.x) {
+  for (int r = threadIdx.x; r < count; r += CTA) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       const double x = __ldcg(&part[(int64_t)r * stride + q]);
@@ -443,20 +428,41 @@ __device__ __forceinline__ R corr_c(R c, double lambda) {
   return phi > 0.0 ? (R)(cd - lambda * phi) : c;
 }
 
-// Stage a field over tile positions [t0, N) of halo H (NaN at solid positions);
-// optionally only the positions within distance `reach` of the brick.
-template <class Sh, int H, class R, class F>
-__device__ __forceinline__ void stage(const Pro<Sh>& s, const F* __restrict__ f, R* __restrict__ tile, bool correct,
-                                      double lambda, const int32_t* s_idx) {
+// Stage NF fields into halo-H tiles (NaN at solid positions); field 0 is the
+// order parameter when `correct` (corrected on the fly). Every thread first
+// reads the site indices of all its positions, then issues all its gathers
+// before the first use, so a CTA waits for one round of L2/HBM latency instead
+// of one per position. The fields are read-only for the kernel (__ldg).
+template <class Sh, int H, int NF, class R, class F>
+__device__ __forceinline__ void stage(const F* const (&src)[NF], R* const (&dst)[NF], bool correct, double lambda,
+                                      const int32_t* __restrict__ s_idx) {
   using T = Tile<Sh, H>;
-  for (int t = threadIdx.x; t < T::N; t += blockDim.x) {
-    const int j = s_idx ? s_idx[t] : tile_site<Sh, H>(s, t);
-    R v = nan_v<R>();
-    if (j >= 0) {
-      v = (R)f[j];
-      if (correct) v = corr_c<R>(v, lambda);
+  constexpr int PER = (T::N + CTA - 1) / CTA;
+  int j[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int t = threadIdx.x + u * CTA;
+    j[u] = (t < T::N) ? s_idx[t] : -1;
+  }
+  F v[PER][NF];
+#pragma unroll
+  for (int u = 0; u < PER; ++u)
+#pragma unroll
+    for (int f = 0; f < NF; ++f) v[u][f] = j[u] >= 0 ? __ldg(src[f] + j[u]) : F(0);
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int t = threadIdx.x + u * CTA;
+    if (t < T::N) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        R x = nan_v<R>();
+        if (j[u] >= 0) {
+          x = (R)v[u][f];
+          if (f == 0 && correct) x = corr_c<R>(x, lambda);
+        }
+        dst[f][t] = x;
+      }
     }
-    tile[t] = v;
   }
 }
 
@@ -517,7 +523,11 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   prologue<Sh>(D, wk.y, s);
   load_step_scalars<Sh>(D, s);
   build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
-  stage<Sh, 1>(s, static_cast<const F*>(D.c), s_c, true, s.lambda, it.idx);
+  {
+    const F* const src[1] = {static_cast<const F*>(D.c)};
+    R* const dst[1] = {s_c};
+    stage<Sh, 1, 1>(src, dst, true, s.lambda, it.idx);
+  }
   __syncthreads();
   const DevPrm& Pm = D.prm;
   const R alpha = R(ALPHA), cs2 = R(CS2);
@@ -530,7 +540,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   F* __restrict__ fp = static_cast<F*>(D.p);
   F* __restrict__ fmu = static_cast<F*>(D.mu);
   const int first = s.rec.first, cnt = s.rec.cnt;
-  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+  for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int64_t i = first + r;
     const int pos = T::pos(s.slot_of[r]);
     const R c0 = s_c[pos];
@@ -604,13 +614,17 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
   const LatDesc& D = descs[wk.x];
   prologue<Sh>(D, wk.y, s);
   build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
-  stage<Sh, 1>(s, static_cast<const F*>(D.mu), s_m, false, 0.0, it.idx);
+  {
+    const F* const src[1] = {static_cast<const F*>(D.mu)};
+    R* const dst[1] = {s_m};
+    stage<Sh, 1, 1>(src, dst, false, 0.0, it.idx);
+  }
   __syncthreads();
   const bool hbb = D.prm.hbb != 0;
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
   const int first = s.rec.first, cnt = s.rec.cnt;
-  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+  for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int pos = T::pos(s.slot_of[r]);
     const R m0 = s_m[pos];
     R lap = 0;
