@@ -22,14 +22,13 @@
 
 namespace fe {
 
-// Two resident CTAs per SM for FP32 arithmetic (<= 128 registers); FP64 needs
-// the full register budget.
+// Resident CTAs per SM: FP32 arithmetic fits 128 registers a thread, FP64
+// needs the full budget of 255.
 template <class S>
 struct CollideMinBlocks {
-  static constexpr int value = sizeof(typename S::real) == 8 ? 1 : 2;
+  static constexpr int value = 65536 / ((sizeof(typename S::real) == 8 ? 256 : 128) * P4T);
 };
 
-constexpr int WARPS = CTA / 32;
 constexpr int NPAIR = (Q - 1) / 2;   // 9 opposite pairs
 constexpr int NSTASH = 6 * NPAIR;    // stashed values per thread
 
@@ -40,7 +39,7 @@ struct CollideSmem {
   using T = Tile<Sh, 2>;
   static constexpr int NT16 = (T::N * 4 + 15) & ~15;
   static constexpr int NTR = (T::N * (int)sizeof(R) + 15) & ~15;
-  static constexpr int STASH = NSTASH * CTA * (int)sizeof(R);
+  static constexpr int STASH = NSTASH * P4T * (int)sizeof(R);
   static constexpr int BYTES = NT16 + 3 * NTR + STASH;
 };
 
@@ -75,7 +74,7 @@ __device__ __forceinline__ void dir_terms(const SiteScal<R>& q, R w, R uk, R fpr
 }
 
 template <class S, class Sh, int MRT>
-__global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
+__global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
   using R = typename S::real;
   using P = typename S::pop;
@@ -91,20 +90,19 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
   R* s_c = reinterpret_cast<R*>(dsm + SM::NT16);
   R* s_p = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTR);
   R* s_l = reinterpret_cast<R*>(dsm + SM::NT16 + 2 * SM::NTR);
-  R* s_st = reinterpret_cast<R*>(dsm + SM::NT16 + 3 * SM::NTR) + threadIdx.x;  // [v * CTA]
+  R* s_st = reinterpret_cast<R*>(dsm + SM::NT16 + 3 * SM::NTR) + threadIdx.x;  // [v * P4T]
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
-  prologue<Sh>(D, brick, s);
-  load_step_scalars<Sh>(D, s);
-  __syncthreads();
-  build_idx_tile<Sh, 2>(s, s_idx, s_rbits, s_rbase);
-  __syncthreads();
+  // the prologue's barriers publish the record and masks that the index
+  // tile reads; the tile builder ends with a barrier
+  prologue<Sh, P4T>(D, brick, s);
+  build_idx_tile<Sh, 2, P4T>(s, s_idx, s_rbits, s_rbase);
   {
     const F* const src[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
                              static_cast<const F*>(D.lapmu)};
     R* const dst[3] = {s_c, s_p, s_l};
-    stage<Sh, 2, 3>(src, dst, true, s.lambda, s_idx);
+    stage<Sh, 2, 3, P4T>(src, dst, true, s.lambda, s_idx);
   }
   __syncthreads();
 
@@ -125,7 +123,7 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
   int bad = 0;
   const int first = s.rec.first, cnt = s.rec.cnt;
 
-  for (int r = threadIdx.x; r < cnt; r += CTA) {
+  for (int r = threadIdx.x; r < cnt; r += P4T) {
     const int64_t i = first + r;
     const int pos = T::pos(s.slot_of[r]);
     SiteScal<R> q;
@@ -156,12 +154,12 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
       const R cdc = cd_val(q.c, cm, cp, hbb), cdp = cd_val(q.p, pm, pp, hbb);
       const R bca = bd_val(q.c, cm, cp, cm2, cp2, hbb), bcb = bd_val(q.c, cp, cm, cp2, cm2, hbb);
       const R bpa = bd_val(q.p, pm, pp, pm2, pp2, hbb), bpb = bd_val(q.p, pp, pm, pp2, pm2, hbb);
-      s_st[(v + 0) * CTA] = cdc;
-      s_st[(v + 1) * CTA] = cdp;
-      s_st[(v + 2) * CTA] = bca;
-      s_st[(v + 3) * CTA] = bcb;
-      s_st[(v + 4) * CTA] = bpa;
-      s_st[(v + 5) * CTA] = bpb;
+      s_st[(v + 0) * P4T] = cdc;
+      s_st[(v + 1) * P4T] = cdp;
+      s_st[(v + 2) * P4T] = bca;
+      s_st[(v + 3) * P4T] = bcb;
+      s_st[(v + 4) * P4T] = bpa;
+      s_st[(v + 5) * P4T] = bpb;
       // pairs: central terms count twice, biased ones as a difference
       const R aw = alpha * weight<R>(k);
       const R dbc = bca - bcb, dbp = bpa - bpb;
@@ -262,9 +260,9 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
       const int o = T::off(k), v = 6 * (k >> 1);
-      const R cdc = s_st[(v + 0) * CTA], cdp = s_st[(v + 1) * CTA];
-      const R bca = s_st[(v + 2) * CTA], bcb = s_st[(v + 3) * CTA];
-      const R bpa = s_st[(v + 4) * CTA], bpb = s_st[(v + 5) * CTA];
+      const R cdc = s_st[(v + 0) * P4T], cdp = s_st[(v + 1) * P4T];
+      const R bca = s_st[(v + 2) * P4T], bcb = s_st[(v + 3) * P4T];
+      const R bpa = s_st[(v + 4) * P4T], bpb = s_st[(v + 5) * P4T];
       const R lm = s_l[pos - o], lp = s_l[pos + o];
       const R avg_a = is_site(lp) ? R(0.5) * (lmu + lp) : lmu;
       const R avg_b = is_site(lm) ? R(0.5) * (lmu + lm) : lmu;
@@ -342,14 +340,14 @@ __global__ void __launch_bounds__(CTA, CollideMinBlocks<S>::value)
   }
   bad = __any_sync(0xffffffffu, bad);
   if (lane == 0) {
-    double* part = D.part4 + ((int64_t)brick * WARPS + wid) * 6;
+    double* part = D.part4 + ((int64_t)brick * P4W + wid) * 6;
 #pragma unroll
     for (int qv = 0; qv < 6; ++qv) part[qv] = st[qv];
     if (bad) atomicOr(&D.ctl->status, 1);
     __threadfence();
     // the last warp of the launch (per lattice) advances the step counter and
     // queues the next mass correction
-    if (atomicAdd(&D.ctl->count4, 1u) == (unsigned)(D.nbricks * WARPS) - 1u) {
+    if (atomicAdd(&D.ctl->count4, 1u) == (unsigned)(D.nbricks * P4W) - 1u) {
       Ctl* C = D.ctl;
       C->t += 1;
       if (Pm.open_bnd) C->open_step += 1;

@@ -329,8 +329,8 @@ struct Engine {
       *f = q;
     }
     if ((rc = alloc(&D.part1, (size_t)D.nchunks * 2))) return rc;
-    if ((rc = alloc(&D.part4, (size_t)nbk * WARPS * 6))) return rc;
-    FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * WARPS * 6 * 8));
+    if ((rc = alloc(&D.part4, (size_t)nbk * P4W * 6))) return rc;
+    FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * P4W * 6 * 8));
     if ((rc = alloc(&d_partm, (size_t)D.nchunks * 2))) return rc;
     if ((rc = alloc(&d_ctl, 1))) return rc;
     Ctl c0{};
@@ -387,8 +387,8 @@ struct Engine {
     rec(3);
     k_lapmu<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work);
     rec(4);
-    if (hd.prm.use_mrt) k_collide<S, Sh, 1><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
-    else k_collide<S, Sh, 0><<<nb, CTA, smem_p4, st>>>(d_desc, d_work, par);
+    if (hd.prm.use_mrt) k_collide<S, Sh, 1><<<nb, P4T, smem_p4, st>>>(d_desc, d_work, par);
+    else k_collide<S, Sh, 0><<<nb, P4T, smem_p4, st>>>(d_desc, d_work, par);
     rec(5);
     launches += 4;
   }

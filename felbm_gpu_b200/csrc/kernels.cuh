@@ -120,6 +120,11 @@ __device__ __forceinline__ bool is_site(R v) {
 // brick shapes and tiles
 // ---------------------------------------------------------------------------
 constexpr int CTA = 256;
+// Threads per collide CTA; each collide warp leaves one flow-statistics
+// record. (128-thread CTAs measured slower: shared memory then limits an SM
+// to three of them, 12 warps instead of 16.)
+constexpr int P4T = 256;
+constexpr int P4W = P4T / 32;
 
 template <int BX_, int BY_, int BZ_>
 struct BrickShape {
@@ -154,25 +159,56 @@ struct Pro {
   uint64_t nmask[64][Sh::W];
   int32_t nbase[64][Sh::W];
   uint16_t slot_of[Sh::C];
-  double red[CTA / 32][6];
   double lambda;
   float ff;
+};
+
+// forcing_factor_at (reference felbm_gpu_main.cu:587-594)
+__device__ __forceinline__ double forcing_factor_dev(const DevPrm& P, const Ctl& C) {
+  if (!C.ff_auto) return C.ff_manual;
+  const double PI = 3.14159265358979323846;
+  if (P.forcing_timedep == 1) return sin(2.0 * PI * double(C.t) / P.forcing_period);
+  if (P.forcing_timedep == 2) {
+    const double x = sin(2.0 * PI * double(C.t) / P.forcing_period);
+    return (x < 0) ? -1.0 : ((x > 0) ? 1.0 : 0.0);
+  }
+  return 1.0;
+}
+
+// The step scalars of the lattice's control block into the prologue state
+// (called by one thread).
+template <class Sh>
+__device__ __forceinline__ void load_step_scalars(const LatDesc& D, Pro<Sh>& s) {
+  {
+    const Ctl& C = *D.ctl;
+    s.ff = (float)forcing_factor_dev(D.prm, C);
+    s.lambda = C.lambda;
+  }
+}
+
+// Shared state of the reductions of the flat (chunk) kernels; Pro<Sh> has the
+// same two members.
+struct Red {
+  double red[CTA / 32][6];
   int last;
 };
 
 // Load the brick record and the neighbour bricks' occupancy into shared
 // memory, and list the brick's fluid slots in site order.
-template <class Sh>
+template <class Sh, int NT = CTA, bool SCALARS = true>
 __device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s) {
   const int tid = threadIdx.x;
   {
     const int4* src = reinterpret_cast<const int4*>(D.rec + brick);
     int4* dst = reinterpret_cast<int4*>(&s.rec);
     constexpr int N4 = sizeof(BrickRec) / 16;
+    static_assert(N4 <= NT - 32, "the record is copied by the leading warps");
     if (tid < N4) dst[tid] = __ldg(src + tid);
+    // the step scalars load in parallel, from the last warp
+    if (SCALARS && tid == NT - 1) load_step_scalars<Sh>(D, s);
   }
   __syncthreads();
-  for (int q = tid; q < 64 * Sh::W; q += CTA) {
+  for (int q = tid; q < 64 * Sh::W; q += NT) {
     const int slot = q / Sh::W, w = q - slot * Sh::W;
     const int id = s.rec.nbr[slot];
     if (id >= 0) {
@@ -182,7 +218,7 @@ __device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s
   }
   __syncthreads();
   const int own = s.rec.seg[0][HMAX] + 4 * (s.rec.seg[1][HMAX] + 4 * s.rec.seg[2][Sh::HZ ? HMAX : 0]);
-  for (int q = tid; q < Sh::C; q += CTA) {
+  for (int q = tid; q < Sh::C; q += NT) {
     const int w = q >> 6, b = q & 63;
     const uint64_t m = s.nmask[own][w];
     if ((m >> b) & 1ull) s.slot_of[s.nbase[own][w] - s.rec.first + __popcll(m & ((1ull << b) - 1ull))] = (uint16_t)q;
@@ -192,12 +228,12 @@ __device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s
 // Site indices of a whole halo-H tile, built row by row: for each (y, z) row
 // and each neighbour brick it crosses, the row's occupancy bits and first site
 // index, then per position one popcount. Ends with a barrier.
-template <class Sh, int H>
+template <class Sh, int H, int NT = CTA>
 __device__ __forceinline__ void build_idx_tile(const Pro<Sh>& s, int32_t* __restrict__ s_idx,
                                                uint32_t* __restrict__ s_rbits, int32_t* __restrict__ s_rbase) {
   using T = Tile<Sh, H>;
   constexpr int ROWS = T::TY * T::TZ;
-  for (int q = threadIdx.x; q < ROWS * 4; q += CTA) {
+  for (int q = threadIdx.x; q < ROWS * 4; q += NT) {
     const int row = q >> 2, sx = q & 3;
     const int ty = row % T::TY, tz = row / T::TY;
     const int ay = ty + (HMAX - H), az = Sh::HZ ? tz + (HMAX - H) : 0;
@@ -215,7 +251,7 @@ __device__ __forceinline__ void build_idx_tile(const Pro<Sh>& s, int32_t* __rest
     s_rbase[q] = base;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < T::N; t += CTA) {
+  for (int t = threadIdx.x; t < T::N; t += NT) {
     const int row = t / T::TX, tx = t - row * T::TX;
     const int ax = tx + (HMAX - H);
     const int q = row * 4 + s.rec.seg[0][ax];
@@ -233,34 +269,6 @@ struct IdxTile {
   int32_t idx[T::N];
   uint32_t rbits[T::TY * T::TZ * 4];
   int32_t rbase[T::TY * T::TZ * 4];
-};
-
-// forcing_factor_at (reference felbm_gpu_main.cu:587-594)
-__device__ __forceinline__ double forcing_factor_dev(const DevPrm& P, const Ctl& C) {
-  if (!C.ff_auto) return C.ff_manual;
-  const double PI = 3.14159265358979323846;
-  if (P.forcing_timedep == 1) return sin(2.0 * PI * double(C.t) / P.forcing_period);
-  if (P.forcing_timedep == 2) {
-    const double x = sin(2.0 * PI * double(C.t) / P.forcing_period);
-    return (x < 0) ? -1.0 : ((x > 0) ? 1.0 : 0.0);
-  }
-  return 1.0;
-}
-
-template <class Sh>
-__device__ __forceinline__ void load_step_scalars(const LatDesc& D, Pro<Sh>& s) {
-  if (threadIdx.x == 0) {
-    const Ctl& C = *D.ctl;
-    s.ff = (float)forcing_factor_dev(D.prm, C);
-    s.lambda = C.lambda;
-  }
-}
-
-// Shared state of the reductions of the flat (chunk) kernels; Pro<Sh> has the
-// same two members.
-struct Red {
-  double red[CTA / 32][6];
-  int last;
 };
 
 // Block reduction of NV doubles into thread 0 (the last one as a max when mx).
@@ -433,15 +441,15 @@ __device__ __forceinline__ R corr_c(R c, double lambda) {
 // reads the site indices of all its positions, then issues all its gathers
 // before the first use, so a CTA waits for one round of L2/HBM latency instead
 // of one per position. The fields are read-only for the kernel (__ldg).
-template <class Sh, int H, int NF, class R, class F>
+template <class Sh, int H, int NF, int NT = CTA, class R, class F>
 __device__ __forceinline__ void stage(const F* const (&src)[NF], R* const (&dst)[NF], bool correct, double lambda,
                                       const int32_t* __restrict__ s_idx) {
   using T = Tile<Sh, H>;
-  constexpr int PER = (T::N + CTA - 1) / CTA;
+  constexpr int PER = (T::N + NT - 1) / NT;
   int j[PER];
 #pragma unroll
   for (int u = 0; u < PER; ++u) {
-    const int t = threadIdx.x + u * CTA;
+    const int t = threadIdx.x + u * NT;
     j[u] = (t < T::N) ? s_idx[t] : -1;
   }
   F v[PER][NF];
@@ -451,7 +459,7 @@ __device__ __forceinline__ void stage(const F* const (&src)[NF], R* const (&dst)
     for (int f = 0; f < NF; ++f) v[u][f] = j[u] >= 0 ? __ldg(src[f] + j[u]) : F(0);
 #pragma unroll
   for (int u = 0; u < PER; ++u) {
-    const int t = threadIdx.x + u * CTA;
+    const int t = threadIdx.x + u * NT;
     if (t < T::N) {
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
@@ -521,7 +529,6 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   prologue<Sh>(D, wk.y, s);
-  load_step_scalars<Sh>(D, s);
   build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
   {
     const F* const src[1] = {static_cast<const F*>(D.c)};
@@ -612,7 +619,7 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
   __shared__ R s_m[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  prologue<Sh>(D, wk.y, s);
+  prologue<Sh, CTA, false>(D, wk.y, s);
   build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
   {
     const F* const src[1] = {static_cast<const F*>(D.mu)};
@@ -900,7 +907,7 @@ __global__ void __launch_bounds__(CTA) k_stats_finalize(const LatDesc* __restric
   __shared__ Red s;
   const LatDesc& D = descs[lat];
   double tot[6];
-  sum_partials<6>(D.part4, D.nbricks * (CTA / 32), 6, tot, s, true);  // one record per warp
+  sum_partials<6>(D.part4, D.nbricks * P4W, 6, tot, s, true);  // one record per collide warp
   if (threadIdx.x == 0)
     for (int q = 0; q < 6; ++q) D.ctl->stats[q] = tot[q];
 }
