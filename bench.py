@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16s", "bf16s"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served sweep and request stream")
+    ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per solve of the 64-solve sweep")
+    ap.add_argument("--stream-seconds", type=float, default=15.0, help="arrival window of the request stream")
+    ap.add_argument("--stream-rate", type=float, default=4.0, help="Poisson arrival rate (requests / s)")
     return ap.parse_args()
 
 
@@ -183,6 +187,167 @@ def cpu_sample_mlups(storage_label: str, seconds: float = 12.0):
                       f"({o.n} sites), {steps} steps in {dt:.1f} s"}
 
 
+def sweep_specs(count: int, steps: int, seed: int = 7):
+    """The batching sweep: uneven solves, 2-D cylinder packs 64^2 to 512^2 and
+    3-D random-field media 48^3 to 128^3, porosity U[0.3, 0.6], contact angle
+    U[30, 150] deg, mobility coefficient U[0.005, 0.05], MRT, mass correction,
+    slab initial condition, body force 1e-6."""
+    from felbm_gpu_b200 import default_params, geometry
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        por, theta, mob = rng.uniform(0.3, 0.6), rng.uniform(30, 150), rng.uniform(0.005, 0.05)
+        if k % 2 == 0:
+            L = int(rng.integers(64, 513))
+            solid, _ = geometry.cylinders((1, L, L), 6.0, 12.0, por, seed=seed * 1000 + k)
+        else:
+            L = int(rng.integers(48, 129))
+            solid, _ = geometry.grf((L, L, L), 6.0, por, seed=seed * 1000 + k, flow_axis=0)
+        sigma, W = 1e-3, 4.0
+        p = default_params(rho0=1.0, rho1=1.0, tau0=1.0, tau1=1.0, surface_tension=sigma, interface_width=W,
+                           mobility_coeff=mob, phi=6 * sigma * np.cos(np.radians(theta)), gx=1e-6, use_mrt=1,
+                           correct_op_mass=1)
+        out.append({"params": p, "solid": solid, "init": (1, (0.0, 0.0, 0.0, 0.0, L / 2)), "W": W,
+                    "steps": steps, "sites": int(np.count_nonzero(solid == 0))})
+    return out
+
+
+def stream_specs(seconds: float, rate: float, seed: int = 11):
+    """The served request stream: Poisson arrivals; geometry (2-D pack or 3-D
+    random field), size log-uniform 64^2 x 1 .. 200^3, contact angle and step
+    count drawn from the seed. Step counts are 1/20 of the workload's
+    1000-20,000 (50-1000) so the stream fits a short run."""
+    from felbm_gpu_b200 import default_params, geometry
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        k = len(out)
+        sites_target = float(np.exp(rng.uniform(np.log(64 ** 2), np.log(200 ** 3))))
+        por, theta = rng.uniform(0.3, 0.6), rng.uniform(30, 150)
+        if sites_target < 512 ** 2 and rng.random() < 0.5:
+            L = max(64, int(round(np.sqrt(sites_target))))
+            solid, _ = geometry.cylinders((1, L, L), 6.0, 12.0, por, seed=seed * 1000 + k)
+        else:
+            L = int(np.clip(round(sites_target ** (1 / 3)), 48, 200))
+            solid, _ = geometry.grf((L, L, L), 6.0, por, seed=seed * 1000 + k, flow_axis=0)
+        sigma, W = 1e-3, 4.0
+        p = default_params(rho0=1.0, rho1=1.0, tau0=1.0, tau1=1.0, surface_tension=sigma, interface_width=W,
+                           mobility_coeff=0.02, phi=6 * sigma * np.cos(np.radians(theta)), gx=1e-6, use_mrt=1,
+                           correct_op_mass=1)
+        out.append({"arrival": t, "params": p, "solid": solid, "init": (1, (0.0, 0.0, 0.0, 0.0, L / 2)),
+                    "W": W, "steps": int(rng.integers(50, 1001)), "sites": int(np.count_nonzero(solid == 0))})
+    return out
+
+
+def run_alone(spec, storage: str):
+    """One solve through the plain engine: create, upload, run, fields back."""
+    from felbm_gpu_b200 import MultiPhaseGPU, _capi, geometry
+    import ctypes as C
+    p = _capi.FeParams()
+    C.pointer(p)[0] = spec["params"]
+    p.storage = _capi.STORAGE[storage]
+    kind, a = spec["init"]
+    c = geometry.order_parameter(spec["solid"], "slab", spec["W"], origin=a[:3], axis=int(a[3]), thickness=a[4])
+    h0, g0 = geometry.equilibrium(c, 1.0, p.rho0, p.rho1)
+    e = MultiPhaseGPU(p, spec["solid"])
+    try:
+        e.upload_state(h0, g0)
+        e.record_target_mass()
+        e.run(spec["steps"])
+        return e.download(), e.current_mass(), e.get_target_mass()
+    finally:
+        e.free()
+
+
+def serve_legs(args):
+    """Served sweep and request stream against the plain engine on the same GPU."""
+    import torch
+    from felbm_gpu_b200.serving import Server
+    storage = "f32"
+    out = {}
+    # -- the 64-solve sweep: all submitted at once --------------------------
+    specs = sweep_specs(64, args.sweep_steps)
+    work = sum(s["sites"] * s["steps"] for s in specs)
+    run_alone(specs[0], storage)  # warm-up (library, context, kernels)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seq = [run_alone(s, storage) for s in specs]
+    t_seq = time.perf_counter() - t0
+    srv = Server(storage=storage, chunk_steps=50)
+    t0 = time.perf_counter()
+    for k, s in enumerate(specs):
+        srv.submit(k, s["params"], s["solid"], s["steps"], init=s["init"], init_width=s["W"])
+    res = []
+    while len(res) < len(specs):
+        res += srv.poll()
+        time.sleep(0.002)
+    t_srv = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    res.sort(key=lambda r: r.id)
+    same = all(r.status == 0 and np.array_equal(r.fields["c"], seq[r.id][0]["c"]) for r in res)
+    dc = max(float(np.max(np.abs(r.fields["c"] - seq[r.id][0]["c"]))) for r in res)
+    drift = max(abs(r.mass_final - r.mass0) / abs(r.mass0) for r in res)
+    out["sweep"] = {"solves": len(specs), "steps_each": args.sweep_steps, "site_updates": work,
+                    "served_mlups": work / t_srv / 1e6, "sequential_mlups": work / t_seq / 1e6,
+                    "speedup": t_seq / t_srv, "served_s": t_srv, "sequential_s": t_seq,
+                    "ttr_p50_s": st["ttr_p50"], "ttr_p99_s": st["ttr_p99"],
+                    "results_identical_to_alone": bool(same), "max_abs_dc_vs_alone": dc,
+                    "max_rel_mass_drift": drift,
+                    "what": "64 uneven solves (2-D packs 64^2-512^2, 3-D GRF 48^3-128^3, porosity, angle, "
+                            "mobility from seed 7), MRT FP32, submitted together to the request loop vs run one "
+                            "after another through the plain engine; both include engine creation, upload and "
+                            "field download; host wall clock"}
+    # -- the Poisson request stream -----------------------------------------
+    reqs = stream_specs(args.stream_seconds, args.stream_rate)
+    if reqs:
+        srv = Server(storage=storage, chunk_steps=50)
+        t0 = time.perf_counter()
+        res, nxt = [], 0
+        while len(res) < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt]["arrival"] <= now:
+                s = reqs[nxt]
+                srv.submit(nxt, s["params"], s["solid"], s["steps"], init=s["init"], init_width=s["W"],
+                           want_fields=False)
+                nxt += 1
+            res += srv.poll()
+            time.sleep(0.002)
+        t_srv = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        ttr = np.array([r.time_to_result for r in res])
+        # the same requests, one after another through the plain engine: a
+        # request starts at its arrival or when the previous one finished
+        durs = []
+        for s in reqs:
+            t1 = time.perf_counter()
+            run_alone(s, storage)
+            durs.append(time.perf_counter() - t1)
+        free_at, ttr_seq = 0.0, []
+        for s, d in zip(reqs, durs):
+            start = max(s["arrival"], free_at)
+            free_at = start + d
+            ttr_seq.append(free_at - s["arrival"])
+        work = sum(s["sites"] * s["steps"] for s in reqs)
+        out["stream"] = {"requests": len(reqs), "rate_per_s": args.stream_rate, "window_s": args.stream_seconds,
+                         "site_updates": work, "served_mlups_busy": st["mlups_busy"],
+                         "served_ttr_p50_s": float(np.percentile(ttr, 50)),
+                         "served_ttr_p99_s": float(np.percentile(ttr, 99)),
+                         "sequential_ttr_p50_s": float(np.percentile(ttr_seq, 50)),
+                         "sequential_ttr_p99_s": float(np.percentile(ttr_seq, 99)),
+                         "served_makespan_s": t_srv, "sequential_makespan_s": free_at,
+                         "peak_active": st["peak_active"],
+                         "what": "Poisson arrivals, sizes log-uniform 64^2..200^3 (2-D pack or 3-D GRF), angle "
+                                 "from seed 11, steps 50-1000 (1/20 of the workload's), MRT FP32; sequential = "
+                                 "the same requests queued one at a time on the plain engine (measured solve "
+                                 "times, simulated queue)"}
+    return out
+
+
 def run_reference_arm(args, ws, rank):
     if rank != 0:
         return 0
@@ -310,6 +475,10 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample_mlups(args.storage)
+    serving = None
+    if ws == 1 and not args.no_serve:
+        eng.free()
+        serving = serve_legs(args)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -320,7 +489,7 @@ def main():
                            "sites": int(n), "porosity": por, "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (state > 1 GB), no flush"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary()}
+                "clocks": clk.summary(), "serving": serving}
         print(json.dumps(line), flush=True)
     eng.free()
     if dist:

@@ -6,7 +6,7 @@ This package is a thin Python mirror of the reference engine interface for
 tests, benchmarks and scripting.
 """
 from . import _capi  # noqa: F401  (raises ImportError if the library is missing)
-from .engine import MultiPhaseGPU, OpenBoundary, default_params  # noqa: F401
+from .engine import Batch, MultiPhaseGPU, OpenBoundary, default_params  # noqa: F401
 from . import geometry  # noqa: F401
 
-__all__ = ["MultiPhaseGPU", "OpenBoundary", "default_params", "geometry"]
+__all__ = ["Batch", "MultiPhaseGPU", "OpenBoundary", "default_params", "geometry"]

@@ -71,6 +71,36 @@ class FeFields(C.Structure):
     _fields_ = [("rho", _dp), ("c", _dp), ("ux", _dp), ("uy", _dp), ("uz", _dp), ("p", _dp), ("mu", _dp)]
 
 
+class FeServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("max_active", C.c_int), ("hbm_reserve_frac", C.c_double),
+                ("chunk_steps", C.c_int), ("storage", C.c_int), ("fill_sites", C.c_int64)]
+
+
+class FeRequest(C.Structure):
+    _fields_ = [("id", C.c_int64), ("params", FeParams), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("solid", C.POINTER(C.c_uint8)), ("h0", C.POINTER(C.c_double)), ("g0", C.POINTER(C.c_double)),
+                ("init_kind", C.c_int), ("init_a", C.c_double * 5), ("init_width", C.c_double),
+                ("init_p", C.c_double), ("steps", C.c_int64), ("conv_tol", C.c_double),
+                ("want_fields", C.c_int)]
+
+
+class FeResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int), ("message", C.c_char * 160),
+                ("sites", C.c_int64), ("steps_done", C.c_int64),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("mass0", C.c_double), ("mass_final", C.c_double), ("stats", C.c_double * 6),
+                ("rho", C.POINTER(C.c_double)), ("c", C.POINTER(C.c_double)), ("ux", C.POINTER(C.c_double)),
+                ("uy", C.POINTER(C.c_double)), ("uz", C.POINTER(C.c_double)), ("p", C.POINTER(C.c_double))]
+
+
+class FeServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("queued", C.c_int64), ("active", C.c_int64), ("peak_active", C.c_int64),
+                ("site_steps", C.c_int64), ("busy_seconds", C.c_double), ("elapsed_seconds", C.c_double),
+                ("mlups_busy", C.c_double), ("mlups_wall", C.c_double),
+                ("ttr_p50", C.c_double), ("ttr_p99", C.c_double), ("ttr_max", C.c_double)]
+
+
 _vp = C.c_void_p
 _i64p = C.POINTER(C.c_int64)
 _u8p = C.POINTER(C.c_uint8)
@@ -108,6 +138,23 @@ SIGNATURES = {
     "fe_time_run": (C.c_int, [_vp, C.c_int, _fp]),
     "fe_time_kernels": (C.c_int, [_vp, C.c_int, _fp, C.c_int]),
     "fe_launch_count": (C.c_int, [_vp, _i64p]),
+    "fe_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "fe_batch_destroy": (C.c_int, [_vp]),
+    "fe_batch_add": (C.c_int, [_vp, _vp]),
+    "fe_batch_remove": (C.c_int, [_vp, _vp]),
+    "fe_batch_size": (C.c_int, [_vp, C.POINTER(C.c_int), _i64p]),
+    "fe_batch_run": (C.c_int, [_vp, C.c_int]),
+    "fe_batch_launch": (C.c_int, [_vp, C.c_int]),
+    "fe_batch_wait": (C.c_int, [_vp]),
+    "fe_batch_time_run": (C.c_int, [_vp, C.c_int, _fp]),
+    "fe_batch_launch_count": (C.c_int, [_vp, _i64p]),
+    "fe_server_create": (C.c_int, [C.POINTER(FeServerConfig), C.POINTER(C.c_void_p)]),
+    "fe_server_submit": (C.c_int, [_vp, C.POINTER(FeRequest)]),
+    "fe_server_poll": (C.c_int, [_vp, C.POINTER(FeResult), C.c_int, C.POINTER(C.c_int)]),
+    "fe_server_free_result": (C.c_int, [C.POINTER(FeResult)]),
+    "fe_server_wait_idle": (C.c_int, [_vp, C.c_double]),
+    "fe_server_get_stats": (C.c_int, [_vp, C.POINTER(FeServerStats)]),
+    "fe_server_destroy": (C.c_int, [_vp]),
     "fe_last_error": (C.c_char_p, []),
     "fe_version": (C.c_char_p, []),
     "fe_geom_grf": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int,

@@ -211,6 +211,7 @@ struct Engine {
   bool stats_pending = false;
   double* h_stats = nullptr;  // pinned [6]
   double target_mass_host = 0.0;
+  struct Batch* owner = nullptr;  // batch the engine is a member of
 
   ~Engine() { release(); }
   void release() {
@@ -263,6 +264,7 @@ struct Engine {
       d.rate_value[q] = P.mrt_rate_value[q];
     }
     d.use_mrt = P.use_mrt; d.hbb = P.use_halfway_bb; d.correct_mass = P.correct_op_mass;
+    d.need_j = (P.rho0 != P.rho1 || open_bnd) ? 1 : 0;
     d.forcing_timedep = P.forcing_timedep; d.forcing_period = P.forcing_period;
     d.c_ref = P.c_ref; d.p_ref = P.p_ref;
     // 16-bit deviations: h_k - w_k c_ref spans about w_k, g_k - w_k p_ref about
@@ -362,10 +364,6 @@ struct Engine {
     return FE_OK;
   }
 
-  // The momentum fields are read by P2 only for the drho pressure correction,
-  // and by the open-boundary kernels.
-  bool need_j() const { return hd.prm.drho != 0.0 || open_bnd; }
-
   // ---- one step (plain launches) -----------------------------------------
   template <class S>
   void launch_bc(cudaStream_t st) {
@@ -379,7 +377,7 @@ struct Engine {
     const int nb = hd.nbricks;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
     rec(0);
-    k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, need_j() ? 1 : 0);
+    k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
     rec(2);
@@ -592,6 +590,309 @@ struct Engine {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Batch: many lattices advanced together, one launch per pass over the
+// concatenated work lists of all members (P1 over their site chunks, P2-P4
+// over their bricks, grouped by brick shape and collision kind), captured as
+// CUDA graphs. Members keep their own buffers, control blocks and
+// reductions; every kernel finds its lattice through the work item, so the
+// result of a member is the one it gets alone. A rebuild (membership change,
+// or a member stepped on its own) maps each member's current buffer to slot
+// 0 of its batch descriptor, so the batch parity is uniform.
+// ---------------------------------------------------------------------------
+struct Batch {
+  struct Group {
+    int shape2d = 0, mrt = 0;
+    int2* d_work = nullptr;
+    int nwork = 0;
+  };
+  int device = 0;
+  int storage = -1;
+  cudaStream_t stream = nullptr;
+  std::vector<Engine*> mem;
+  std::vector<int> join_parity;     // member parity at the last rebuild
+  std::vector<Group> groups;
+  LatDesc* d_desc = nullptr;
+  int2* d_cwork = nullptr;
+  int ncwork = 0;
+  std::vector<void*> allocs;
+  int64_t since_build = 0;          // steps since the last rebuild
+  bool dirty = true;
+  int inflight = 0;                 // steps launched by fe_batch_launch, not yet waited for
+  cudaGraphExec_t graph1[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+  int64_t launches = 0;
+
+  ~Batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (inflight) finish(inflight);
+    inflight = 0;
+    settle();
+    for (Engine* e : mem) e->owner = nullptr;
+    drop_graphs();
+    free_arrays();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void free_arrays() {
+    for (void* a : allocs) cudaFree(a);
+    allocs.clear();
+    groups.clear();
+    d_desc = nullptr;
+    d_cwork = nullptr;
+    ncwork = 0;
+  }
+  void drop_graphs() {
+    for (int p = 0; p < 2; ++p) {
+      if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
+      if (graph2[p]) cudaGraphExecDestroy(graph2[p]);
+      graph1[p] = graph2[p] = nullptr;
+    }
+  }
+  int create(int dev) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      return fe_fail(FE_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (dev >= 0) FE_CUDA(cudaSetDevice(dev));
+    FE_CUDA(cudaGetDevice(&device));
+    FE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    return FE_OK;
+  }
+  int find(const Engine* e) const {
+    for (size_t q = 0; q < mem.size(); ++q)
+      if (mem[q] == e) return (int)q;
+    return -1;
+  }
+  int add(Engine* e) {
+    if (inflight) return fe_fail(FE_ERR_STATE, "batch steps in flight (fe_batch_wait first)");
+    if (find(e) >= 0) return fe_fail(FE_ERR_STATE, "engine already in the batch");
+    if (e->owner) return fe_fail(FE_ERR_STATE, "engine is a member of another batch");
+    if (e->device != device) return fe_fail(FE_ERR_ARG, "engine and batch on different devices");
+    if (storage >= 0 && e->storage != storage) return fe_fail(FE_ERR_ARG, "a batch holds one storage type");
+    storage = e->storage;
+    cudaStreamSynchronize(e->stream);
+    e->owner = this;
+    mem.push_back(e);
+    dirty = true;
+    return FE_OK;
+  }
+  int remove(Engine* e) {
+    const int q = find(e);
+    if (q < 0) return fe_fail(FE_ERR_STATE, "engine not in the batch");
+    if (inflight) {  // a member that goes away: finish the steps in flight first
+      int rc;
+      if ((rc = wait())) return rc;
+    }
+    FE_CUDA(cudaStreamSynchronize(stream));
+    settle();
+    e->owner = nullptr;
+    mem.erase(mem.begin() + q);
+    if (q < (int)join_parity.size()) join_parity.erase(join_parity.begin() + q);
+    if (mem.empty()) storage = -1;
+    dirty = true;
+    return FE_OK;
+  }
+  // members' own parity after the batch steps since the rebuild
+  void settle() {
+    if (dirty) return;  // no batch step since the members' parity was read
+    for (size_t q = 0; q < mem.size() && q < join_parity.size(); ++q)
+      mem[q]->parity = join_parity[q] ^ (int)(since_build & 1);
+  }
+  template <class T>
+  int upload_vec(T** p, const std::vector<T>& v) {
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
+    if (cudaMalloc(&q, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fe_fail(FE_ERR_MEMORY, "batch arrays");
+    }
+    allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    if (!v.empty()) FE_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return FE_OK;
+  }
+  int rebuild() {
+    drop_graphs();
+    free_arrays();
+    since_build = 0;
+    join_parity.assign(mem.size(), 0);
+    std::vector<LatDesc> descs(mem.size());
+    std::vector<int2> cw;
+    int rc;
+    for (size_t q = 0; q < mem.size(); ++q) {
+      Engine* e = mem[q];
+      FE_CUDA(cudaStreamSynchronize(e->stream));
+      join_parity[q] = e->parity;
+      LatDesc d = e->hd;
+      for (int f = 0; f < 2; ++f) {
+        d.pop[0][f] = e->hd.pop[e->parity][f];
+        d.pop[1][f] = e->hd.pop[e->parity ^ 1][f];
+      }
+      descs[q] = d;
+      for (int c = 0; c < d.nchunks; ++c) cw.push_back(make_int2((int)q, c));
+      if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;  // queued correction, forcing from t
+    }
+    for (int sh = 0; sh < 2; ++sh)
+      for (int mrt = 0; mrt < 2; ++mrt) {
+        std::vector<int2> w;
+        for (size_t q = 0; q < mem.size(); ++q)
+          if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0))
+            for (int b = 0; b < mem[q]->hd.nbricks; ++b) w.push_back(make_int2((int)q, b));
+        if (w.empty()) continue;
+        Group g;
+        g.shape2d = sh;
+        g.mrt = mrt;
+        g.nwork = (int)w.size();
+        if ((rc = upload_vec(&g.d_work, w))) return rc;
+        groups.push_back(g);
+      }
+    if ((rc = upload_vec(&d_desc, descs))) return rc;
+    if ((rc = upload_vec(&d_cwork, cw))) return rc;
+    ncwork = (int)cw.size();
+    dirty = false;
+    return FE_OK;
+  }
+
+  template <class S, class Sh>
+  void launch_group_p2(const Group& g, cudaStream_t st) {
+    k_cfield<S, Sh, 0><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, FieldOut{});
+  }
+  template <class S, class Sh>
+  void launch_group_p3(const Group& g, cudaStream_t st) {
+    k_lapmu<S, Sh><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work);
+  }
+  template <class S, class Sh>
+  void launch_group_p4(const Group& g, int par, cudaStream_t st) {
+    const size_t sm = CollideSmem<Sh, typename S::real>::BYTES;
+    if (g.mrt) k_collide<S, Sh, 1><<<g.nwork, P4T, sm, st>>>(d_desc, g.d_work, par);
+    else k_collide<S, Sh, 0><<<g.nwork, P4T, sm, st>>>(d_desc, g.d_work, par);
+  }
+  template <class S>
+  void launch_step_t(int par, cudaStream_t st) {
+    k_moments<S><<<ncwork, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
+    for (size_t q = 0; q < mem.size(); ++q) {
+      const Engine* e = mem[q];
+      if (!e->open_bnd) continue;
+      const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf, nall = nio + nb;
+      if (nio) k_bc_fields<S><<<(nio + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
+      if (nb) k_bc_buffers<S><<<(nb + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
+      if (nall) k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
+    }
+    for (const Group& g : groups) {
+      if (g.shape2d) launch_group_p2<S, Shape2D>(g, st);
+      else launch_group_p2<S, Shape3D>(g, st);
+    }
+    for (const Group& g : groups) {
+      if (g.shape2d) launch_group_p3<S, Shape2D>(g, st);
+      else launch_group_p3<S, Shape3D>(g, st);
+    }
+    for (const Group& g : groups) {
+      if (g.shape2d) launch_group_p4<S, Shape2D>(g, par, st);
+      else launch_group_p4<S, Shape3D>(g, par, st);
+    }
+  }
+  void launch_step(int par, cudaStream_t st) {
+    switch (storage) {
+      case FE_F64: launch_step_t<StF64>(par, st); break;
+      case FE_F32: launch_step_t<StF32>(par, st); break;
+      case FE_F16S: launch_step_t<StF16S>(par, st); break;
+      default: launch_step_t<StBF16S>(par, st); break;
+    }
+  }
+  // kernels of one step, the count launch_step_t makes
+  int64_t launches_per_step() const {
+    int64_t k = 1 + 3 * (int64_t)groups.size();
+    for (const Engine* e : mem)
+      if (e->open_bnd) {
+        const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf;
+        k += (nio ? 1 : 0) + (nb ? 1 : 0) + (nio + nb ? 1 : 0);
+      }
+    return k;
+  }
+  int build_graphs() {
+    for (int p = 0; p < 2; ++p)
+      for (int len = 1; len <= 2; ++len) {
+        cudaGraph_t g;
+        FE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < len; ++s) launch_step(p ^ (s & 1), stream);
+        cudaError_t e1 = cudaStreamEndCapture(stream, &g);
+        if (e1 != cudaSuccess) return fe_fail(FE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e1));
+        cudaGraphExec_t ex;
+        cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) return fe_fail(FE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+        (len == 1 ? graph1 : graph2)[p] = ex;
+      }
+    return FE_OK;
+  }
+  // descriptors, control blocks and graphs ready for a run
+  int prepare() {
+    int rc;
+    // a member stepped on its own since the rebuild: remap its buffers
+    for (size_t q = 0; q < mem.size() && !dirty; ++q)
+      if (mem[q]->parity != (join_parity[q] ^ (int)(since_build & 1))) dirty = true;
+    if (dirty) {
+      if ((rc = rebuild())) return rc;
+    } else {
+      for (Engine* e : mem) {
+        FE_CUDA(cudaStreamSynchronize(e->stream));
+        if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;
+      }
+    }
+    if (!graph1[0] && (rc = build_graphs())) return rc;
+    return FE_OK;
+  }
+  // graph launches of nsteps on the batch stream (after prepare)
+  int run_async(int nsteps) {
+    const int64_t kps = launches_per_step();
+    int par = (int)(since_build & 1);
+    int s = 0;
+    while (s < nsteps) {
+      if (nsteps - s >= 2) {
+        FE_CUDA(cudaGraphLaunch(graph2[par], stream));
+        s += 2;
+        launches += 2 * kps;
+      } else {
+        FE_CUDA(cudaGraphLaunch(graph1[par], stream));
+        par ^= 1;
+        s += 1;
+        launches += kps;
+      }
+    }
+    FE_CUDA(cudaGetLastError());
+    return FE_OK;
+  }
+  int finish(int nsteps) {
+    since_build += nsteps;
+    for (Engine* e : mem) e->t_host += nsteps;
+    settle();
+    return FE_OK;
+  }
+  int run(int nsteps) {
+    int rc;
+    if ((rc = launch(nsteps))) return rc;
+    return wait();
+  }
+  // queue nsteps and return; members must not be used until wait()
+  int launch(int nsteps) {
+    if (inflight) return fe_fail(FE_ERR_STATE, "batch steps already in flight");
+    if (mem.empty() || nsteps == 0) return FE_OK;
+    int rc;
+    if ((rc = prepare())) return rc;
+    if ((rc = run_async(nsteps))) return rc;
+    inflight = nsteps;
+    return FE_OK;
+  }
+  int wait() {
+    if (!inflight) return FE_OK;
+    const int n = inflight;
+    inflight = 0;
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return finish(n);
+  }
+};
+
 }  // namespace fe
 
 using fe::Engine;
@@ -651,6 +952,7 @@ int fe_engine_create(const fe_params* p, int nx, int ny, int nz, const uint8_t* 
 
 int fe_engine_destroy(fe_engine* e) {
   if (!e) return FE_OK;
+  if (e->e.owner) e->e.owner->remove(&e->e);
   cudaStreamSynchronize(e->e.stream);
   delete e;
   return FE_OK;
@@ -779,6 +1081,7 @@ int fe_set_open_bnd(fe_engine* e, const fe_open_bnd* b) {
   d.inlet_c_a = b->inlet_c_a; d.inlet_mode = b->inlet_mode;
   d.inlet_period = b->inlet_period; d.inlet_duty = b->inlet_duty; d.inlet_ramp = b->inlet_ramp;
   d.split_pos = b->split_pos;
+  d.need_j = 1;
   E.open_bnd = true;
   E.drop_graphs();
   return E.upload_desc();
@@ -957,6 +1260,101 @@ int fe_time_kernels(fe_engine* e, int nsteps, float* ms, int nk) {
 int fe_launch_count(const fe_engine* e, int64_t* count) {
   FE_GUARD(e);
   if (count) *count = e->e.launches;
+  return FE_OK;
+}
+
+// ---- batches ---------------------------------------------------------------
+struct fe_batch {
+  fe::Batch b;
+};
+
+#define FE_BGUARD(b) \
+  if (!(b)) return fe_fail(FE_ERR_ARG, "null batch")
+
+int fe_batch_create(int device, fe_batch** out) {
+  if (!out) return fe_fail(FE_ERR_ARG, "null output");
+  *out = nullptr;
+  fe_batch* b = new (std::nothrow) fe_batch();
+  if (!b) return fe_fail(FE_ERR_MEMORY, "host allocation");
+  const int rc = b->b.create(device);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return FE_OK;
+}
+
+int fe_batch_destroy(fe_batch* b) {
+  delete b;
+  return FE_OK;
+}
+
+int fe_batch_add(fe_batch* b, fe_engine* e) {
+  FE_BGUARD(b);
+  FE_GUARD(e);
+  return b->b.add(&e->e);
+}
+
+int fe_batch_remove(fe_batch* b, fe_engine* e) {
+  FE_BGUARD(b);
+  FE_GUARD(e);
+  return b->b.remove(&e->e);
+}
+
+int fe_batch_size(const fe_batch* b, int* members, int64_t* sites) {
+  FE_BGUARD(b);
+  if (members) *members = (int)b->b.mem.size();
+  if (sites) {
+    int64_t n = 0;
+    for (const Engine* e : b->b.mem) n += e->hd.n;
+    *sites = n;
+  }
+  return FE_OK;
+}
+
+int fe_batch_run(fe_batch* b, int nsteps) {
+  FE_BGUARD(b);
+  if (nsteps < 0) return fe_fail(FE_ERR_ARG, "nsteps < 0");
+  return b->b.run(nsteps);
+}
+
+int fe_batch_launch(fe_batch* b, int nsteps) {
+  FE_BGUARD(b);
+  if (nsteps < 0) return fe_fail(FE_ERR_ARG, "nsteps < 0");
+  return b->b.launch(nsteps);
+}
+
+int fe_batch_wait(fe_batch* b) {
+  FE_BGUARD(b);
+  return b->b.wait();
+}
+
+int fe_batch_time_run(fe_batch* b, int nsteps, float* ms) {
+  FE_BGUARD(b);
+  if (nsteps < 1 || !ms) return fe_fail(FE_ERR_ARG, "fe_batch_time_run: bad arguments");
+  fe::Batch& B = b->b;
+  if (B.mem.empty()) return fe_fail(FE_ERR_STATE, "empty batch");
+  if (B.inflight) return fe_fail(FE_ERR_STATE, "batch steps in flight");
+  int rc;
+  // graphs and descriptors ready before the timed region
+  if ((rc = B.prepare())) return rc;
+  cudaEvent_t e0, e1;
+  FE_CUDA(cudaEventCreate(&e0));
+  FE_CUDA(cudaEventCreate(&e1));
+  FE_CUDA(cudaEventRecord(e0, B.stream));
+  if ((rc = B.run_async(nsteps))) return rc;
+  FE_CUDA(cudaEventRecord(e1, B.stream));
+  FE_CUDA(cudaEventSynchronize(e1));
+  FE_CUDA(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return B.finish(nsteps);
+}
+
+int fe_batch_launch_count(const fe_batch* b, int64_t* count) {
+  FE_BGUARD(b);
+  if (count) *count = b->b.launches;
   return FE_OK;
 }
 

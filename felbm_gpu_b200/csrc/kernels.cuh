@@ -376,6 +376,7 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   double acc[2] = {0.0, 0.0};
+  write_j |= D.prm.need_j;
   const int64_t i0 = (int64_t)chunk * CHUNK;
   const int64_t iend = i0 + CHUNK < D.n ? i0 + CHUNK : D.n;
   for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
     fc[i] = (F)c;
     fp[i] = (F)p;
     if (write_j) {  // read only by P2's pressure correction (drho != 0), the
-      fjx[i] = (F)jx;  // open-boundary kernels and field downloads
+      fjx[i] = (F)jx;  // open-boundary kernels and field downloads (need_j | forced)
       fjy[i] = (F)jy;
       fjz[i] = (F)jz;
     }

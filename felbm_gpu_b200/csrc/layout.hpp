@@ -70,6 +70,7 @@ struct DevPrm {
   double rate_value[7];
   int rate_mode[7];
   int use_mrt, hbb, correct_mass;
+  int need_j;  // P1 writes the momentum (drho != 0 or open boundaries)
   int forcing_timedep;
   double forcing_period;
   // open boundary

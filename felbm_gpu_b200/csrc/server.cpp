@@ -1,0 +1,464 @@
+// Serving: a request loop over the public C-ABI (fe_engine_*, fe_batch_*).
+// No counterpart in the reference, which runs one solve per process
+// (felbm_gpu_main.cu). One host thread owns the device work:
+//  * admission: queued solves become resident (engine created, state
+//    uploaded) while a slot is free and their footprint fits the budget;
+//  * scheduling: each chunk runs the resident solves with the least
+//    remaining work, up to fill_sites sites, as one batch (the GPU's
+//    throughput saturates at a few million sites, so adding more solves to a
+//    chunk only slows every member's step rate);
+//  * overlap: a chunk is launched asynchronously, and while it runs the loop
+//    reads back the solves that retired in the previous chunk and admits new
+//    ones (their work goes on their own engine streams);
+//  * retirement: after the step count, or the convergence test.
+// Submission and polling only touch the queues under a mutex.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/felbm_b200.h"
+#include "fe_internal.hpp"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Req {
+  fe_request r;               // arrays are held by the owned vectors below
+  std::vector<uint8_t> solid;
+  std::vector<double> h0, g0;
+  int64_t sites = 0;
+  double t_submit = 0.0;
+};
+
+struct Live {
+  Req q;
+  fe_engine* e = nullptr;
+  int64_t done = 0;
+  double t_admit = 0.0;
+  double mass0 = 0.0;
+  double last_u = NAN;
+  double bytes = 0.0;         // footprint charged to the budget
+  bool in_batch = false;
+  int status = FE_OK;         // nonzero: failed, report it
+};
+
+size_t pop_bytes(int storage) { return storage == FE_F64 ? 8 : (storage == FE_F32 ? 4 : 2); }
+size_t fld_bytes(int storage) { return storage == FE_F64 ? 8 : 4; }
+
+// Device bytes of one resident solve: two ping-pong buffers of h and g, the
+// seven per-site fields, the FP64 transfer buffer (upload/download), and the
+// site/brick tables (generous per-site bound).
+double footprint(int64_t n, int storage) {
+  const double per = 4.0 * 19 * pop_bytes(storage) + 7.0 * fld_bytes(storage) + 2.0 * 19 * 8 + 64;
+  return (double)n * per + (double)(64 << 20);
+}
+
+double percentile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (double)(v.size() - 1);
+  const size_t lo = (size_t)std::floor(pos), hi = std::min(v.size() - 1, lo + 1);
+  return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
+}
+
+}  // namespace
+
+struct fe_server {
+  fe_server_config cfg{};
+  fe_batch* batch = nullptr;
+  Clock::time_point t0;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;       // work arrived / stop
+  std::condition_variable cv_idle;  // queue and resident set drained
+  std::deque<Req> queue;
+  std::vector<Live> live;           // resident solves (loop thread only)
+  std::vector<Live> retiring;       // stepped out, results not read back yet
+  std::vector<fe_result> finished;
+  bool stop = false;
+  double budget = 0.0, committed = 0.0, reserve = 0.0;
+  // statistics (under mu)
+  int64_t submitted = 0, admitted = 0, completed = 0, active = 0, peak_active = 0, site_steps = 0;
+  double busy = 0.0;
+  std::vector<double> ttr;
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+  void report(fe_result& r, bool ok) {
+    std::lock_guard<std::mutex> g(mu);
+    finished.push_back(r);
+    if (ok) ttr.push_back(r.t_done - r.t_submit);
+    ++completed;
+    --active;
+  }
+
+  fe_result base_result(const Live& L) const {
+    fe_result r{};
+    r.id = L.q.r.id;
+    r.sites = L.q.sites;
+    r.steps_done = L.done;
+    r.t_submit = L.q.t_submit;
+    r.t_admit = L.t_admit;
+    r.mass0 = L.mass0;
+    return r;
+  }
+
+  void release(Live& L) {
+    if (L.e) fe_engine_destroy(L.e);  // leaves the batch first
+    L.e = nullptr;
+    committed -= L.bytes;
+    L.bytes = 0.0;
+  }
+
+  void fail(Live& L, int status) {
+    fe_result r = base_result(L);
+    r.status = status;
+    std::snprintf(r.message, sizeof(r.message), "%s", fe_last_error());
+    release(L);
+    r.t_done = now();
+    report(r, false);
+  }
+
+  // Results of a retired solve (its engine is out of the batch).
+  void read_back(Live& L) {
+    fe_result r = base_result(L);
+    int rc = fe_flow_stats(L.e, r.stats);
+    if (!rc) rc = fe_current_mass(L.e, &r.mass_final);
+    if (!rc && L.q.r.want_fields) {
+      const size_t nb = std::max<size_t>((size_t)L.q.sites * sizeof(double), 8);
+      double** dst[6] = {&r.rho, &r.c, &r.ux, &r.uy, &r.uz, &r.p};
+      for (double** d : dst) {
+        *d = static_cast<double*>(std::malloc(nb));
+        if (!*d) rc = FE_ERR_MEMORY;
+      }
+      fe_fields f{r.rho, r.c, r.ux, r.uy, r.uz, r.p, nullptr};
+      if (!rc) rc = fe_download_fields(L.e, &f);
+    }
+    if (rc) {
+      r.status = rc;
+      std::snprintf(r.message, sizeof(r.message), "%s", fe_last_error());
+    }
+    r.t_done = now();
+    report(r, rc == FE_OK);
+  }
+
+  // Creates the engine of an admitted solve and uploads its state.
+  bool make_resident(Live& L) {
+    Req& q = L.q;
+    fe_params p = q.r.params;
+    p.storage = cfg.storage;
+    int rc = fe_engine_create(&p, q.r.nx, q.r.ny, q.r.nz, q.solid.data(), cfg.device, &L.e);
+    if (rc) { fail(L, rc); return false; }
+    const int64_t vn = 19 * q.sites;
+    if (q.h0.empty()) {
+      std::vector<double> c(q.sites), pr(q.sites, q.r.init_p);
+      q.h0.resize(vn);
+      q.g0.resize(vn);
+      if ((rc = fe_init_order_parameter(q.solid.data(), q.r.nx, q.r.ny, q.r.nz, q.r.init_kind, q.r.init_a,
+                                        q.r.init_width, c.data())) ||
+          (rc = fe_init_equilibrium(q.sites, c.data(), pr.data(), nullptr, nullptr, nullptr, p.rho0, p.rho1,
+                                    q.h0.data(), q.g0.data()))) {
+        fail(L, rc);
+        return false;
+      }
+    }
+    if ((rc = fe_upload_state(L.e, q.h0.data(), q.g0.data(), vn))) { fail(L, rc); return false; }
+    std::vector<double>().swap(q.h0);  // the state lives on the device now
+    std::vector<double>().swap(q.g0);
+    std::vector<uint8_t>().swap(q.solid);
+    if (p.correct_op_mass && (rc = fe_record_target_mass(L.e))) { fail(L, rc); return false; }
+    if ((rc = fe_current_mass(L.e, &L.mass0))) { fail(L, rc); return false; }
+    return true;
+  }
+
+  bool fits(int64_t sites) {
+    if (cfg.max_active > 0 && (int)(live.size() + retiring.size()) >= cfg.max_active) return false;
+    const double need = footprint(sites, cfg.storage);
+    if (committed + need > budget) return false;
+    size_t fr = 0, tot = 0;  // memory other users took since the server started
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return (double)fr - need >= reserve;
+  }
+
+  // Admits queued solves (oldest first) while they fit.
+  void admit() {
+    for (;;) {
+      Req q;
+      {
+        std::lock_guard<std::mutex> g(mu);
+        if (stop || queue.empty()) return;
+        // with nothing resident, the oldest solve is admitted even if its
+        // estimate exceeds the budget: engine creation then reports an
+        // out-of-memory failure for it instead of a queue that never moves
+        if (!fits(queue.front().sites) && !(live.empty() && retiring.empty())) return;
+        q = std::move(queue.front());
+        queue.pop_front();
+        ++admitted;
+        ++active;
+        peak_active = std::max(peak_active, active);
+      }
+      Live L;
+      L.q = std::move(q);
+      L.t_admit = now();
+      L.bytes = footprint(L.q.sites, cfg.storage);
+      committed += L.bytes;
+      if (make_resident(L)) live.push_back(std::move(L));
+    }
+  }
+
+  void drain_retiring() {
+    for (Live& L : retiring) {
+      read_back(L);
+      release(L);
+    }
+    retiring.clear();
+  }
+
+  // The chunk's running set: least remaining work first, up to fill_sites.
+  std::vector<int> choose() {
+    std::vector<int> idx(live.size());
+    for (size_t q = 0; q < live.size(); ++q) idx[q] = (int)q;
+    auto work = [&](int q) { return (double)live[q].q.sites * (double)(live[q].q.r.steps - live[q].done); };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return work(a) < work(b); });
+    std::vector<int> run;
+    int64_t sites = 0;
+    for (int q : idx) {
+      if (!run.empty() && cfg.fill_sites > 0 && sites + live[q].q.sites > cfg.fill_sites) continue;
+      run.push_back(q);
+      sites += live[q].q.sites;
+    }
+    return run;
+  }
+
+  void loop() {
+    cudaSetDevice(cfg.device);
+    {
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) cudaGetLastError();
+      reserve = cfg.hbm_reserve_frac * (double)tot;
+      budget = (double)fr - reserve;
+    }
+    for (;;) {
+      {
+        std::lock_guard<std::mutex> g(mu);
+        if (stop) break;
+      }
+      if (live.empty()) {
+        drain_retiring();
+        admit();
+        if (live.empty()) {
+          std::unique_lock<std::mutex> g(mu);
+          if (stop) break;
+          if (queue.empty()) {
+            cv_idle.notify_all();
+            cv.wait(g, [&] { return stop || !queue.empty(); });
+          }
+          continue;
+        }
+      }
+      // batch membership of this chunk
+      const std::vector<int> run = choose();
+      std::vector<char> sel(live.size(), 0);
+      for (int q : run) sel[q] = 1;
+      for (size_t q = 0; q < live.size(); ++q)
+        if (live[q].in_batch && !sel[q]) {
+          fe_batch_remove(batch, live[q].e);
+          live[q].in_batch = false;
+        }
+      int64_t chunk = cfg.chunk_steps, sites = 0;
+      for (int q : run) {
+        Live& L = live[q];
+        if (!L.in_batch) {
+          const int rc = fe_batch_add(batch, L.e);
+          if (rc) L.status = rc;
+          else L.in_batch = true;
+        }
+        chunk = std::min(chunk, L.q.r.steps - L.done);
+        sites += L.q.sites;
+      }
+      chunk = std::max<int64_t>(chunk, 1);
+      const double tb = now();
+      int rc = fe_batch_launch(batch, (int)chunk);
+      // while the chunk runs: results of the last retirements, new solves
+      drain_retiring();
+      admit();
+      sel.resize(live.size(), 0);  // solves admitted meanwhile did not run
+      if (!rc) rc = fe_batch_wait(batch);
+      const double te = now();
+      if (rc) {  // the batch failed: report every solve of the chunk
+        for (int q : run) live[q].status = rc;
+      } else {
+        std::lock_guard<std::mutex> g(mu);
+        busy += te - tb;
+        site_steps += sites * chunk;
+      }
+      std::vector<Live> keep;
+      for (size_t q = 0; q < live.size(); ++q) {
+        Live& L = live[q];
+        if (L.status) {
+          fail(L, L.status);
+          continue;
+        }
+        bool ret = false;
+        if (sel[q]) {
+          L.done += chunk;
+          ret = L.done >= L.q.r.steps;
+          if (!ret && L.q.r.conv_tol > 0.0) {
+            double st[6];
+            if (fe_flow_stats(L.e, st) == FE_OK) {
+              const double u = std::sqrt(st[0] * st[0] + st[1] * st[1] + st[2] * st[2]) / (double)L.q.sites;
+              if (std::isfinite(L.last_u) &&
+                  std::fabs(u - L.last_u) <= L.q.r.conv_tol * std::max(std::fabs(u), 1e-300))
+                ret = true;
+              L.last_u = u;
+            }
+          }
+        }
+        if (ret) {
+          fe_batch_remove(batch, L.e);
+          L.in_batch = false;
+          retiring.push_back(std::move(L));
+        } else {
+          keep.push_back(std::move(L));
+        }
+      }
+      live.swap(keep);
+    }
+    drain_retiring();
+    for (Live& L : live) release(L);
+    live.clear();
+    std::lock_guard<std::mutex> g(mu);
+    cv_idle.notify_all();
+  }
+};
+
+extern "C" {
+
+int fe_server_create(const fe_server_config* cfg, fe_server** out) {
+  if (!cfg || !out) return fe_fail(FE_ERR_ARG, "fe_server_create: bad arguments");
+  if (cfg->chunk_steps < 1) return fe_fail(FE_ERR_ARG, "chunk_steps must be > 0");
+  if (cfg->storage < FE_F64 || cfg->storage > FE_BF16S) return fe_fail(FE_ERR_ARG, "unknown storage");
+  if (cfg->hbm_reserve_frac < 0.0 || cfg->hbm_reserve_frac >= 1.0)
+    return fe_fail(FE_ERR_ARG, "hbm_reserve_frac must be in [0, 1)");
+  *out = nullptr;
+  fe_server* s = new (std::nothrow) fe_server();
+  if (!s) return fe_fail(FE_ERR_MEMORY, "host allocation");
+  s->cfg = *cfg;
+  const int rc = fe_batch_create(cfg->device, &s->batch);
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  s->t0 = Clock::now();
+  s->th = std::thread([s] { s->loop(); });
+  *out = s;
+  return FE_OK;
+}
+
+int fe_server_submit(fe_server* s, const fe_request* r) {
+  if (!s || !r) return fe_fail(FE_ERR_ARG, "fe_server_submit: bad arguments");
+  if (!r->solid || r->nx < 1 || r->ny < 1 || r->nz < 1 || r->steps < 1)
+    return fe_fail(FE_ERR_ARG, "fe_server_submit: bad request");
+  if ((r->h0 == nullptr) != (r->g0 == nullptr)) return fe_fail(FE_ERR_ARG, "give both h0 and g0, or neither");
+  Req q;
+  q.r = *r;
+  const size_t nodes = (size_t)r->nx * r->ny * r->nz;
+  q.solid.assign(r->solid, r->solid + nodes);
+  int64_t n = 0;
+  const int rc = fe_geom_sites(q.solid.data(), r->nx, r->ny, r->nz, &n, nullptr);
+  if (rc) return rc;
+  if (n == 0) return fe_fail(FE_ERR_ARG, "request geometry has no fluid site");
+  q.sites = n;
+  if (r->h0) {
+    q.h0.assign(r->h0, r->h0 + 19 * n);
+    q.g0.assign(r->g0, r->g0 + 19 * n);
+  }
+  q.r.solid = nullptr;  // the copies above are used
+  q.r.h0 = q.r.g0 = nullptr;
+  std::lock_guard<std::mutex> g(s->mu);
+  q.t_submit = s->now();
+  s->queue.push_back(std::move(q));
+  ++s->submitted;
+  s->cv.notify_all();
+  return FE_OK;
+}
+
+int fe_server_poll(fe_server* s, fe_result* out, int max, int* n) {
+  if (!s || !n || (max > 0 && !out)) return fe_fail(FE_ERR_ARG, "fe_server_poll: bad arguments");
+  std::lock_guard<std::mutex> g(s->mu);
+  const int k = std::max(0, std::min<int>(max, (int)s->finished.size()));
+  for (int q = 0; q < k; ++q) out[q] = s->finished[q];
+  s->finished.erase(s->finished.begin(), s->finished.begin() + k);
+  *n = k;
+  return FE_OK;
+}
+
+int fe_server_free_result(fe_result* r) {
+  if (!r) return FE_OK;
+  double** f[6] = {&r->rho, &r->c, &r->ux, &r->uy, &r->uz, &r->p};
+  for (double** d : f) {
+    std::free(*d);
+    *d = nullptr;
+  }
+  return FE_OK;
+}
+
+int fe_server_wait_idle(fe_server* s, double timeout_s) {
+  if (!s) return fe_fail(FE_ERR_ARG, "null server");
+  std::unique_lock<std::mutex> g(s->mu);
+  const bool ok = s->cv_idle.wait_for(g, std::chrono::duration<double>(timeout_s),
+                                      [&] { return s->queue.empty() && s->active == 0; });
+  return ok ? FE_OK : fe_fail(FE_ERR_STATE, "fe_server_wait_idle: timeout");
+}
+
+int fe_server_get_stats(fe_server* s, fe_server_stats* st) {
+  if (!s || !st) return fe_fail(FE_ERR_ARG, "fe_server_get_stats: bad arguments");
+  std::lock_guard<std::mutex> g(s->mu);
+  *st = fe_server_stats{};
+  st->submitted = s->submitted;
+  st->admitted = s->admitted;
+  st->completed = s->completed;
+  st->queued = (int64_t)s->queue.size();
+  st->active = s->active;
+  st->peak_active = s->peak_active;
+  st->site_steps = s->site_steps;
+  st->busy_seconds = s->busy;
+  st->elapsed_seconds = s->now();
+  st->mlups_busy = s->busy > 0 ? (double)s->site_steps / s->busy / 1e6 : 0.0;
+  st->mlups_wall = st->elapsed_seconds > 0 ? (double)s->site_steps / st->elapsed_seconds / 1e6 : 0.0;
+  st->ttr_p50 = percentile(s->ttr, 0.50);
+  st->ttr_p99 = percentile(s->ttr, 0.99);
+  st->ttr_max = s->ttr.empty() ? 0.0 : *std::max_element(s->ttr.begin(), s->ttr.end());
+  return FE_OK;
+}
+
+int fe_server_destroy(fe_server* s) {
+  if (!s) return FE_OK;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stop = true;
+    s->cv.notify_all();
+  }
+  if (s->th.joinable()) s->th.join();
+  for (fe_result& r : s->finished) fe_server_free_result(&r);
+  fe_batch_destroy(s->batch);
+  delete s;
+  return FE_OK;
+}
+
+}  // extern "C"

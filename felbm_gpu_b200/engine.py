@@ -234,3 +234,52 @@ class MultiPhaseGPU:
         c = C.c_int64()
         check(lib.fe_launch_count(self._h, C.byref(c)))
         return c.value
+
+
+class Batch:
+    """Many engines advanced together (fe_batch_*): one launch per pass over
+    all members, CUDA graphs; each member gets the result it gets alone."""
+
+    def __init__(self, device: int = -1):
+        h = C.c_void_p()
+        check(lib.fe_batch_create(device, C.byref(h)))
+        self._h = h
+        self.members: list[MultiPhaseGPU] = []
+
+    def add(self, eng: MultiPhaseGPU):
+        check(lib.fe_batch_add(self._h, eng._h))
+        self.members.append(eng)
+
+    def remove(self, eng: MultiPhaseGPU):
+        check(lib.fe_batch_remove(self._h, eng._h))
+        self.members.remove(eng)
+
+    def size(self) -> tuple[int, int]:
+        m, n = C.c_int(), C.c_int64()
+        check(lib.fe_batch_size(self._h, C.byref(m), C.byref(n)))
+        return m.value, n.value
+
+    def run(self, nsteps: int):
+        check(lib.fe_batch_run(self._h, nsteps))
+
+    def time_run(self, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib.fe_batch_time_run(self._h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def launch_count(self) -> int:
+        c = C.c_int64()
+        check(lib.fe_batch_launch_count(self._h, C.byref(c)))
+        return c.value
+
+    def free(self):
+        if self._h:
+            lib.fe_batch_destroy(self._h)
+            self._h = None
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

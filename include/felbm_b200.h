@@ -254,10 +254,111 @@ int fe_init_equilibrium(int64_t n, const double* c, const double* p, const doubl
 #define FE_NOALLOC_MAX_SITES 33554432LL
 int fe_mass_weight_noalloc(const double* d_h, int64_t n, double* d_out, void* stream);
 
+/* ---- batches -------------------------------------------------------------
+ * No counterpart in the reference (one MultiPhaseGPU per process there).
+ * A batch advances many engines (independent lattices of any size, same
+ * device and storage type) together: each pass of the step is one launch
+ * over the concatenated brick/chunk lists of all members, captured as CUDA
+ * graphs, so small lattices share the GPU instead of each leaving it idle.
+ * Every member keeps its own state, parameters, mass target and statistics,
+ * and gets bit-for-bit the result it gets from fe_run alone. fe_batch_run
+ * behaves as fe_run on every member (queued mass correction after each step,
+ * forcing factor from the step counter) and returns when the steps are done.
+ * Engines stay usable on their own between batch runs; fe_engine_destroy of
+ * a member removes it first. */
+typedef struct fe_batch fe_batch;
+int fe_batch_create(int device, fe_batch** out);
+int fe_batch_destroy(fe_batch* b);
+int fe_batch_add(fe_batch* b, fe_engine* e);
+int fe_batch_remove(fe_batch* b, fe_engine* e);
+int fe_batch_size(const fe_batch* b, int* members, int64_t* sites);
+int fe_batch_run(fe_batch* b, int nsteps);
+/* fe_batch_run in two halves: fe_batch_launch queues the steps on the batch
+ * stream and returns at once, so the caller's host work (creating and
+ * uploading the next engines, reading back retired ones) overlaps them;
+ * fe_batch_wait waits for them. In between, members must not be used and
+ * fe_batch_add fails (fe_batch_remove waits first). */
+int fe_batch_launch(fe_batch* b, int nsteps);
+int fe_batch_wait(fe_batch* b);
+/* fe_batch_run of nsteps timed with CUDA events on the batch stream. */
+int fe_batch_time_run(fe_batch* b, int nsteps, float* ms);
+int fe_batch_launch_count(const fe_batch* b, int64_t* count);
+
+/* ---- serving -------------------------------------------------------------
+ * No counterpart in the reference. A request loop on its own host thread.
+ * Solves submitted at any time wait in a queue and are admitted (engine
+ * created, state uploaded, kept resident on the device) while a slot is free
+ * and their estimated footprint fits the memory budget: the device memory
+ * free at fe_server_create minus hbm_reserve_frac of the device's total.
+ * Resident solves advance in chunks of at most chunk_steps steps; each chunk
+ * runs the resident solves with the least remaining work (sites x remaining
+ * steps) together in one batch, adding solves until their sites reach
+ * fill_sites (<= 0: all of them), so a small solve is not held to the step
+ * rate of a large batch. Admission and retirement happen between chunks and
+ * their host work (engine creation, upload, read-back) overlaps the chunk on
+ * the GPU: continuous batching. A solve retires after its step count or,
+ * when conv_tol > 0, once the mean velocity changes by less than conv_tol
+ * (relative) between two of its chunks. Results carry the time-to-result
+ * (submit -> results read back) and, on request, the fields. Every solve
+ * gets bit-for-bit the result it gets alone (fe_batch). Requests with open
+ * boundaries are not served. */
+typedef struct fe_server fe_server;
+typedef struct fe_server_config {
+  int device;
+  int max_active;             /* resident solves at most (<= 0: no limit)  */
+  double hbm_reserve_frac;    /* device memory kept free (fraction of total) */
+  int chunk_steps;            /* steps between admission points (> 0)     */
+  int storage;                /* FE_F64 .. FE_BF16S, all requests          */
+  int64_t fill_sites;         /* sites per chunk (<= 0: every resident solve) */
+} fe_server_config;
+typedef struct fe_request {
+  int64_t id;
+  fe_params params;           /* params.storage is overridden by the server's */
+  int nx, ny, nz;
+  const uint8_t* solid;       /* nz*ny*nx, copied at submit                */
+  const double* h0;           /* initial state (reference layout, copied)  */
+  const double* g0;           /* or NULL: built from the init fields below */
+  int init_kind;              /* fe_init_order_parameter kind              */
+  double init_a[5];
+  double init_width;
+  double init_p;              /* initial pressure level                    */
+  int64_t steps;              /* retire after this many steps              */
+  double conv_tol;            /* > 0: convergence test (see above)         */
+  int want_fields;            /* 1: the result carries rho, c, u, p        */
+} fe_request;
+typedef struct fe_result {
+  int64_t id;
+  int status;                 /* FE_OK, or the failing call's status       */
+  char message[160];
+  int64_t sites, steps_done;
+  double t_submit, t_admit, t_done;   /* seconds since fe_server_create   */
+  double mass0, mass_final;   /* order-parameter mass at admission / end   */
+  double stats[6];            /* flow statistics at retirement             */
+  double *rho, *c, *ux, *uy, *uz, *p; /* n each (reference order) or NULL */
+} fe_result;
+typedef struct fe_server_stats {
+  int64_t submitted, admitted, completed, queued, active, peak_active; /* active = resident */
+  int64_t site_steps;         /* fluid-site updates done                   */
+  double busy_seconds;        /* time inside batch runs                    */
+  double elapsed_seconds;     /* since fe_server_create                    */
+  double mlups_busy, mlups_wall;
+  double ttr_p50, ttr_p99, ttr_max;   /* time-to-result of completed solves */
+} fe_server_stats;
+int fe_server_create(const fe_server_config* cfg, fe_server** out);
+/* Thread-safe; copies the request's arrays. */
+int fe_server_submit(fe_server* s, const fe_request* r);
+/* Moves up to max finished results into out; *n = how many. */
+int fe_server_poll(fe_server* s, fe_result* out, int max, int* n);
+int fe_server_free_result(fe_result* r);
+/* Blocks until nothing is queued or active (or timeout_s passes: FE_ERR_STATE). */
+int fe_server_wait_idle(fe_server* s, double timeout_s);
+int fe_server_get_stats(fe_server* s, fe_server_stats* st);
+/* Stops the loop (active solves are dropped) and frees everything. */
+int fe_server_destroy(fe_server* s);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* Time nsteps of fe_run with CUDA events on the engine's stream; ms_total is
- * the device time, ms_collide the summed device time of the fused collision
- * kernel measured in a separate instrumented pass of nsteps_collide steps. */
+ * the device time. */
 int fe_time_run(fe_engine* e, int nsteps, float* ms_total);
 int fe_time_kernels(fe_engine* e, int nsteps, float* ms_per_kernel, int nkernels);
 /* Number of kernels the engine launched since creation. */

@@ -1,0 +1,127 @@
+"""Batches (fe_batch_*): many lattices advanced by one launch per pass. Every
+member must get bit-for-bit the result it gets from fe_run alone (same
+kernels, per-lattice control blocks and deterministic per-lattice
+reductions), through membership changes and members stepped on their own
+between batch runs."""
+import numpy as np
+import pytest
+
+from cases import make_case
+from felbm_gpu_b200 import Batch, MultiPhaseGPU
+from parity import with_storage
+
+pytestmark = pytest.mark.gpu
+
+MIX = ["spheres_mrt", "cyl2d_mrt", "grf_mrt_mass", "grf_bgk_mass", "openbnd_bgk", "spheres_mrt_wet"]
+
+
+def make_engine(name, storage):
+    case = make_case(name)
+    e = MultiPhaseGPU(with_storage(case.params, storage), case.solid)
+    if case.open_bnd is not None:
+        e.set_open_bnd(case.open_bnd)
+    e.upload_state(case.h0, case.g0)
+    if case.correct_mass:
+        e.record_target_mass()
+    return e
+
+
+def alone(name, storage, steps):
+    e = make_engine(name, storage)
+    try:
+        e.run(steps)
+        h, g = e.download_state()
+        return h, g, e.download(), e.flow_stats()
+    finally:
+        e.free()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16s"])
+def test_batch_equals_alone(require_gpu, storage):
+    steps = 23
+    ref = {n: alone(n, storage, steps) for n in MIX}
+    b = Batch()
+    engines = {n: make_engine(n, storage) for n in MIX}
+    try:
+        for e in engines.values():
+            b.add(e)
+        assert b.size()[0] == len(MIX)
+        b.run(10)
+        b.run(13)
+        for n, e in engines.items():
+            h, g = e.download_state()
+            f = e.download()
+            hr, gr, fr, sr = ref[n]
+            assert np.array_equal(h, hr), (n, np.max(np.abs(h - hr)))
+            assert np.array_equal(g, gr), (n, np.max(np.abs(g - gr)))
+            for k in ("c", "rho", "ux", "p", "mu"):
+                assert np.array_equal(f[k], fr[k]), (n, k)
+            assert np.array_equal(e.flow_stats(), sr), n
+        assert b.launch_count() > 0
+    finally:
+        b.free()
+        for e in engines.values():
+            e.free()
+
+
+def test_batch_membership_and_solo_steps(require_gpu):
+    """Members join late, leave early, and one member is stepped on its own
+    between batch runs; each still matches its own step count run alone."""
+    storage = "f64"
+    a = make_engine("spheres_mrt", storage)
+    c = make_engine("grf_mrt_mass", storage)
+    d = make_engine("cyl2d_mrt", storage)
+    b = Batch()
+    try:
+        b.add(a)
+        b.run(5)            # a: 5
+        b.add(c)
+        b.run(4)            # a: 9, c: 4
+        c.run(3)            # c: 7 on its own
+        b.add(d)
+        b.run(6)            # a: 15, c: 13, d: 6
+        b.remove(a)
+        b.run(1)            # c: 14, d: 7
+        for e, name, steps in ((a, "spheres_mrt", 15), (c, "grf_mrt_mass", 14), (d, "cyl2d_mrt", 7)):
+            h, g = e.download_state()
+            hr, gr, _, _ = alone(name, storage, steps)
+            assert np.array_equal(h, hr), (name, np.max(np.abs(h - hr)))
+            assert np.array_equal(g, gr), (name, np.max(np.abs(g - gr)))
+    finally:
+        b.free()
+        for e in (a, c, d):
+            e.free()
+
+
+def test_batch_destroying_a_member(require_gpu):
+    a = make_engine("spheres_mrt", "f32")
+    c = make_engine("cyl2d_mrt", "f32")
+    b = Batch()
+    try:
+        b.add(a)
+        b.add(c)
+        b.run(2)
+        a.free()            # leaves the batch first
+        b.members.remove(a)
+        assert b.size()[0] == 1
+        b.run(3)
+        h, _ = c.download_state()
+        hr, _, _, _ = alone("cyl2d_mrt", "f32", 5)
+        assert np.array_equal(h, hr)
+    finally:
+        b.free()
+        c.free()
+
+
+def test_batch_rejects_mixed_storage(require_gpu):
+    a = make_engine("spheres_mrt", "f32")
+    c = make_engine("spheres_mrt", "f64")
+    b = Batch()
+    try:
+        b.add(a)
+        with pytest.raises(Exception, match="one storage type"):
+            b.add(c)
+    finally:
+        b.free()
+        a.free()
+        c.free()
