@@ -205,6 +205,8 @@ struct Engine {
   size_t smem_p4 = 0;
   bool open_bnd = false;
   double ff_manual = 1.0;
+  int ctl_mode = 0;           // run mode and forcing factor last written to
+  double ctl_ff = 1.0;        // the control block (its initial values)
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
   cudaGraphExec_t graph2[2] = {nullptr, nullptr};
   cudaEvent_t ev_stats = nullptr;
@@ -403,13 +405,17 @@ struct Engine {
   }
 
   int set_ctl_mode(int run_mode, double ff) {
+    run_mode = run_mode ? 1 : 0;
+    if (run_mode == ctl_mode && ff == ctl_ff) return FE_OK;  // already on the device
     // auto_correct, ff_auto, ff_manual are contiguous in Ctl
-    struct { int32_t auto_correct, ff_auto; double ff_manual; } m{run_mode ? 1 : 0, run_mode ? 1 : 0, ff};
+    struct { int32_t auto_correct, ff_auto; double ff_manual; } m{run_mode, run_mode, ff};
     static_assert(offsetof(Ctl, ff_auto) == offsetof(Ctl, auto_correct) + 4, "Ctl layout");
     static_assert(offsetof(Ctl, ff_manual) == offsetof(Ctl, auto_correct) + 8, "Ctl layout");
     FE_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(d_ctl) + offsetof(Ctl, auto_correct), &m, sizeof(m),
                             cudaMemcpyHostToDevice, stream));
     FE_CUDA(cudaStreamSynchronize(stream));
+    ctl_mode = run_mode;
+    ctl_ff = ff;
     return FE_OK;
   }
 
@@ -614,8 +620,9 @@ struct Batch {
   std::vector<Group> groups;
   LatDesc* d_desc = nullptr;
   int2* d_cwork = nullptr;
+  int2* d_gwork = nullptr;          // the groups' work lists, one after another
+  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0;  // bytes (grow-only)
   int ncwork = 0;
-  std::vector<void*> allocs;
   int64_t since_build = 0;          // steps since the last rebuild
   bool dirty = true;
   int inflight = 0;                 // steps launched by fe_batch_launch, not yet waited for
@@ -634,11 +641,12 @@ struct Batch {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_arrays() {
-    for (void* a : allocs) cudaFree(a);
-    allocs.clear();
+    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork})
+      if (a) cudaFree(a);
     groups.clear();
     d_desc = nullptr;
-    d_cwork = nullptr;
+    d_cwork = d_gwork = nullptr;
+    cap_desc = cap_cwork = cap_gwork = 0;
     ncwork = 0;
   }
   void drop_graphs() {
@@ -699,22 +707,30 @@ struct Batch {
     for (size_t q = 0; q < mem.size() && q < join_parity.size(); ++q)
       mem[q]->parity = join_parity[q] ^ (int)(since_build & 1);
   }
+  // Copies v to *p, growing the buffer (capacity *cap bytes) only when it is
+  // too small, so membership changes allocate and free nothing.
   template <class T>
-  int upload_vec(T** p, const std::vector<T>& v) {
-    void* q = nullptr;
+  int upload_vec(T** p, size_t* cap, const std::vector<T>& v) {
     const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
-    if (cudaMalloc(&q, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return fe_fail(FE_ERR_MEMORY, "batch arrays");
+    if (bytes > *cap) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+      *cap = 0;
+      void* q = nullptr;
+      const size_t want = bytes + bytes / 2;
+      if (cudaMalloc(&q, want) != cudaSuccess) {
+        cudaGetLastError();
+        return fe_fail(FE_ERR_MEMORY, "batch arrays");
+      }
+      *p = static_cast<T*>(q);
+      *cap = want;
     }
-    allocs.push_back(q);
-    *p = static_cast<T*>(q);
     if (!v.empty()) FE_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
     return FE_OK;
   }
   int rebuild() {
     drop_graphs();
-    free_arrays();
+    groups.clear();
     since_build = 0;
     join_parity.assign(mem.size(), 0);
     std::vector<LatDesc> descs(mem.size());
@@ -733,22 +749,26 @@ struct Batch {
       for (int c = 0; c < d.nchunks; ++c) cw.push_back(make_int2((int)q, c));
       if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;  // queued correction, forcing from t
     }
+    std::vector<int2> gw;
+    std::vector<size_t> offs;
     for (int sh = 0; sh < 2; ++sh)
       for (int mrt = 0; mrt < 2; ++mrt) {
-        std::vector<int2> w;
+        const size_t off = gw.size();
         for (size_t q = 0; q < mem.size(); ++q)
           if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0))
-            for (int b = 0; b < mem[q]->hd.nbricks; ++b) w.push_back(make_int2((int)q, b));
-        if (w.empty()) continue;
+            for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
+        if (gw.size() == off) continue;
         Group g;
         g.shape2d = sh;
         g.mrt = mrt;
-        g.nwork = (int)w.size();
-        if ((rc = upload_vec(&g.d_work, w))) return rc;
+        g.nwork = (int)(gw.size() - off);
         groups.push_back(g);
+        offs.push_back(off);
       }
-    if ((rc = upload_vec(&d_desc, descs))) return rc;
-    if ((rc = upload_vec(&d_cwork, cw))) return rc;
+    if ((rc = upload_vec(&d_gwork, &cap_gwork, gw))) return rc;
+    for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
+    if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
+    if ((rc = upload_vec(&d_cwork, &cap_cwork, cw))) return rc;
     ncwork = (int)cw.size();
     dirty = false;
     return FE_OK;

@@ -420,6 +420,7 @@ int fe_init_order_parameter(const uint8_t* solid, int nx, int ny, int nz, int ki
 int fe_init_equilibrium(int64_t n, const double* c, const double* p, const double* ux, const double* uy,
                         const double* uz, double rho0, double rho1, double* h, double* g) {
   if (!c || !p || !h || !g || n < 0) return fe_fail(FE_ERR_ARG, "fe_init_equilibrium: bad arguments");
+#pragma omp parallel for schedule(static) if (n > 65536)
   for (int64_t i = 0; i < n; ++i) {
     const double vx = ux ? ux[i] : 0.0, vy = uy ? uy[i] : 0.0, vz = uz ? uz[i] : 0.0;
     const double rho = rho1 + (rho0 - rho1) * c[i];

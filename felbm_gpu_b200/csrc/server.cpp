@@ -7,9 +7,11 @@
 //    remaining work, up to fill_sites sites, as one batch (the GPU's
 //    throughput saturates at a few million sites, so adding more solves to a
 //    chunk only slows every member's step rate);
-//  * overlap: a chunk is launched asynchronously, and while it runs the loop
-//    reads back the solves that retired in the previous chunk and admits new
-//    ones (their work goes on their own engine streams);
+//  * overlap: a prep thread builds initial states on the host ahead of
+//    admission; a chunk is launched asynchronously, and while it runs the
+//    loop reads back the solves that retired in the previous chunk and admits
+//    new ones (their work goes on their own engine streams); retired engines
+//    are freed after the chunk (freeing device memory waits for the GPU);
 //  * retirement: after the step count, or the convergence test.
 // Submission and polling only touch the queues under a mutex.
 #include <cuda_runtime.h>
@@ -40,6 +42,10 @@ struct Req {
   std::vector<double> h0, g0;
   int64_t sites = 0;
   double t_submit = 0.0;
+  bool ready = false;         // initial state present (given, or built by the prep thread)
+  bool preparing = false;
+  int prep_status = FE_OK;
+  std::string prep_message;
 };
 
 struct Live {
@@ -79,13 +85,15 @@ struct fe_server {
   fe_server_config cfg{};
   fe_batch* batch = nullptr;
   Clock::time_point t0;
-  std::thread th;
+  std::thread th, prep;
   std::mutex mu;
-  std::condition_variable cv;       // work arrived / stop
+  std::condition_variable cv;       // a prepared solve is queued / stop
+  std::condition_variable cv_prep;  // a solve needs its initial state / stop
   std::condition_variable cv_idle;  // queue and resident set drained
   std::deque<Req> queue;
   std::vector<Live> live;           // resident solves (loop thread only)
   std::vector<Live> retiring;       // stepped out, results not read back yet
+  std::vector<Live> to_free;        // read back; engines freed after the chunk
   std::vector<fe_result> finished;
   bool stop = false;
   double budget = 0.0, committed = 0.0, reserve = 0.0;
@@ -159,21 +167,13 @@ struct fe_server {
     Req& q = L.q;
     fe_params p = q.r.params;
     p.storage = cfg.storage;
+    if (q.prep_status) {
+      fail(L, fe_fail(q.prep_status, q.prep_message));
+      return false;
+    }
     int rc = fe_engine_create(&p, q.r.nx, q.r.ny, q.r.nz, q.solid.data(), cfg.device, &L.e);
     if (rc) { fail(L, rc); return false; }
     const int64_t vn = 19 * q.sites;
-    if (q.h0.empty()) {
-      std::vector<double> c(q.sites), pr(q.sites, q.r.init_p);
-      q.h0.resize(vn);
-      q.g0.resize(vn);
-      if ((rc = fe_init_order_parameter(q.solid.data(), q.r.nx, q.r.ny, q.r.nz, q.r.init_kind, q.r.init_a,
-                                        q.r.init_width, c.data())) ||
-          (rc = fe_init_equilibrium(q.sites, c.data(), pr.data(), nullptr, nullptr, nullptr, p.rho0, p.rho1,
-                                    q.h0.data(), q.g0.data()))) {
-        fail(L, rc);
-        return false;
-      }
-    }
     if ((rc = fe_upload_state(L.e, q.h0.data(), q.g0.data(), vn))) { fail(L, rc); return false; }
     std::vector<double>().swap(q.h0);  // the state lives on the device now
     std::vector<double>().swap(q.g0);
@@ -181,6 +181,41 @@ struct fe_server {
     if (p.correct_op_mass && (rc = fe_record_target_mass(L.e))) { fail(L, rc); return false; }
     if ((rc = fe_current_mass(L.e, &L.mass0))) { fail(L, rc); return false; }
     return true;
+  }
+
+  // Builds the initial states of queued solves (oldest first) on the host,
+  // ahead of their admission, so the loop thread only creates engines and
+  // uploads. Queue elements stay in place: the loop pops only ready ones.
+  void prep_loop() {
+    for (;;) {
+      Req* q = nullptr;
+      {
+        std::unique_lock<std::mutex> g(mu);
+        auto next = [&]() -> Req* {
+          for (Req& r : queue)
+            if (!r.ready && !r.preparing) return &r;
+          return nullptr;
+        };
+        cv_prep.wait(g, [&] { return stop || next() != nullptr; });
+        if (stop) return;
+        q = next();
+        q->preparing = true;
+      }
+      std::vector<double> c(q->sites), pr(q->sites, q->r.init_p), h(19 * q->sites), gg(19 * q->sites);
+      int rc = fe_init_order_parameter(q->solid.data(), q->r.nx, q->r.ny, q->r.nz, q->r.init_kind, q->r.init_a,
+                                       q->r.init_width, c.data());
+      if (!rc)
+        rc = fe_init_equilibrium(q->sites, c.data(), pr.data(), nullptr, nullptr, nullptr, q->r.params.rho0,
+                                 q->r.params.rho1, h.data(), gg.data());
+      std::lock_guard<std::mutex> g(mu);
+      q->h0.swap(h);
+      q->g0.swap(gg);
+      q->prep_status = rc;
+      if (rc) q->prep_message = fe_last_error();
+      q->preparing = false;
+      q->ready = true;
+      cv.notify_all();
+    }
   }
 
   bool fits(int64_t sites) {
@@ -201,7 +236,7 @@ struct fe_server {
       Req q;
       {
         std::lock_guard<std::mutex> g(mu);
-        if (stop || queue.empty()) return;
+        if (stop || queue.empty() || !queue.front().ready) return;
         // with nothing resident, the oldest solve is admitted even if its
         // estimate exceeds the budget: engine creation then reports an
         // out-of-memory failure for it instead of a queue that never moves
@@ -221,12 +256,18 @@ struct fe_server {
     }
   }
 
+  // Reads back retired solves; their engines are freed by free_retired()
+  // (freeing device memory waits for the GPU, so not while a chunk runs).
   void drain_retiring() {
     for (Live& L : retiring) {
       read_back(L);
-      release(L);
+      to_free.push_back(std::move(L));
     }
     retiring.clear();
+  }
+  void free_retired() {
+    for (Live& L : to_free) release(L);
+    to_free.clear();
   }
 
   // The chunk's running set: least remaining work first, up to fill_sites.
@@ -260,14 +301,13 @@ struct fe_server {
       }
       if (live.empty()) {
         drain_retiring();
+        free_retired();
         admit();
         if (live.empty()) {
           std::unique_lock<std::mutex> g(mu);
           if (stop) break;
-          if (queue.empty()) {
-            cv_idle.notify_all();
-            cv.wait(g, [&] { return stop || !queue.empty(); });
-          }
+          if (queue.empty()) cv_idle.notify_all();
+          cv.wait(g, [&] { return stop || (!queue.empty() && queue.front().ready); });
           continue;
         }
       }
@@ -300,6 +340,7 @@ struct fe_server {
       sel.resize(live.size(), 0);  // solves admitted meanwhile did not run
       if (!rc) rc = fe_batch_wait(batch);
       const double te = now();
+      free_retired();
       if (rc) {  // the batch failed: report every solve of the chunk
         for (int q : run) live[q].status = rc;
       } else {
@@ -340,6 +381,7 @@ struct fe_server {
       live.swap(keep);
     }
     drain_retiring();
+    free_retired();
     for (Live& L : live) release(L);
     live.clear();
     std::lock_guard<std::mutex> g(mu);
@@ -366,6 +408,7 @@ int fe_server_create(const fe_server_config* cfg, fe_server** out) {
   }
   s->t0 = Clock::now();
   s->th = std::thread([s] { s->loop(); });
+  s->prep = std::thread([s] { s->prep_loop(); });
   *out = s;
   return FE_OK;
 }
@@ -387,6 +430,7 @@ int fe_server_submit(fe_server* s, const fe_request* r) {
   if (r->h0) {
     q.h0.assign(r->h0, r->h0 + 19 * n);
     q.g0.assign(r->g0, r->g0 + 19 * n);
+    q.ready = true;
   }
   q.r.solid = nullptr;  // the copies above are used
   q.r.h0 = q.r.g0 = nullptr;
@@ -395,6 +439,7 @@ int fe_server_submit(fe_server* s, const fe_request* r) {
   s->queue.push_back(std::move(q));
   ++s->submitted;
   s->cv.notify_all();
+  s->cv_prep.notify_all();
   return FE_OK;
 }
 
@@ -453,8 +498,10 @@ int fe_server_destroy(fe_server* s) {
     std::lock_guard<std::mutex> g(s->mu);
     s->stop = true;
     s->cv.notify_all();
+    s->cv_prep.notify_all();
   }
   if (s->th.joinable()) s->th.join();
+  if (s->prep.joinable()) s->prep.join();
   for (fe_result& r : s->finished) fe_server_free_result(&r);
   fe_batch_destroy(s->batch);
   delete s;
