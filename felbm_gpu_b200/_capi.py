@@ -71,6 +71,10 @@ class FeFields(C.Structure):
     _fields_ = [("rho", _dp), ("c", _dp), ("ux", _dp), ("uy", _dp), ("uz", _dp), ("p", _dp), ("mu", _dp)]
 
 
+class FeTracerConfig(C.Structure):
+    _fields_ = [("substeps", C.c_int), ("order", C.c_int), ("velocity_skip", C.c_int), ("seed", C.c_uint64)]
+
+
 class FeServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("max_active", C.c_int), ("hbm_reserve_frac", C.c_double),
                 ("chunk_steps", C.c_int), ("storage", C.c_int), ("fill_sites", C.c_int64)]
@@ -148,6 +152,13 @@ SIGNATURES = {
     "fe_batch_wait": (C.c_int, [_vp]),
     "fe_batch_time_run": (C.c_int, [_vp, C.c_int, _fp]),
     "fe_batch_launch_count": (C.c_int, [_vp, _i64p]),
+    "fe_tracers_create": (C.c_int, [_vp, C.POINTER(FeTracerConfig), C.c_int64, _dp, _dp, _i64p,
+                                    C.POINTER(C.c_void_p)]),
+    "fe_tracers_destroy": (C.c_int, [_vp]),
+    "fe_tracers_step": (C.c_int, [_vp]),
+    "fe_tracers_download": (C.c_int, [_vp, _dp, _dp]),
+    "fe_tracers_seed": (C.c_int, [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int64,
+                                  C.c_uint64, _dp, _i32p]),
     "fe_server_create": (C.c_int, [C.POINTER(FeServerConfig), C.POINTER(C.c_void_p)]),
     "fe_server_submit": (C.c_int, [_vp, C.POINTER(FeRequest)]),
     "fe_server_poll": (C.c_int, [_vp, C.POINTER(FeResult), C.c_int, C.POINTER(C.c_int)]),

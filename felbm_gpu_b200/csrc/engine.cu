@@ -21,6 +21,7 @@
 #include "collide.cuh"
 #include "fe_internal.hpp"
 #include "kernels.cuh"
+#include "tracers.cuh"
 
 namespace fe {
 
@@ -551,12 +552,24 @@ struct Engine {
   }
 
   // download()/download_raw(): P1 (+BC) and P2 in output mode, no step.
-  template <class S, class Sh>
+  // OUT 1: reference site order; OUT 2: node-indexed grids.
+  template <class S, class Sh, int OUT>
   void fields_launch(FieldOut o) {
     k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
-    k_cfield<S, Sh, 1><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
+    k_cfield<S, Sh, OUT><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     launches += 2;
+  }
+  // Corrected velocity of the current state into node-indexed device grids
+  // (solid nodes are left as they are), on the engine stream.
+  int velocity_grid(double* ux, double* uy, double* uz) {
+    int rc;
+    if ((rc = set_ctl_mode(0, ff_manual))) return rc;
+    FieldOut o{nullptr, nullptr, ux, uy, uz, nullptr, nullptr};
+    FE_DISPATCH(*this, (fields_launch<S FE_COMMA Sh FE_COMMA 2>(o)));
+    FE_CUDA(cudaGetLastError());
+    double zero = 0.0;  // as fields(): the step recomputes lambda
+    return write_ctl_field(offsetof(Ctl, lambda), &zero, 8);
   }
   int fields(const fe_fields* f) {
     const int64_t n = hd.n;
@@ -567,7 +580,7 @@ struct Engine {
     if ((rc = set_ctl_mode(0, ff_manual))) return rc;
     FieldOut o{d_tmp + 0 * n, d_tmp + 1 * n, d_tmp + 2 * n, d_tmp + 3 * n, d_tmp + 4 * n, d_tmp + 5 * n,
                d_tmp + 6 * n};
-    FE_DISPATCH(*this, fields_launch<S FE_COMMA Sh>(o));
+    FE_DISPATCH(*this, (fields_launch<S FE_COMMA Sh FE_COMMA 1>(o)));
     FE_CUDA(cudaGetLastError());
     double* dst[7] = {f->rho, f->c, f->ux, f->uy, f->uz, f->p, f->mu};
     for (int q = 0; q < 7; ++q)
@@ -910,6 +923,107 @@ struct Batch {
     inflight = 0;
     FE_CUDA(cudaStreamSynchronize(stream));
     return finish(n);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Tracers of one engine (tracers.cuh): positions, diffusivities and ids on
+// the device, advected on a node-indexed snapshot of the engine's velocity.
+// ---------------------------------------------------------------------------
+struct Tracers {
+  Engine* E = nullptr;
+  TracerDesc T{};
+  std::vector<void*> allocs;
+  int velocity_skip = 1;
+  int64_t step = 0;             // tracer steps taken
+  bool have_u = false;
+  cudaStream_t stream = nullptr;
+
+  ~Tracers() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* a : allocs) cudaFree(a);
+  }
+  template <class T_>
+  int alloc(T_** p, size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T_)) != cudaSuccess) {
+      cudaGetLastError();
+      return fe_fail(FE_ERR_MEMORY, "tracer arrays");
+    }
+    allocs.push_back(q);
+    *p = static_cast<T_*>(q);
+    return FE_OK;
+  }
+  int create(Engine* e, const fe_tracer_config* cfg, int64_t n, const double* pos, const double* dm,
+             const int64_t* id) {
+    E = e;
+    stream = e->stream;
+    T.n = n;
+    T.nx = e->hd.nx;
+    T.ny = e->hd.ny;
+    T.nz = e->hd.nz;
+    T.substeps = cfg->substeps;
+    T.order = cfg->order;
+    T.seed = cfg->seed;
+    velocity_skip = cfg->velocity_skip > 0 ? cfg->velocity_skip : 1;
+    const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
+    double *p, *v, *d, *u;
+    int64_t* ids;
+    uint8_t* sol;
+    int rc;
+    if ((rc = alloc(&p, 3 * n)) || (rc = alloc(&v, 3 * n)) || (rc = alloc(&d, n)) || (rc = alloc(&ids, n)) ||
+        (rc = alloc(&u, 3 * nodes)) || (rc = alloc(&sol, nodes)))
+      return rc;
+    std::vector<uint8_t> solid(nodes, 1);
+    for (int64_t i = 0; i < e->hd.n; ++i) solid[e->L.node_of[i]] = 0;
+    for (int64_t q = 0; q < n; ++q) {
+      const int64_t x = (int64_t)std::floor(pos[q] + 0.5), y = (int64_t)std::floor(pos[n + q] + 0.5),
+                    z = (int64_t)std::floor(pos[2 * n + q] + 0.5);
+      if (pos[q] < 0 || pos[q] >= T.nx || pos[n + q] < 0 || pos[n + q] >= T.ny || pos[2 * n + q] < 0 ||
+          pos[2 * n + q] >= T.nz)
+        return fe_fail(FE_ERR_ARG, "tracer outside the lattice");
+      if (solid[(x % T.nx) + T.nx * ((y % T.ny) + (int64_t)T.ny * (z % T.nz))])
+        return fe_fail(FE_ERR_ARG, "tracer seeded on a solid node");
+      if (!(dm[q] >= 0.0)) return fe_fail(FE_ERR_ARG, "negative diffusivity");
+    }
+    std::vector<int64_t> idv(n);
+    for (int64_t q = 0; q < n; ++q) idv[q] = id ? id[q] : q;
+    FE_CUDA(cudaMemcpy(p, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemset(v, 0, 3 * n * sizeof(double)));
+    FE_CUDA(cudaMemcpy(d, dm, n * sizeof(double), cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemcpy(ids, idv.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    FE_CUDA(cudaMemset(u, 0, 3 * nodes * sizeof(double)));  // solid nodes stay 0
+    FE_CUDA(cudaMemcpy(sol, solid.data(), nodes, cudaMemcpyHostToDevice));
+    T.pos = p;
+    T.vel = v;
+    T.dm = d;
+    T.id = ids;
+    T.solid = sol;
+    for (int a = 0; a < 3; ++a) T.u[a] = u + a * nodes;
+    return FE_OK;
+  }
+  int refresh() {
+    double* u = const_cast<double*>(T.u[0]);
+    const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
+    int rc = E->velocity_grid(u, u + nodes, u + 2 * nodes);
+    if (!rc) have_u = true;
+    return rc;
+  }
+  // One lattice step of the tracers on the engine's current velocity.
+  int advance() {
+    int rc;
+    if (!have_u || step % velocity_skip == 0)
+      if ((rc = refresh())) return rc;
+    if (T.n > 0) k_tracers<<<(unsigned)((T.n + 127) / 128), 128, 0, stream>>>(T, step);
+    FE_CUDA(cudaGetLastError());
+    ++step;
+    return FE_OK;
+  }
+  int download(double* pos, double* vel) {
+    if (pos) FE_CUDA(cudaMemcpyAsync(pos, T.pos, 3 * T.n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (vel) FE_CUDA(cudaMemcpyAsync(vel, T.vel, 3 * T.n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
   }
 };
 
@@ -1370,6 +1484,45 @@ int fe_batch_time_run(fe_batch* b, int nsteps, float* ms) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return B.finish(nsteps);
+}
+
+// ---- tracers ---------------------------------------------------------------
+struct fe_tracers {
+  fe::Tracers t;
+};
+
+int fe_tracers_create(fe_engine* e, const fe_tracer_config* cfg, int64_t n, const double* pos, const double* dm,
+                      const int64_t* id, fe_tracers** out) {
+  FE_GUARD(e);
+  if (!cfg || !out || n < 0 || (n > 0 && (!pos || !dm))) return fe_fail(FE_ERR_ARG, "fe_tracers_create: bad arguments");
+  if (cfg->substeps < 1 || (cfg->order != 1 && cfg->order != 2))
+    return fe_fail(FE_ERR_ARG, "fe_tracers_create: substeps >= 1, order 1 or 2");
+  *out = nullptr;
+  fe_tracers* t = new (std::nothrow) fe_tracers();
+  if (!t) return fe_fail(FE_ERR_MEMORY, "host allocation");
+  const int rc = t->t.create(&e->e, cfg, n, pos, dm, id);
+  if (rc) {
+    delete t;
+    return rc;
+  }
+  *out = t;
+  return FE_OK;
+}
+
+int fe_tracers_destroy(fe_tracers* t) {
+  delete t;
+  return FE_OK;
+}
+
+int fe_tracers_step(fe_tracers* t) {
+  if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  if (t->t.E->owner && t->t.E->owner->inflight) return fe_fail(FE_ERR_STATE, "engine's batch steps in flight");
+  return t->t.advance();
+}
+
+int fe_tracers_download(fe_tracers* t, double* pos, double* vel) {
+  if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  return t->t.download(pos, vel);
 }
 
 int fe_batch_launch_count(const fe_batch* b, int64_t* count) {

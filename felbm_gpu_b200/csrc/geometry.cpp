@@ -436,4 +436,48 @@ int fe_init_equilibrium(int64_t n, const double* c, const double* p, const doubl
   return FE_OK;
 }
 
+// Tracer seeding (reference particles_init_mode volume / plane_xz with
+// particles_plane_offsets): uniform points whose nearest node is fluid, drawn
+// from one seeded stream; each plane resampled until its quota is reached.
+int fe_tracers_seed(const uint8_t* solid, int nx, int ny, int nz, int mode, int axis, const double* offsets,
+                    int nplanes, int64_t count, uint64_t seed, double* pos_out, int32_t* plane_out) {
+  if (!solid || !pos_out || !plane_out || nx < 1 || ny < 1 || nz < 1 || count < 0 || (mode != 0 && mode != 1) ||
+      (mode == 1 && (!offsets || nplanes < 1 || axis < 0 || axis > 2)))
+    return fe_fail(FE_ERR_ARG, "fe_tracers_seed: bad arguments");
+  const int N[3] = {nx, ny, nz};
+  int64_t fluid = 0;
+  for (int64_t q = 0; q < (int64_t)nx * ny * nz; ++q) fluid += solid[q] ? 0 : 1;
+  if (fluid == 0 && count > 0) return fe_fail(FE_ERR_ARG, "fe_tracers_seed: no fluid node");
+  const int planes = mode == 1 ? nplanes : 1;
+  const int64_t total = count * planes;
+  Rng rng(seed);
+  auto fluid_at = [&](const double* x) {
+    int64_t i[3];
+    for (int a = 0; a < 3; ++a) {
+      i[a] = (int64_t)std::floor(x[a] + 0.5) % N[a];
+      if (i[a] < 0) i[a] += N[a];
+    }
+    return solid[i[0] + (int64_t)nx * (i[1] + (int64_t)ny * i[2])] == 0;
+  };
+  int64_t k = 0;
+  for (int pl = 0; pl < planes; ++pl) {
+    int64_t got = 0, tries = 0;
+    while (got < count) {
+      if (++tries > 1000 * (count + 1000)) return fe_fail(FE_ERR_ARG, "fe_tracers_seed: plane has no fluid");
+      double x[3];
+      for (int a = 0; a < 3; ++a) x[a] = N[a] > 1 ? rng.uniform() * N[a] : 0.0;
+      if (mode == 1) {
+        double c = std::fmod(offsets[pl], (double)N[axis]);
+        x[axis] = c < 0 ? c + N[axis] : c;
+      }
+      if (!fluid_at(x)) continue;
+      for (int a = 0; a < 3; ++a) pos_out[a * total + k] = x[a];
+      plane_out[k] = mode == 1 ? pl : 0;
+      ++k;
+      ++got;
+    }
+  }
+  return FE_OK;
+}
+
 }  // extern "C"

@@ -512,11 +512,31 @@ __device__ __forceinline__ R lap_val(R f0, R fm, R fp, R bnd, bool hbb) {
 // correction (reference k_grad_cd_mf :897-913, k_pack_lap_c :159-165,
 // k_lap_mf :996-1010, k_mu_axpy :149-153, k_vel_press_corr :177-196).
 // Open-boundary nodes were resolved by k_bc_final: their mu, p are final.
-// OUT != 0: also write c, rho, u, p, mu in the reference site order (download).
+// OUT == 1: also write c, rho, u, p, mu in the reference site order (download);
+// OUT == 2: the same, indexed by node x + nx*(y + ny*z) (dense grids for tracers).
 // ---------------------------------------------------------------------------
 struct FieldOut {
-  double *rho, *c, *ux, *uy, *uz, *p, *mu;
+  double *rho, *c, *ux, *uy, *uz, *p, *mu;  // any may be null
+  __device__ __forceinline__ void put(int64_t q, double vc, double vrho, double vx, double vy, double vz, double vp,
+                                      double vmu) const {
+    if (c) c[q] = vc;
+    if (rho) rho[q] = vrho;
+    if (ux) ux[q] = vx;
+    if (uy) uy[q] = vy;
+    if (uz) uz[q] = vz;
+    if (p) p[q] = vp;
+    if (mu) mu[q] = vmu;
+  }
 };
+
+// Node index x + nx*(y + ny*z) of slot `slot` of brick `brick`.
+template <class Sh>
+__device__ __forceinline__ int64_t node_of(const LatDesc& D, int brick, int slot) {
+  const int x = D.brick_xyz[3 * brick + 0] * Sh::BX + (slot & (Sh::BX - 1));
+  const int y = D.brick_xyz[3 * brick + 1] * Sh::BY + ((slot >> Sh::LBX) & (Sh::BY - 1));
+  const int z = D.brick_xyz[3 * brick + 2] * Sh::BZ + (slot >> (Sh::LBX + Sh::LBY));
+  return x + (int64_t)D.nx * (y + (int64_t)D.ny * z);
+}
 
 template <class S, class Sh, int OUT>
 __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
@@ -555,13 +575,10 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
     if (flag & BC_SITE) {
       if (OUT) {
-        const int64_t q = D.ref_of[i];
+        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, s.slot_of[r]) : (int64_t)D.ref_of[i];
         const F* ub = static_cast<const F*>(D.u_bc);
-        out.c[q] = (double)c0;
-        out.rho[q] = (double)(rho1 + drho * c0);
-        out.ux[q] = (double)ub[i]; out.uy[q] = (double)ub[D.n + i]; out.uz[q] = (double)ub[2 * D.n + i];
-        out.p[q] = (double)fp[i];
-        out.mu[q] = (double) static_cast<const F*>(D.mu)[i];
+        out.put(q, (double)c0, (double)(rho1 + drho * c0), (double)ub[i], (double)ub[D.n + i],
+                (double)ub[2 * D.n + i], (double)fp[i], (double) static_cast<const F*>(D.mu)[i]);
       }
       continue;  // fields resolved by the open-boundary kernels
     }
@@ -593,14 +610,8 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
       const R p = (R)fp[i] + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
       if (Pm.drho != 0.0) fp[i] = (F)p;
       if (OUT) {
-        const int64_t q = D.ref_of[i];
-        out.c[q] = (double)c0;
-        out.rho[q] = (double)rho;
-        out.ux[q] = (double)ux;
-        out.uy[q] = (double)uy;
-        out.uz[q] = (double)uz;
-        out.p[q] = (double)p;
-        out.mu[q] = (double)mu;
+        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, s.slot_of[r]) : (int64_t)D.ref_of[i];
+        out.put(q, (double)c0, (double)rho, (double)ux, (double)uy, (double)uz, (double)p, (double)mu);
       }
     }
   }

@@ -1,0 +1,157 @@
+// Passive tracers on the GPU (the reference's host ParticleManager, driven at
+// felbm_gpu_main.cu:421-581,752-777; its felbm_local source is not available,
+// so the integrator below is this library's definition):
+//  * velocity: trilinear interpolation, with periodic wrap, of a node-indexed
+//    snapshot of the corrected velocity (solid nodes hold 0). As in the
+//    reference driver, which writes the same snapshot into its current and
+//    next arrays (felbm_gpu_main.cu:466-481), the velocity is constant over a
+//    step; the snapshot is refreshed every velocity_skip steps;
+//  * advection: `substeps` substeps of dt = 1/substeps per lattice step,
+//    explicit Euler (order 1) or Heun's trapezoid (order 2);
+//  * diffusion: per tracer molecular diffusivity Dm, a kick sqrt(2 Dm dt) N(0,1)
+//    per axis and substep; no kick along z in a 2-D lattice (nz == 1,
+//    reference README "2D runs"); Dm == 0 draws no random numbers;
+//  * random numbers: Philox4x32-10 (Salmon et al., SC'11, "Parallel random
+//    numbers: as easy as 1, 2, 3"), counter (tracer id, step, substep, draw),
+//    key = the 64-bit seed, so a trajectory does not depend on the thread
+//    that computes it; normals by the Box-Muller transform of 53-bit
+//    uniforms;
+//  * walls: a substep whose end position's nearest node is solid is
+//    rejected (the tracer stays where it was for that substep).
+#pragma once
+#include <cstdint>
+
+namespace fe {
+
+struct TracerDesc {
+  int64_t n;                  // tracers
+  int nx, ny, nz;
+  int substeps, order;
+  uint64_t seed;
+  double* pos;                // [3][n]
+  double* vel;                // [3][n] interpolated velocity at the end of the step
+  const double* dm;           // [n]
+  const int64_t* id;          // [n]
+  const double* u[3];         // node-indexed velocity snapshot
+  const uint8_t* solid;       // [nodes]
+};
+
+// One Philox4x32-10 block: 10 rounds of two 32x32->64 multiplies, the key
+// bumped by the Weyl constants between rounds.
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)c[0] * 0xD2511F53u, p1 = (uint64_t)c[2] * 0xCD9E8D57u;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+// Two standard normals from one Philox block (Box-Muller on two uniforms of
+// 53 bits each; the first uniform is shifted into (0, 1]).
+__device__ __forceinline__ void normal_pair(uint64_t seed, int64_t id, int64_t step, int sub, int draw, double& z0,
+                                            double& z1) {
+  uint32_t c[4] = {(uint32_t)id, (uint32_t)((uint64_t)id >> 32), (uint32_t)step,
+                   (uint32_t)(sub * 2 + draw)};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const double inv53 = 1.0 / 9007199254740992.0;  // 2^-53
+  const double u1 = ((double)(((uint64_t)(c[0] >> 5) << 26) | (c[1] >> 6)) + 1.0) * inv53;
+  const double u2 = (double)(((uint64_t)(c[2] >> 5) << 26) | (c[3] >> 6)) * inv53;
+  const double r = sqrt(-2.0 * log(u1));
+  double sv, cv;
+  sincospi(2.0 * u2, &sv, &cv);
+  z0 = r * cv;
+  z1 = r * sv;
+}
+
+__device__ __forceinline__ double wrap(double x, int L) {
+  x = fmod(x, (double)L);
+  return x < 0.0 ? x + L : x;
+}
+
+// Trilinear interpolation of the velocity snapshot at a wrapped position.
+__device__ __forceinline__ void interp(const TracerDesc& T, double x, double y, double z, double v[3]) {
+  const double fx = floor(x), fy = floor(y), fz = floor(z);
+  const double ax = x - fx, ay = y - fy, az = z - fz;
+  const int x0 = (int)fx % T.nx, y0 = (int)fy % T.ny, z0 = (int)fz % T.nz;
+  const int x1 = (x0 + 1) % T.nx, y1 = (y0 + 1) % T.ny, z1 = (z0 + 1) % T.nz;
+  const int64_t sy = T.nx, sz = (int64_t)T.nx * T.ny;
+  const int64_t idx[8] = {x0 + y0 * sy + z0 * sz, x1 + y0 * sy + z0 * sz, x0 + y1 * sy + z0 * sz,
+                          x1 + y1 * sy + z0 * sz, x0 + y0 * sy + z1 * sz, x1 + y0 * sy + z1 * sz,
+                          x0 + y1 * sy + z1 * sz, x1 + y1 * sy + z1 * sz};
+  const double w[8] = {(1 - ax) * (1 - ay) * (1 - az), ax * (1 - ay) * (1 - az), (1 - ax) * ay * (1 - az),
+                       ax * ay * (1 - az),             (1 - ax) * (1 - ay) * az, ax * (1 - ay) * az,
+                       (1 - ax) * ay * az,             ax * ay * az};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += w[q] * T.u[a][idx[q]];
+    v[a] = s;
+  }
+}
+
+__device__ __forceinline__ bool blocked(const TracerDesc& T, double x, double y, double z) {
+  const int ix = (int)floor(x + 0.5) % T.nx, iy = (int)floor(y + 0.5) % T.ny, iz = (int)floor(z + 0.5) % T.nz;
+  return T.solid[ix + (int64_t)T.nx * (iy + (int64_t)T.ny * iz)] != 0;
+}
+
+// One lattice step of every tracer (step = the tracer step counter).
+__global__ void k_tracers(TracerDesc T, int64_t step) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= T.n) return;
+  double x = T.pos[p], y = T.pos[T.n + p], z = T.pos[2 * T.n + p];
+  const double dm = T.dm[p];
+  const int64_t id = T.id[p];
+  const double dt = 1.0 / T.substeps;
+  const double kick = dm > 0.0 ? sqrt(2.0 * dm * dt) : 0.0;
+  for (int s = 0; s < T.substeps; ++s) {
+    double k1[3], nx, ny, nz;
+    interp(T, x, y, z, k1);
+    if (T.order == 1) {
+      nx = x + dt * k1[0];
+      ny = y + dt * k1[1];
+      nz = z + dt * k1[2];
+    } else {
+      double k2[3];
+      interp(T, wrap(x + dt * k1[0], T.nx), wrap(y + dt * k1[1], T.ny), wrap(z + dt * k1[2], T.nz), k2);
+      nx = x + 0.5 * dt * (k1[0] + k2[0]);
+      ny = y + 0.5 * dt * (k1[1] + k2[1]);
+      nz = z + 0.5 * dt * (k1[2] + k2[2]);
+    }
+    if (kick > 0.0) {
+      double g0, g1, g2, g3;
+      normal_pair(T.seed, id, step, s, 0, g0, g1);
+      nx += kick * g0;
+      ny += kick * g1;
+      if (T.nz > 1) {
+        normal_pair(T.seed, id, step, s, 1, g2, g3);
+        nz += kick * g2;
+      }
+    }
+    nx = wrap(nx, T.nx);
+    ny = wrap(ny, T.ny);
+    nz = wrap(nz, T.nz);
+    if (!blocked(T, nx, ny, nz)) {
+      x = nx;
+      y = ny;
+      z = nz;
+    }
+  }
+  T.pos[p] = x;
+  T.pos[T.n + p] = y;
+  T.pos[2 * T.n + p] = z;
+  double v[3];
+  interp(T, x, y, z, v);
+  T.vel[p] = v[0];
+  T.vel[T.n + p] = v[1];
+  T.vel[2 * T.n + p] = v[2];
+}
+
+}  // namespace fe

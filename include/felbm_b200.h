@@ -356,6 +356,44 @@ int fe_server_get_stats(fe_server* s, fe_server_stats* st);
 /* Stops the loop (active solves are dropped) and frees everything. */
 int fe_server_destroy(fe_server* s);
 
+/* ---- tracers ---------------------------------------------------------------
+ * Replace the reference's host ParticleManager path (felbm_gpu_main.cu:
+ * 421-581, 752-777: velocity copied to the host and scattered every step).
+ * Here tracers live on the GPU beside their engine. fe_tracers_step advances
+ * them one lattice step on the engine's current corrected velocity
+ * (trilinear interpolation of a node-indexed snapshot refreshed every
+ * velocity_skip steps, the reference's particles_velocity_skip), with
+ * `substeps` Euler (order 1) or Heun (order 2) substeps, a Brownian kick
+ * sqrt(2 Dm dt) N(0,1) per axis from a counter-based Philox4x32-10 stream
+ * keyed by seed and tracer id (none along z in a 2-D lattice; Dm = 0 draws
+ * nothing), and moves onto solid nodes rejected. Call it after each engine
+ * step, as the reference driver calls pm.update(). Positions are node
+ * coordinates, periodic, [3][n] (all x, then y, then z). Tracers use their
+ * engine's stream and must be destroyed before it. */
+typedef struct fe_tracers fe_tracers;
+typedef struct fe_tracer_config {
+  int substeps;               /* >= 1 */
+  int order;                  /* 1 or 2 */
+  int velocity_skip;          /* refresh the velocity every this many steps */
+  uint64_t seed;
+} fe_tracer_config;
+/* n tracers at pos [3][n] with diffusivities dm [n] and ids [n] (NULL: 0..n-1;
+ * the random stream of a tracer depends on its id). */
+int fe_tracers_create(fe_engine* e, const fe_tracer_config* cfg, int64_t n, const double* pos,
+                      const double* dm, const int64_t* id, fe_tracers** out);
+int fe_tracers_destroy(fe_tracers* t);
+int fe_tracers_step(fe_tracers* t);
+/* pos, vel: [3][n] host arrays (either may be NULL); vel is the velocity
+ * interpolated at each tracer's position at the end of the last step. */
+int fe_tracers_download(fe_tracers* t, double* pos, double* vel);
+/* Seeding (reference particles_init_mode): mode 0 uniform in the fluid
+ * volume (count tracers); mode 1 planes normal to `axis` at the coordinates
+ * offsets[0..nplanes-1], count tracers per plane, each plane resampled until
+ * its quota of non-solid points is reached. pos_out [3][total],
+ * plane_out [total] (plane index, or 0 for mode 0). */
+int fe_tracers_seed(const uint8_t* solid, int nx, int ny, int nz, int mode, int axis, const double* offsets,
+                    int nplanes, int64_t count, uint64_t seed, double* pos_out, int32_t* plane_out);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* Time nsteps of fe_run with CUDA events on the engine's stream; ms_total is
  * the device time. */
