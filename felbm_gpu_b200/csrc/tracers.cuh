@@ -10,7 +10,8 @@
 //    explicit Euler (order 1) or Heun's trapezoid (order 2);
 //  * diffusion: per tracer molecular diffusivity Dm, a kick sqrt(2 Dm dt) N(0,1)
 //    per axis and substep; no kick along z in a 2-D lattice (nz == 1,
-//    reference README "2D runs"); Dm == 0 draws no random numbers;
+//    reference README "2D runs"), where tracers do not move along z at all;
+//    Dm == 0 draws no random numbers;
 //  * random numbers: Philox4x32-10 (Salmon et al., SC'11, "Parallel random
 //    numbers: as easy as 1, 2, 3"), counter (tracer id, step, substep, draw),
 //    key = the 64-bit seed, so a trajectory does not depend on the thread
@@ -70,9 +71,11 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, int64_t id, int64_t s
   z1 = r * sv;
 }
 
+// Periodic wrap into [0, L) (a tiny negative x would round to L itself).
 __device__ __forceinline__ double wrap(double x, int L) {
   x = fmod(x, (double)L);
-  return x < 0.0 ? x + L : x;
+  if (x < 0.0) x += L;
+  return x >= L ? x - L : x;
 }
 
 // Trilinear interpolation of the velocity snapshot at a wrapped position.
@@ -137,7 +140,7 @@ __global__ void k_tracers(TracerDesc T, int64_t step) {
     }
     nx = wrap(nx, T.nx);
     ny = wrap(ny, T.ny);
-    nz = wrap(nz, T.nz);
+    nz = T.nz > 1 ? wrap(nz, T.nz) : z;  // a 2-D lattice: no motion along z
     if (!blocked(T, nx, ny, nz)) {
       x = nx;
       y = ny;

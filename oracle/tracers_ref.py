@@ -7,7 +7,8 @@ once here): trilinear interpolation of a node-indexed velocity snapshot with
 periodic wrap, Euler or Heun substeps, Brownian kicks sqrt(2 Dm dt) N(0,1)
 from Philox4x32-10 (Salmon et al. 2011) with counter (id, step, substep,
 draw) and the seed as key, Box-Muller normals from 53-bit uniforms, no z kick
-in 2-D, moves onto solid nodes rejected.
+in 2-D (where tracers do not move along z at all), moves onto solid nodes
+rejected.
 """
 from __future__ import annotations
 
@@ -59,7 +60,8 @@ def velocity_grid(shape, nodes: np.ndarray, ux, uy, uz) -> np.ndarray:
 
 def _wrap(x, L):
     x = np.fmod(x, L)
-    return np.where(x < 0.0, x + L, x)
+    x = np.where(x < 0.0, x + L, x)
+    return np.where(x >= L, x - L, x)
 
 
 def interp(u, shape, x, y, z):
@@ -115,7 +117,8 @@ def step(pos, dm, ids, u, solid, step_index: int, substeps: int = 1, order: int 
             if nz > 1:
                 g2, _ = normal_pair(seed, ids, step_index, s, 1)
                 nzp = np.where(move, nzp + kick * g2, nzp)
-        nxp, nyp, nzp = _wrap(nxp, nx), _wrap(nyp, ny), _wrap(nzp, nz)
+        nxp, nyp = _wrap(nxp, nx), _wrap(nyp, ny)
+        nzp = _wrap(nzp, nz) if nz > 1 else z  # 2-D: no motion along z
         ok = ~blocked(sf, shape, nxp, nyp, nzp)
         x, y, z = np.where(ok, nxp, x), np.where(ok, nyp, y), np.where(ok, nzp, z)
     vel = interp(u, shape, x, y, z)

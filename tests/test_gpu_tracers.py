@@ -1,0 +1,115 @@
+"""GPU tracers against the CPU restatement. The workload's bar: zero-
+diffusivity trajectories to 1e-10 in FP64 against the FP64 oracle (here the
+whole chain: CPU-oracle flow + numpy tracers vs engine + GPU tracers);
+diffusive tracers match the restatement step for step on the engine's own
+velocity (same Philox stream), and their dispersion matches 2 Dm t."""
+import numpy as np
+import pytest
+
+from cases import make_case
+from felbm_gpu_b200 import MultiPhaseGPU, geometry
+from felbm_gpu_b200.tracers import Tracers, seed
+from oracle import tracers_ref as tr
+from oracle.oracle_py import Oracle
+from parity import with_storage
+
+pytestmark = pytest.mark.gpu
+
+
+def flow_case(name="spheres_mrt"):
+    # a stronger body force than the parity case, so tracers move
+    return make_case(name, gx=2e-4) if name != "cyl2d_mrt" else make_case(name)
+
+
+def grid(solid, f):
+    nodes = geometry.site_nodes(solid)
+    return tr.velocity_grid(solid.shape, nodes, f["ux"], f["uy"], f["uz"])
+
+
+@pytest.mark.parametrize("order,substeps", [(2, 2), (1, 1)])
+def test_tracers_match_restatement_on_engine_velocity(require_gpu, order, substeps):
+    case = flow_case()
+    e = MultiPhaseGPU(with_storage(case.params, "f64"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        pos0, pid = seed(case.solid, 200, rng_seed=5)
+        dm = np.where(np.arange(200) % 2 == 0, 0.0, 1e-3)
+        ids = np.arange(200) + 1000
+        t = Tracers(e, pos0, dm, ids=ids, substeps=substeps, order=order, rng_seed=99)
+        pos = pos0.copy()
+        for s in range(30):
+            e.run(1)
+            t.step()
+            u = grid(case.solid, e.download())
+            pos, vel = tr.step(pos, dm, ids, u, case.solid, s, substeps=substeps, order=order, seed=99)
+        gp, gv = t.download()
+        t.free()
+    finally:
+        e.free()
+    assert np.max(np.abs(gp - pos)) <= 1e-10, np.max(np.abs(gp - pos))
+    assert np.max(np.abs(gv - vel)) <= 1e-12
+    assert np.max(np.abs(pos - pos0)) > 1e-3       # they moved
+
+
+def test_zero_diffusivity_trajectories_match_fp64_oracle(require_gpu):
+    """The full chain in FP64: oracle flow + restated tracers vs engine +
+    GPU tracers, Dm = 0, 40 steps, <= 1e-10 (the workload's bound)."""
+    case = flow_case()
+    o = Oracle(case.params, case.solid)
+    o.upload_state(case.h0, case.g0)
+    e = MultiPhaseGPU(with_storage(case.params, "f64"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        pos0, _ = seed(case.solid, 300, rng_seed=9)
+        t = Tracers(e, pos0, 0.0, substeps=2, order=2)
+        pos = pos0.copy()
+        ids = np.arange(300)
+        for s in range(40):
+            e.run(1)
+            t.step()
+            o.step(1)
+            pos, _ = tr.step(pos, np.zeros(300), ids, grid(case.solid, o.download()), case.solid, s, substeps=2)
+        gp, _ = t.download()
+        t.free()
+    finally:
+        e.free()
+    assert np.max(np.abs(gp - pos)) <= 1e-10, np.max(np.abs(gp - pos))
+
+
+def test_dispersion_statistics(require_gpu):
+    """All fluid, no flow: variance 2 Dm t per axis (95 % band); 2-D lattices
+    get no z motion."""
+    solid = np.zeros((24, 24, 24), np.uint8)
+    case = make_case("fluid_bgk")
+    e = MultiPhaseGPU(with_storage(case.params, "f64"), solid)
+    c = np.full(int(solid.size), 0.5)
+    h0, g0 = geometry.equilibrium(c, 1.0, case.params.rho0, case.params.rho0)
+    try:
+        e.upload_state(h0, g0)
+        n, dm, steps = 20000, 0.05, 30
+        t = Tracers(e, np.full((3, n), 12.0), dm, substeps=2, rng_seed=4)
+        for _ in range(steps):
+            t.step()          # the state is at rest: velocity ~ 0
+        p, _ = t.download()
+        t.free()
+    finally:
+        e.free()
+    var = ((p - 12.0) ** 2).mean(axis=1)
+    assert np.all(np.abs(var / (2 * dm * steps) - 1.0) < 2.8 * np.sqrt(2.0 / n)), var
+
+
+def test_2d_tracers_stay_in_plane(require_gpu):
+    case = make_case("cyl2d_mrt")
+    e = MultiPhaseGPU(with_storage(case.params, "f32"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        pos0, _ = seed(case.solid, 100, rng_seed=2)
+        t = Tracers(e, pos0, 0.01, rng_seed=3)
+        for _ in range(10):
+            e.run(1)
+            t.step()
+        p, _ = t.download()
+        t.free()
+    finally:
+        e.free()
+    assert np.all(p[2] == 0.0) and np.max(np.abs(p[:2] - pos0[:2])) > 0
