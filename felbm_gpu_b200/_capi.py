@@ -159,6 +159,14 @@ SIGNATURES = {
     "fe_tracers_download": (C.c_int, [_vp, _dp, _dp]),
     "fe_tracers_seed": (C.c_int, [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int64,
                                   C.c_uint64, _dp, _i32p]),
+    "fe_write_fields_h5": (C.c_int, [_vp, C.c_char_p, C.c_int]),
+    "fe_write_geometry_h5": (C.c_int, [C.c_char_p, _u8p, C.c_int, C.c_int, C.c_int]),
+    "fe_checkpoint_write": (C.c_int, [_vp, C.c_char_p, C.c_uint32]),
+    "fe_settle_mass_correction": (C.c_int, [_vp]),
+    "fe_checkpoint_read": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_uint32)]),
+    "fe_write_particles_h5": (C.c_int, [C.c_char_p, C.c_int64, _dp, _dp, _i64p, _dp, _i32p]),
+    "fe_h5_read_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _i64p, C.POINTER(C.c_int),
+                                     C.c_void_p, C.c_int64]),
     "fe_server_create": (C.c_int, [C.POINTER(FeServerConfig), C.POINTER(C.c_void_p)]),
     "fe_server_submit": (C.c_int, [_vp, C.POINTER(FeRequest)]),
     "fe_server_poll": (C.c_int, [_vp, C.POINTER(FeResult), C.c_int, C.POINTER(C.c_int)]),

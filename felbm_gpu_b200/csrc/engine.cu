@@ -535,6 +535,23 @@ struct Engine {
     return FE_OK;
   }
 
+  // A queued mass correction written into the stored h now (instead of at
+  // the next pass); the queue is then empty.
+  int settle_correction() {
+    Ctl c;
+    int rc;
+    if ((rc = read_ctl(&c))) return rc;
+    if (!c.pending || !hd.prm.correct_mass) return FE_OK;
+    if ((rc = mass_pass())) return rc;
+    FE_DISPATCH(*this, (k_inject<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity)));
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    struct { int32_t pending; } z{0};
+    if ((rc = write_ctl_field(offsetof(Ctl, pending), &z, 4))) return rc;
+    double zero = 0.0;
+    return write_ctl_field(offsetof(Ctl, lambda), &zero, 8);
+  }
+
   int upload(const double* h, const double* g) {
     const int64_t Vn = (int64_t)Q * hd.n;
     int rc;
@@ -1271,6 +1288,11 @@ int fe_apply_mass_correction(fe_engine* e, double* drift) {
   if ((rc = E.read_ctl(&c))) return rc;
   *drift = c.drift;
   return FE_OK;
+}
+
+int fe_settle_mass_correction(fe_engine* e) {
+  FE_GUARD(e);
+  return e->e.settle_correction();
 }
 
 int fe_record_target_mass(fe_engine* e) {

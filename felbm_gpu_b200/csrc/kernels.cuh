@@ -848,6 +848,43 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
   }
 }
 
+// A queued mass correction written into the stored h (the reference's
+// k_inject_mass, device_engine.cuh:1128-1139), with the arithmetic of
+// k_download_state's injection, so the stored state becomes what a download
+// returns; lambda from ctl (formed by k_mass).
+template <class S>
+__global__ void __launch_bounds__(CTA) k_inject(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                 int parity) {
+  using R = typename S::real;
+  using P = typename S::pop;
+  const int2 wk = work[blockIdx.x];
+  const LatDesc& D = descs[wk.x];
+  P* h = static_cast<P*>(D.pop[parity][0]);
+  const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
+  const double lambda = D.ctl->lambda;
+  if (lambda == 0.0) return;
+  const int64_t n = D.n, i0 = (int64_t)wk.y * CHUNK;
+  const int64_t iend = i0 + CHUNK < n ? i0 + CHUNK : n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
+    const int64_t a = pbase(i);
+    R hv[Q];
+    double cd = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      hv[k] = ld_pop<S>(h, a + k * AOSOA, k, shh);
+      cd += (double)hv[k];
+    }
+    const double phi = cd * (1.0 - cd);
+    if (!(phi > 0.0)) continue;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      R v = hv[k];
+      v += (R)(weight<double>(k) * (-lambda * phi));
+      st_pop<S>(h, a + k * AOSOA, k, v, shh);
+    }
+  }
+}
+
 // Post-stream state from the reference layout (reference upload_state,
 // multiphase_gpu.cuh:354-359).
 template <class S>

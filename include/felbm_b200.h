@@ -394,6 +394,34 @@ int fe_tracers_download(fe_tracers* t, double* pos, double* vel);
 int fe_tracers_seed(const uint8_t* solid, int nx, int ny, int nz, int mode, int axis, const double* offsets,
                     int nplanes, int64_t count, uint64_t seed, double* pos_out, int32_t* plane_out);
 
+/* ---- files ----------------------------------------------------------------
+ * The reference driver's on-disk formats (felbm_gpu_main.cu:86-189), HDF5
+ * with the same dataset names, shapes and types, written without libhdf5
+ * (contiguous datasets, no gzip). Fields of the current state (refreshed as
+ * fe_download_fields): density, concentration, u_x, u_y, u_z, pressure, n
+ * values each in the reference order, float32 or float64. */
+int fe_write_fields_h5(fe_engine* e, const char* path, int float32);
+/* geometry.h5: coords [n][3] int (x, y, z of each site) and size [3] int. */
+int fe_write_geometry_h5(const char* path, const uint8_t* solid, int nx, int ny, int nz);
+/* Checkpoint (write_checkpoint / read_checkpoint, :151-189): h, g (Vn
+ * doubles), step (uint), target_mass, Vn (int). Reading refuses a Vn that
+ * differs from the engine's, uploads the state and keeps the file's M0. */
+int fe_checkpoint_write(fe_engine* e, const char* path, uint32_t step);
+/* Writes a queued mass correction into the stored populations now, where
+ * it would otherwise be applied at the next step (the state is then what
+ * fe_download_state returns). fe_checkpoint_write calls it first, so the run
+ * that continues and a restart from the file hold the same state. */
+int fe_settle_mass_correction(fe_engine* e);
+int fe_checkpoint_read(fe_engine* e, const char* path, uint32_t* step);
+/* particles_<step>.h5: position [n][3], velocity [n][3] (if vel), id, Dm (if
+ * dm), plane_id (if plane_id); pos and vel as [3][n] (fe_tracers_download). */
+int fe_write_particles_h5(const char* path, int64_t n, const double* pos, const double* vel, const int64_t* id,
+                          const double* dm, const int32_t* plane_id);
+/* One dataset of a file written here: type 0 double, 1 float, 2 int32,
+ * 3 uint32; dims[rank]; raw bytes into data (NULL: shape only). */
+int fe_h5_read_dataset(const char* path, const char* name, int* type, int64_t* dims, int* rank, void* data,
+                       int64_t capacity_bytes);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* Time nsteps of fe_run with CUDA events on the engine's stream; ms_total is
  * the device time. */

@@ -1,0 +1,94 @@
+"""HDF5 files without a GPU: geometry and particle files round-trip through
+the library's reader, and the bytes follow the HDF5 file-format
+specification's structures (checked here by an independent parse: superblock
+version 0, end-of-file address, root symbol table with its B-tree, local heap
+and symbol-table node, names sorted, version-1 dataset object headers with
+dataspace, datatype and contiguous layout messages)."""
+import os
+
+import numpy as np
+
+from felbm_gpu_b200 import files, geometry
+
+
+def test_geometry_round_trip(tmp_path):
+    solid = geometry.spheres((10, 12, 14), 2.5, 4, 2.0, 3)
+    p = str(tmp_path / "geometry.h5")
+    files.write_geometry(p, solid)
+    coords = files.read_dataset(p, "coords")
+    nodes = geometry.site_nodes(solid)
+    nz, ny, nx = solid.shape
+    want = np.stack([nodes % nx, (nodes // nx) % ny, nodes // (nx * ny)], axis=1)
+    assert coords.dtype == np.int32 and np.array_equal(coords, want)
+    assert np.array_equal(files.read_dataset(p, "size"), want.max(axis=0) + 1)
+
+
+def test_particles_round_trip(tmp_path):
+    rng = np.random.default_rng(0)
+    n = 37
+    pos, vel = rng.random((3, n)), rng.random((3, n))
+    ids, dm, pid = np.arange(n) + 5, rng.random(n), np.arange(n, dtype=np.int32) % 2
+    p = str(tmp_path / "particles_10.h5")
+    files.write_particles(p, pos, vel, ids, dm, pid)
+    assert np.array_equal(files.read_dataset(p, "position"), pos.T)
+    assert np.array_equal(files.read_dataset(p, "velocity"), vel.T)
+    assert np.array_equal(files.read_dataset(p, "id"), ids)
+    assert np.array_equal(files.read_dataset(p, "Dm"), dm)
+    assert np.array_equal(files.read_dataset(p, "plane_id"), pid)
+
+
+def _u(b, off, n):
+    return int.from_bytes(b[off:off + n], "little")
+
+
+def test_structure_follows_the_specification(tmp_path):
+    p = str(tmp_path / "particles_1.h5")
+    files.write_particles(p, np.zeros((3, 4)), None, None, np.ones(4), None)
+    b = open(p, "rb").read()
+    assert b[:8] == b"\x89HDF\r\n\x1a\n" and b[8] == 0            # superblock version 0
+    assert b[13] == 8 and b[14] == 8                               # offsets / lengths
+    assert _u(b, 40, 8) == len(b)                                  # end-of-file address
+    assert _u(b, 32, 8) == 2 ** 64 - 1 == _u(b, 48, 8)             # undefined addresses
+    root, btree, heap = _u(b, 64, 8), _u(b, 80, 8), _u(b, 88, 8)
+    assert _u(b, 72, 4) == 1                                       # cached symbol table
+    assert b[root] == 1 and _u(b, root + 16, 2) == 0x0011          # v1 header: symbol-table message
+    assert (_u(b, root + 24, 8), _u(b, root + 32, 8)) == (btree, heap)
+    assert b[heap:heap + 4] == b"HEAP" and b[btree:btree + 4] == b"TREE"
+    data = _u(b, heap + 24, 8)
+    assert b[data] == 0                                            # offset 0: the empty name
+    snod = _u(b, btree + 32, 8)
+    assert b[snod:snod + 4] == b"SNOD" and b[snod + 4] == 1
+    nsym = _u(b, snod + 6, 2)
+    names = []
+    for s in range(nsym):
+        e = snod + 8 + 40 * s
+        off = _u(b, e, 8)
+        names.append(b[data + off:b.index(b"\0", data + off)].decode())
+        oh = _u(b, e + 8, 8)
+        assert b[oh] == 1 and oh % 8 == 0
+        types = []
+        q = oh + 16
+        for _ in range(_u(b, oh + 2, 2)):
+            types.append(_u(b, q, 2))
+            assert _u(b, q + 2, 2) % 8 == 0
+            q += 8 + _u(b, q + 2, 2)
+        assert types == [0x0001, 0x0003, 0x0005, 0x0008]
+    assert names == sorted(names) == ["Dm", "id", "position"]
+    # the key after the child is the last name
+    assert _u(b, btree + 40, 8) == _u(b, snod + 8 + 40 * (nsym - 1), 8)
+    dm_oh = _u(b, snod + 8 + 8, 8)                                 # "Dm" sorts first
+    # datatype of Dm: IEEE little-endian double (class 1, size 8, bias 1023)
+    q = dm_oh + 16
+    q += 8 + _u(b, q + 2, 2)                                       # skip the dataspace
+    assert b[q + 8] & 0x0F == 1 and _u(b, q + 12, 4) == 8 and _u(b, q + 8 + 16, 4) == 1023
+    os.remove(p)
+
+
+def test_reader_rejects_other_files(tmp_path):
+    p = str(tmp_path / "x.h5")
+    open(p, "wb").write(b"not hdf5" * 40)
+    try:
+        files.read_dataset(p, "a")
+        raise AssertionError("no error")
+    except Exception as ex:
+        assert "not an HDF5 file" in str(ex)
