@@ -81,10 +81,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   using F = typename S::fld;
   using T = Tile<Sh, 2>;
   using SM = CollideSmem<Sh, R>;
-  constexpr int ROWS4 = T::TY * T::TZ * 4;
-  __shared__ Pro<Sh> s;
-  __shared__ uint32_t s_rbits[ROWS4];
-  __shared__ int32_t s_rbase[ROWS4];
+  __shared__ Head<Sh> s;
   extern __shared__ __align__(16) unsigned char dsm[];
   int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
   R* s_c = reinterpret_cast<R*>(dsm + SM::NT16);
@@ -94,10 +91,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
-  // the prologue's barriers publish the record and masks that the index
-  // tile reads; the tile builder ends with a barrier
-  prologue<Sh, P4T>(D, brick, s);
-  build_idx_tile<Sh, 2, P4T>(s, s_idx, s_rbits, s_rbase);
+  load_brick<Sh, 2, P4T>(D, brick, s, s_idx);
   {
     const F* const src[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
                              static_cast<const F*>(D.lapmu)};
@@ -121,7 +115,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   const Shift shg{(float)Pm.p_ref, (float)(1.0 / Pm.g_scale), (float)Pm.g_scale};
   double st[6] = {0, 0, 0, 0, 0, 0};
   int bad = 0;
-  const int first = s.rec.first, cnt = s.rec.cnt;
+  const int first = s.first, cnt = s.cnt;
 
   for (int r = threadIdx.x; r < cnt; r += P4T) {
     const int64_t i = first + r;

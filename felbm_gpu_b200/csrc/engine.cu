@@ -354,7 +354,30 @@ struct Engine {
     if (rc) return rc;
     FE_CUDA(cudaMallocHost(&h_stats, 6 * sizeof(double)));
     FE_CUDA(cudaEventCreateWithFlags(&ev_stats, cudaEventDisableTiming));
-    return upload_desc();
+    FE_DISPATCH(*this, rc = alloc_tiles<Sh>());
+    if (rc) return rc;
+    if ((rc = upload_desc())) return rc;
+    FE_DISPATCH(*this, (k_build_tiles<Sh><<<nbk, CTA, 0, stream>>>(d_desc, d_work)));
+    FE_CUDA(cudaGetLastError());
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+
+  // Site-index tiles (halo 2 and 1) and slot lists of every brick, built
+  // once on the device by k_build_tiles and read by the stencil passes.
+  template <class Sh>
+  int alloc_tiles() {
+    int32_t *t2, *t1;
+    uint16_t* sl;
+    const size_t nbk = (size_t)hd.nbricks;
+    int rc;
+    if ((rc = alloc(&t2, nbk * Tile<Sh, 2>::N)) || (rc = alloc(&t1, nbk * Tile<Sh, 1>::N)) ||
+        (rc = alloc(&sl, nbk * Sh::C)))
+      return rc;
+    hd.tile2 = t2;
+    hd.tile1 = t1;
+    hd.slots = sl;
+    return FE_OK;
   }
 
   // Dynamic shared memory of the collide pass (CollideSmem).

@@ -177,8 +177,8 @@ __device__ __forceinline__ double forcing_factor_dev(const DevPrm& P, const Ctl&
 
 // The step scalars of the lattice's control block into the prologue state
 // (called by one thread).
-template <class Sh>
-__device__ __forceinline__ void load_step_scalars(const LatDesc& D, Pro<Sh>& s) {
+template <class SMem>
+__device__ __forceinline__ void load_step_scalars(const LatDesc& D, SMem& s) {
   {
     const Ctl& C = *D.ctl;
     s.ff = (float)forcing_factor_dev(D.prm, C);
@@ -205,7 +205,7 @@ __device__ __forceinline__ void prologue(const LatDesc& D, int brick, Pro<Sh>& s
     static_assert(N4 <= NT - 32, "the record is copied by the leading warps");
     if (tid < N4) dst[tid] = __ldg(src + tid);
     // the step scalars load in parallel, from the last warp
-    if (SCALARS && tid == NT - 1) load_step_scalars<Sh>(D, s);
+    if (SCALARS && tid == NT - 1) load_step_scalars(D, s);
   }
   __syncthreads();
   for (int q = tid; q < 64 * Sh::W; q += NT) {
@@ -270,6 +270,61 @@ struct IdxTile {
   uint32_t rbits[T::TY * T::TZ * 4];
   int32_t rbase[T::TY * T::TZ * 4];
 };
+
+// Per-CTA head of the stencil passes: the brick's fluid slots in site order,
+// its site range and the step scalars.
+template <class Sh>
+struct alignas(16) Head {
+  uint16_t slot_of[Sh::C];
+  double lambda;
+  float ff;
+  int first, cnt;
+};
+
+// The brick's head and its halo-H site-index tile, precomputed once by
+// k_build_tiles (the geometry is static), in one phase of independent
+// coalesced loads; ends with a barrier. s_idx must be 16-byte aligned.
+template <class Sh, int H, int NT = CTA, bool SCALARS = true>
+__device__ __forceinline__ void load_brick(const LatDesc& D, int brick, Head<Sh>& s, int32_t* __restrict__ s_idx) {
+  using T = Tile<Sh, H>;
+  static_assert(T::N % 4 == 0 && Sh::C % 8 == 0, "16-byte rows");
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s.first = __ldg(&D.rec[brick].first);
+    s.cnt = __ldg(&D.rec[brick].cnt);
+  }
+  if (SCALARS && tid == NT - 1) load_step_scalars(D, s);
+  const int4* src = reinterpret_cast<const int4*>(H == 2 ? D.tile2 : D.tile1) + (int64_t)brick * (T::N / 4);
+  int4* dst = reinterpret_cast<int4*>(s_idx);
+  for (int q = tid; q < T::N / 4; q += NT) dst[q] = __ldg(src + q);
+  const uint4* ss = reinterpret_cast<const uint4*>(D.slots) + (int64_t)brick * (Sh::C / 8);
+  uint4* sd = reinterpret_cast<uint4*>(s.slot_of);
+  for (int q = tid; q < Sh::C / 8; q += NT) sd[q] = __ldg(ss + q);
+  __syncthreads();
+}
+
+// Setup: the site-index tiles (halo 2 and halo 1) and the slot list of every
+// brick, from the occupancy words; one CTA per brick, run once per lattice.
+template <class Sh>
+__global__ void __launch_bounds__(CTA) k_build_tiles(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
+  using T2 = Tile<Sh, 2>;
+  using T1 = Tile<Sh, 1>;
+  __shared__ Pro<Sh> s;
+  __shared__ IdxTile<Sh, 2> t2;
+  __shared__ IdxTile<Sh, 1> t1;
+  const int2 wk = work[blockIdx.x];
+  const LatDesc& D = descs[wk.x];
+  const int brick = wk.y;
+  prologue<Sh, CTA, false>(D, brick, s);
+  build_idx_tile<Sh, 2>(s, t2.idx, t2.rbits, t2.rbase);
+  build_idx_tile<Sh, 1>(s, t1.idx, t1.rbits, t1.rbase);
+  int32_t* g2 = const_cast<int32_t*>(D.tile2) + (int64_t)brick * T2::N;
+  int32_t* g1 = const_cast<int32_t*>(D.tile1) + (int64_t)brick * T1::N;
+  uint16_t* gs = const_cast<uint16_t*>(D.slots) + (int64_t)brick * Sh::C;
+  for (int t = threadIdx.x; t < T2::N; t += CTA) g2[t] = t2.idx[t];
+  for (int t = threadIdx.x; t < T1::N; t += CTA) g1[t] = t1.idx[t];
+  for (int r = threadIdx.x; r < Sh::C; r += CTA) gs[r] = r < s.rec.cnt ? s.slot_of[r] : (uint16_t)0;
+}
 
 // Block reduction of NV doubles into thread 0 (the last one as a max when mx).
 // SMem is Pro<Sh> or Red.
@@ -544,17 +599,16 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   using R = typename S::real;
   using F = typename S::fld;
   using T = Tile<Sh, 1>;
-  __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 1> it;
+  __shared__ Head<Sh> s;
+  __shared__ __align__(16) int32_t s_idx[T::N];
   __shared__ R s_c[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  prologue<Sh>(D, wk.y, s);
-  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  load_brick<Sh, 1>(D, wk.y, s, s_idx);
   {
     const F* const src[1] = {static_cast<const F*>(D.c)};
     R* const dst[1] = {s_c};
-    stage<Sh, 1, 1>(src, dst, true, s.lambda, it.idx);
+    stage<Sh, 1, 1>(src, dst, true, s.lambda, s_idx);
   }
   __syncthreads();
   const DevPrm& Pm = D.prm;
@@ -567,7 +621,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   const F* __restrict__ fjz = static_cast<const F*>(D.jz);
   F* __restrict__ fp = static_cast<F*>(D.p);
   F* __restrict__ fmu = static_cast<F*>(D.mu);
-  const int first = s.rec.first, cnt = s.rec.cnt;
+  const int first = s.first, cnt = s.cnt;
   for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int64_t i = first + r;
     const int pos = T::pos(s.slot_of[r]);
@@ -626,23 +680,22 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
   using R = typename S::real;
   using F = typename S::fld;
   using T = Tile<Sh, 1>;
-  __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 1> it;
+  __shared__ Head<Sh> s;
+  __shared__ __align__(16) int32_t s_idx[T::N];
   __shared__ R s_m[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  prologue<Sh, CTA, false>(D, wk.y, s);
-  build_idx_tile<Sh, 1>(s, it.idx, it.rbits, it.rbase);
+  load_brick<Sh, 1, CTA, false>(D, wk.y, s, s_idx);
   {
     const F* const src[1] = {static_cast<const F*>(D.mu)};
     R* const dst[1] = {s_m};
-    stage<Sh, 1, 1>(src, dst, false, 0.0, it.idx);
+    stage<Sh, 1, 1>(src, dst, false, 0.0, s_idx);
   }
   __syncthreads();
   const bool hbb = D.prm.hbb != 0;
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
-  const int first = s.rec.first, cnt = s.rec.cnt;
+  const int first = s.first, cnt = s.cnt;
   for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int pos = T::pos(s.slot_of[r]);
     const R m0 = s_m[pos];

@@ -106,6 +106,9 @@ struct LatDesc {
   const int32_t* brick_xyz;    // [nbricks][3]
   const BrickRec* rec;         // [nbricks]
   const int32_t* ref_of;       // site -> reference-order index
+  const int32_t* tile2;        // [nbricks][halo-2 tile] site index or -1 (k_build_tiles)
+  const int32_t* tile1;        // [nbricks][halo-1 tile]
+  const uint16_t* slots;       // [nbricks][brick slots] fluid slots in site order
   // state: pop[buffer][0 = h, 1 = g]
   void* pop[2][2];
   // fields (FP64 for FP64 storage, FP32 otherwise)
