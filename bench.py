@@ -38,9 +38,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 Q = 19
-B_ALG = {"f64": 904, "f32": 452, "f16s": 262, "bf16s": 262}       # bytes / site / step (whole step)
+B_ALG = {"f64": 904, "f32": 452, "f16s": 262, "bf16s": 262,       # bytes / site / step (whole step)
+         "f16g": 338, "bf16g": 338}                                # h FP32 (38 moves), g 16-bit (57 moves)
 B_P4 = {"f64": 8 * (19 + 4 + 38), "f32": 4 * (19 + 4 + 38), "f16s": 2 * 19 + 4 * 4 + 2 * 38,
-        "bf16s": 2 * 19 + 4 * 4 + 2 * 38}                          # collide pass: g, 4 fields in; h, g out
+        "bf16s": 2 * 19 + 4 * 4 + 2 * 38,                          # collide pass: g, 4 fields in; h, g out
+        "f16g": 2 * 19 + 4 * 4 + 4 * 19 + 2 * 19, "bf16g": 2 * 19 + 4 * 4 + 4 * 19 + 2 * 19}
 METRIC = "MLUPS (fluid-site lattice updates / s, 1e6) at 300^3 porous, fused MRT"
 
 
@@ -51,7 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=300)
-    ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16s", "bf16s"])
+    ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16s", "bf16s", "f16g", "bf16g"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the served sweep and request stream")

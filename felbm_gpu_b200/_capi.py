@@ -19,10 +19,10 @@ if not os.path.exists(LIB_PATH):
 lib = C.CDLL(LIB_PATH)
 
 FE_OK, FE_ERR_ARG, FE_ERR_CUDA, FE_ERR_NO_DEVICE, FE_ERR_MEMORY, FE_ERR_STATE, FE_ERR_IO, FE_ERR_DIVERGED = range(8)
-FE_F64, FE_F32, FE_F16S, FE_BF16S = range(4)
+FE_F64, FE_F32, FE_F16S, FE_BF16S, FE_F16G, FE_BF16G = range(6)
 FE_MRT_E, FE_MRT_EPS, FE_MRT_Q, FE_MRT_NU, FE_MRT_PI, FE_MRT_M = range(1, 7)
 FE_RATE_S0, FE_RATE_MAGIC, FE_RATE_FIXED = range(3)
-STORAGE = {"f64": FE_F64, "f32": FE_F32, "f16s": FE_F16S, "bf16s": FE_BF16S}
+STORAGE = {"f64": FE_F64, "f32": FE_F32, "f16s": FE_F16S, "bf16s": FE_BF16S, "f16g": FE_F16G, "bf16g": FE_BF16G}
 
 
 class FeParams(C.Structure):

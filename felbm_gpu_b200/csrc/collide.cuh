@@ -77,7 +77,8 @@ template <class S, class Sh, int MRT>
 __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
   using R = typename S::real;
-  using P = typename S::pop;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
   using F = typename S::fld;
   using T = Tile<Sh, 2>;
   using SM = CollideSmem<Sh, R>;
@@ -107,9 +108,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   const R tau0 = (R)Pm.tau0, tau1 = (R)Pm.tau1, ffac = (R)s.ff;
   const R gxa = (R)Pm.gx, gya = (R)Pm.gy, gza = (R)Pm.gz;
   const R fxa = (R)Pm.fx * ffac, fya = (R)Pm.fy * ffac, fza = (R)Pm.fz * ffac;
-  const P* __restrict__ gin = static_cast<const P*>(D.pop[parity][1]);
-  P* __restrict__ hout = static_cast<P*>(D.pop[parity ^ 1][0]);
-  P* __restrict__ gout = static_cast<P*>(D.pop[parity ^ 1][1]);
+  const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
+  PH* __restrict__ hout = static_cast<PH*>(D.pop[parity ^ 1][0]);
+  PG* __restrict__ gout = static_cast<PG*>(D.pop[parity ^ 1][1]);
   const F* __restrict__ fmu = static_cast<const F*>(D.mu);
   const Shift shh{(float)Pm.c_ref, (float)(1.0 / Pm.h_scale), (float)Pm.h_scale};
   const Shift shg{(float)Pm.p_ref, (float)(1.0 / Pm.g_scale), (float)Pm.g_scale};
@@ -130,7 +131,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     const int64_t a0 = pbase(i);
     R g[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) g[k] = ld_pop<S>(gin, a0 + k * AOSOA, k, shg);
+    for (int k = 0; k < Q; ++k) g[k] = ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg);
     // push target of direction k: slot k of x + e_k, or slot opp(k) of x
     // (halfway bounce-back) when x + e_k is solid
     auto dst = [&](int k) -> int64_t {
@@ -242,13 +243,13 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     {  // rest direction: no derivatives, avg = lap(mu) of the site
       R h0, x0;
       dir_terms<R, MRT>(q, weight<R>(0), R(0), R(0), R(0), R(0), R(0), R(0), lmu, g[0], h0, x0, Z[0]);
-      st_pop<S>(hout, a0, 0, h0, shh);
+      st_pop<HV<S>>(hout, a0, 0, h0, shh);
       if (MRT) {
 #pragma unroll
         for (int j = 0; j < Q; ++j)
           if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) mom[j] += R(mrt_M(j, 0)) * x0;
       } else {
-        st_pop<S>(gout, a0, 0, Z[0] + s0 * x0, shg);
+        st_pop<GV<S>>(gout, a0, 0, Z[0] + s0 * x0, shg);
       }
     }
 #pragma unroll
@@ -266,8 +267,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       R ha, hb, xa, xb;
       dir_terms<R, MRT>(q, w, uk, fproj, cdc, cdp, bca, bpa, avg_a, g[k], ha, xa, Z[k]);
       dir_terms<R, MRT>(q, w, -uk, -fproj, -cdc, -cdp, bcb, bpb, avg_b, g[k + 1], hb, xb, Z[k + 1]);
-      st_pop<S>(hout, dst(k), k, ha, shh);
-      st_pop<S>(hout, dst(k + 1), k + 1, hb, shh);
+      st_pop<HV<S>>(hout, dst(k), k, ha, shh);
+      st_pop<HV<S>>(hout, dst(k + 1), k + 1, hb, shh);
       if (MRT) {
         const R sx = xa + xb, dx = xa - xb;
 #pragma unroll
@@ -281,8 +282,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
           else if (mjk != 0) mom[j] += R(mjk) * vv;
         }
       } else {
-        st_pop<S>(gout, dst(k), k, Z[k] + s0 * xa, shg);
-        st_pop<S>(gout, dst(k + 1), k + 1, Z[k + 1] + s0 * xb, shg);
+        st_pop<GV<S>>(gout, dst(k), k, Z[k] + s0 * xa, shg);
+        st_pop<GV<S>>(gout, dst(k + 1), k + 1, Z[k + 1] + s0 * xb, shg);
       }
     }
     if (MRT) {
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
 #pragma unroll
       for (int j = 0; j < Q; ++j)
         if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) back0 += R(mrt_M(j, 0)) * mom[j];
-      st_pop<S>(gout, a0, 0, Z[0] + back0, shg);
+      st_pop<GV<S>>(gout, a0, 0, Z[0] + back0, shg);
 #pragma unroll
       for (int k = 1; k < Q; k += 2) {
         R E = 0, O = 0;
@@ -314,8 +315,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
           else if (mjk == -1) acc -= mom[j];
           else if (mjk != 0) acc += R(mjk) * mom[j];
         }
-        st_pop<S>(gout, dst(k), k, Z[k] + (E + O), shg);
-        st_pop<S>(gout, dst(k + 1), k + 1, Z[k + 1] + (E - O), shg);
+        st_pop<GV<S>>(gout, dst(k), k, Z[k] + (E + O), shg);
+        st_pop<GV<S>>(gout, dst(k + 1), k + 1, Z[k + 1] + (E - O), shg);
       }
     }
   }

@@ -52,7 +52,11 @@ void fe_clear_error() { g_last_error.clear(); }
     case 4: { using S = StF16S; using Sh = Shape3D; CALL; } break;             \
     case 5: { using S = StF16S; using Sh = Shape2D; CALL; } break;             \
     case 6: { using S = StBF16S; using Sh = Shape3D; CALL; } break;            \
-    default: { using S = StBF16S; using Sh = Shape2D; CALL; } break;           \
+    case 7: { using S = StBF16S; using Sh = Shape2D; CALL; } break;            \
+    case 8: { using S = StF16G; using Sh = Shape3D; CALL; } break;             \
+    case 9: { using S = StF16G; using Sh = Shape2D; CALL; } break;             \
+    case 10: { using S = StBF16G; using Sh = Shape3D; CALL; } break;           \
+    default: { using S = StBF16G; using Sh = Shape2D; CALL; } break;           \
   }
 
 static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
@@ -252,7 +256,13 @@ struct Engine {
     return FE_OK;
   }
 
-  size_t pop_size() const { return storage == FE_F64 ? 8 : (storage == FE_F32 ? 4 : 2); }
+  // bytes of one h (f = 0) or g (f = 1) population
+  size_t pop_size(int f) const {
+    if (storage == FE_F64) return 8;
+    if (storage == FE_F32) return 4;
+    if (storage == FE_F16G || storage == FE_BF16G) return f == 0 ? 4 : 2;
+    return 2;
+  }
   size_t fld_size() const { return storage == FE_F64 ? 8 : 4; }
 
   void fill_prm() {
@@ -272,7 +282,7 @@ struct Engine {
     d.c_ref = P.c_ref; d.p_ref = P.p_ref;
     // 16-bit deviations: h_k - w_k c_ref spans about w_k, g_k - w_k p_ref about
     // w_k |p|; a power-of-two scale keeps the stored values near 1.
-    d.h_scale = storage >= FE_F16S ? 64.0 : 1.0;
+    d.h_scale = (storage == FE_F16S || storage == FE_BF16S) ? 64.0 : 1.0;
     d.g_scale = storage >= FE_F16S ? 64.0 : 1.0;
   }
   int upload_desc() {
@@ -284,7 +294,7 @@ struct Engine {
   int create(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid, int dev) {
     P = *p;
     storage = P.storage;
-    if (storage < FE_F64 || storage > FE_BF16S) return fe_fail(FE_ERR_ARG, "unknown storage");
+    if (storage < FE_F64 || storage > FE_BF16G) return fe_fail(FE_ERR_ARG, "unknown storage");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
       cudaGetLastError();
@@ -322,8 +332,8 @@ struct Engine {
     for (int b = 0; b < 2; ++b)
       for (int f = 0; f < 2; ++f) {
         unsigned char* q;
-        if ((rc = alloc(&q, popn * pop_size()))) return rc;
-        FE_CUDA(cudaMemset(q, 0, popn * pop_size()));
+        if ((rc = alloc(&q, popn * pop_size(f)))) return rc;
+        FE_CUDA(cudaMemset(q, 0, popn * pop_size(f)));
         D.pop[b][f] = q;
       }
     void** flds[] = {&D.c, &D.p, &D.jx, &D.jy, &D.jz, &D.mu, &D.lapmu};
@@ -870,7 +880,9 @@ struct Batch {
       case FE_F64: launch_step_t<StF64>(par, st); break;
       case FE_F32: launch_step_t<StF32>(par, st); break;
       case FE_F16S: launch_step_t<StF16S>(par, st); break;
-      default: launch_step_t<StBF16S>(par, st); break;
+      case FE_BF16S: launch_step_t<StBF16S>(par, st); break;
+      case FE_F16G: launch_step_t<StF16G>(par, st); break;
+      default: launch_step_t<StBF16G>(par, st); break;
     }
   }
   // kernels of one step, the count launch_step_t makes
@@ -1095,7 +1107,7 @@ int fe_params_default(fe_params* p) {
   for (int q = 1; q < 7; ++q) p->mrt_rate_mode[q] = fe::mrt_reference_mode(q);
   p->use_halfway_bb = 1;
   p->storage = FE_F64;
-  p->c_ref = 0.5; p->p_ref = 0.0;
+  p->c_ref = 0.5; p->p_ref = 1.0;  // p_ref: the initial pressure level p0 = 1
   return fe_params_derive(p);
 }
 

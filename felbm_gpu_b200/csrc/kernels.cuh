@@ -46,12 +46,18 @@ struct StF64 {
   using fld = double;
   using real = double;
   static constexpr bool shifted = false;
+  using hpop = pop;
+  using gpop = pop;
+  static constexpr bool hshift = shifted, gshift = shifted;
 };
 struct StF32 {
   using pop = float;
   using fld = float;
   using real = float;
   static constexpr bool shifted = false;
+  using hpop = pop;
+  using gpop = pop;
+  static constexpr bool hshift = shifted, gshift = shifted;
 };
 // FP16 / BF16: population k stored as (f_k - w_k * ref) * scale, ref = c_ref
 // for h and p_ref for g; arithmetic in FP32.
@@ -60,12 +66,53 @@ struct StF16S {
   using fld = float;
   using real = float;
   static constexpr bool shifted = true;
+  using hpop = pop;
+  using gpop = pop;
+  static constexpr bool hshift = shifted, gshift = shifted;
 };
 struct StBF16S {
   using pop = __nv_bfloat16;
   using fld = float;
   using real = float;
   static constexpr bool shifted = true;
+  using hpop = pop;
+  using gpop = pop;
+  static constexpr bool hshift = shifted, gshift = shifted;
+};
+
+// Mixed storage: h in FP32 (the order parameter spans 0..1, so a shift
+// gains it no precision), g as scaled FP16 / BF16 deviations from w_k p_ref.
+struct StF16G {
+  using pop = float;
+  using fld = float;
+  using real = float;
+  static constexpr bool shifted = false;
+  using hpop = float;
+  using gpop = __half;
+  static constexpr bool hshift = false, gshift = true;
+};
+struct StBF16G {
+  using pop = float;
+  using fld = float;
+  using real = float;
+  static constexpr bool shifted = false;
+  using hpop = float;
+  using gpop = __nv_bfloat16;
+  static constexpr bool hshift = false, gshift = true;
+};
+
+// The h and the g view of a storage, for ld_pop / st_pop.
+template <class S>
+struct HV {
+  using pop = typename S::hpop;
+  using real = typename S::real;
+  static constexpr bool shifted = S::hshift;
+};
+template <class S>
+struct GV {
+  using pop = typename S::gpop;
+  using real = typename S::real;
+  static constexpr bool shifted = S::gshift;
 };
 
 template <class T> __device__ __forceinline__ float to_f(T v);
@@ -415,14 +462,15 @@ template <class S>
 __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                   int parity, int write_j) {
   using R = typename S::real;
-  using P = typename S::pop;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
   using F = typename S::fld;
   __shared__ Red s;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int chunk = wk.y;
-  const P* __restrict__ hin = static_cast<const P*>(D.pop[parity][0]);
-  const P* __restrict__ gin = static_cast<const P*>(D.pop[parity][1]);
+  const PH* __restrict__ hin = static_cast<const PH*>(D.pop[parity][0]);
+  const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
   F* __restrict__ fc = static_cast<F*>(D.c);
   F* __restrict__ fp = static_cast<F*>(D.p);
   F* __restrict__ fjx = static_cast<F*>(D.jx);
@@ -439,8 +487,8 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
     R hv[Q], gv[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      hv[k] = ld_pop<S>(hin, a + k * AOSOA, k, shh);
-      gv[k] = ld_pop<S>(gin, a + k * AOSOA, k, shg);
+      hv[k] = ld_pop<HV<S>>(hin, a + k * AOSOA, k, shh);
+      gv[k] = ld_pop<GV<S>>(gin, a + k * AOSOA, k, shg);
     }
     R c = 0, p = 0, jx = 0, jy = 0, jz = 0;
     double cd = 0.0;
@@ -870,11 +918,12 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
                                                          int parity, double* __restrict__ h_out,
                                                          double* __restrict__ g_out, int apply_lambda) {
   using R = typename S::real;
-  using P = typename S::pop;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  const P* hin = static_cast<const P*>(D.pop[parity][0]);
-  const P* gin = static_cast<const P*>(D.pop[parity][1]);
+  const PH* hin = static_cast<const PH*>(D.pop[parity][0]);
+  const PG* gin = static_cast<const PG*>(D.pop[parity][1]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   const double lambda = apply_lambda ? D.ctl->lambda : 0.0;
@@ -886,9 +935,9 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      hv[k] = ld_pop<S>(hin, a + k * AOSOA, k, shh);
+      hv[k] = ld_pop<HV<S>>(hin, a + k * AOSOA, k, shh);
       cd += (double)hv[k];
-      g_out[k * n + q] = (double)ld_pop<S>(gin, a + k * AOSOA, k, shg);
+      g_out[k * n + q] = (double)ld_pop<GV<S>>(gin, a + k * AOSOA, k, shg);
     }
     const double phi = cd * (1.0 - cd);
     const bool inj = lambda != 0.0 && phi > 0.0;
@@ -909,10 +958,11 @@ template <class S>
 __global__ void __launch_bounds__(CTA) k_inject(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                  int parity) {
   using R = typename S::real;
-  using P = typename S::pop;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  P* h = static_cast<P*>(D.pop[parity][0]);
+  PH* h = static_cast<PH*>(D.pop[parity][0]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const double lambda = D.ctl->lambda;
   if (lambda == 0.0) return;
@@ -924,7 +974,7 @@ __global__ void __launch_bounds__(CTA) k_inject(const LatDesc* __restrict__ desc
     double cd = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      hv[k] = ld_pop<S>(h, a + k * AOSOA, k, shh);
+      hv[k] = ld_pop<HV<S>>(h, a + k * AOSOA, k, shh);
       cd += (double)hv[k];
     }
     const double phi = cd * (1.0 - cd);
@@ -933,7 +983,7 @@ __global__ void __launch_bounds__(CTA) k_inject(const LatDesc* __restrict__ desc
     for (int k = 0; k < Q; ++k) {
       R v = hv[k];
       v += (R)(weight<double>(k) * (-lambda * phi));
-      st_pop<S>(h, a + k * AOSOA, k, v, shh);
+      st_pop<HV<S>>(h, a + k * AOSOA, k, v, shh);
     }
   }
 }
@@ -944,11 +994,12 @@ template <class S>
 __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                        int parity, const double* __restrict__ h_in,
                                                        const double* __restrict__ g_in) {
-  using P = typename S::pop;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  P* hb = static_cast<P*>(D.pop[parity][0]);
-  P* gb = static_cast<P*>(D.pop[parity][1]);
+  PH* hb = static_cast<PH*>(D.pop[parity][0]);
+  PG* gb = static_cast<PG*>(D.pop[parity][1]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   const int64_t n = D.n, i0 = (int64_t)wk.y * CHUNK;
@@ -957,8 +1008,8 @@ __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict_
     const int64_t a = pbase(i), q = D.ref_of[i];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-      st_pop<S>(hb, a + k * AOSOA, k, (typename S::real)h_in[k * n + q], shh);
-      st_pop<S>(gb, a + k * AOSOA, k, (typename S::real)g_in[k * n + q], shg);
+      st_pop<HV<S>>(hb, a + k * AOSOA, k, (typename S::real)h_in[k * n + q], shh);
+      st_pop<GV<S>>(gb, a + k * AOSOA, k, (typename S::real)g_in[k * n + q], shg);
     }
   }
 }
@@ -969,12 +1020,13 @@ __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict_
 template <class S>
 __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                int parity, double* __restrict__ part) {
-  using P = typename S::pop;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
   __shared__ Red s;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int chunk = wk.y;
-  const P* hin = static_cast<const P*>(D.pop[parity][0]);
+  const PH* hin = static_cast<const PH*>(D.pop[parity][0]);
   const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
   double acc[2] = {0.0, 0.0};
   const int64_t i0 = (int64_t)chunk * CHUNK;
@@ -983,7 +1035,7 @@ __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs,
     const int64_t a = pbase(i);
     double cd = 0.0;
 #pragma unroll
-    for (int k = 0; k < Q; ++k) cd += (double)ld_pop<S>(hin, a + k * AOSOA, k, shh);
+    for (int k = 0; k < Q; ++k) cd += (double)ld_pop<HV<S>>(hin, a + k * AOSOA, k, shh);
     double phi = cd * (1.0 - cd);
     if (phi < 0.0) phi = 0.0;
     acc[0] += cd;

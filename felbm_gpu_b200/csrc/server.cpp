@@ -60,7 +60,12 @@ struct Live {
   int status = FE_OK;         // nonzero: failed, report it
 };
 
-size_t pop_bytes(int storage) { return storage == FE_F64 ? 8 : (storage == FE_F32 ? 4 : 2); }
+// mean bytes of an h and a g population
+double pop_bytes(int storage) {
+  if (storage == FE_F64) return 8;
+  if (storage == FE_F32) return 4;
+  return (storage == FE_F16G || storage == FE_BF16G) ? 3 : 2;
+}
 size_t fld_bytes(int storage) { return storage == FE_F64 ? 8 : 4; }
 
 // Device bytes of one resident solve: two ping-pong buffers of h and g, the
@@ -394,7 +399,7 @@ extern "C" {
 int fe_server_create(const fe_server_config* cfg, fe_server** out) {
   if (!cfg || !out) return fe_fail(FE_ERR_ARG, "fe_server_create: bad arguments");
   if (cfg->chunk_steps < 1) return fe_fail(FE_ERR_ARG, "chunk_steps must be > 0");
-  if (cfg->storage < FE_F64 || cfg->storage > FE_BF16S) return fe_fail(FE_ERR_ARG, "unknown storage");
+  if (cfg->storage < FE_F64 || cfg->storage > FE_BF16G) return fe_fail(FE_ERR_ARG, "unknown storage");
   if (cfg->hbm_reserve_frac < 0.0 || cfg->hbm_reserve_frac >= 1.0)
     return fe_fail(FE_ERR_ARG, "hbm_reserve_frac must be in [0, 1)");
   *out = nullptr;

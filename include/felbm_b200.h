@@ -44,6 +44,10 @@ extern "C" {
 #define FE_F32 1
 #define FE_F16S 2
 #define FE_BF16S 3
+/* Mixed: h in FP32 (the order parameter spans 0..1, so a shift gains it no
+ * precision), g as the FP16 / BF16 deviation from w_k*p_ref. */
+#define FE_F16G 4
+#define FE_BF16G 5
 
 /* forcing_timedep (reference felbm_gpu_main.cu:587-594) */
 #define FE_FORCING_CONSTANT 0
@@ -90,7 +94,7 @@ typedef struct fe_params {
    * one fused path here; they are kept so configs and logs round-trip. */
   int stream_matrix_free, grad_matrix_free, fused, fuse_collision;
   int mrt_fast_transform, stream_inplace;
-  /* storage of the populations, FE_F64 .. FE_BF16S */
+  /* storage of the populations, FE_F64 .. FE_BF16G */
   int storage;
   /* reference scale of the FE_F16S/FE_BF16S deviations (ignored otherwise) */
   double c_ref, p_ref;

@@ -36,7 +36,7 @@ def alone(name, storage, steps):
         e.free()
 
 
-@pytest.mark.parametrize("storage", ["f64", "f32", "f16s"])
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16s", "f16g"])
 def test_batch_equals_alone(require_gpu, storage):
     steps = 23
     ref = {n: alone(n, storage, steps) for n in MIX}
