@@ -73,7 +73,7 @@ __device__ __forceinline__ void dir_terms(const SiteScal<R>& q, R w, R uk, R fpr
   Z = gk + (q.drho_cs2 * dc - q.u_drm) * wut + (ffk - q.u_fg_f) * G;
 }
 
-template <class S, class Sh, int MRT>
+template <class S, class Sh, int MRT, bool HBB>
 __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
   using R = typename S::real;
@@ -102,7 +102,6 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   __syncthreads();
 
   const DevPrm& Pm = D.prm;
-  const bool hbb = Pm.hbb != 0;
   const R cs2 = R(CS2), alpha = R(ALPHA);
   const R rho1 = (R)Pm.rho1, drho = (R)Pm.drho;
   const R tau0 = (R)Pm.tau0, tau1 = (R)Pm.tau1, ffac = (R)s.ff;
@@ -146,9 +145,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const int o = T::off(k), v = 6 * (k >> 1);
       const R cm = s_c[pos - o], cp = s_c[pos + o], cm2 = s_c[pos - 2 * o], cp2 = s_c[pos + 2 * o];
       const R pm = s_p[pos - o], pp = s_p[pos + o], pm2 = s_p[pos - 2 * o], pp2 = s_p[pos + 2 * o];
-      const R cdc = cd_val(q.c, cm, cp, hbb), cdp = cd_val(q.p, pm, pp, hbb);
-      const R bca = bd_val(q.c, cm, cp, cm2, cp2, hbb), bcb = bd_val(q.c, cp, cm, cp2, cm2, hbb);
-      const R bpa = bd_val(q.p, pm, pp, pm2, pp2, hbb), bpb = bd_val(q.p, pp, pm, pp2, pm2, hbb);
+      R cdc, cdp, bca, bcb, bpa, bpb;
+      pair_derivs<HBB>(q.c, cm, cp, cm2, cp2, q.p, pm, pp, pm2, pp2, cdc, cdp, bca, bcb, bpa, bpb);
       s_st[(v + 0) * P4T] = cdc;
       s_st[(v + 1) * P4T] = cdp;
       s_st[(v + 2) * P4T] = bca;

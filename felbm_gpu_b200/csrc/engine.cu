@@ -188,6 +188,17 @@ static int build_layout(const uint8_t* solid, int nx, int ny, int nz, HostLayout
 
 enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
 
+// One launch of the collide pass, the variant chosen by the collision model
+// and the near-wall rule.
+template <class S, class Sh>
+static void launch_collide(bool mrt, bool hbb, int nwork, size_t smem, cudaStream_t st, const LatDesc* desc,
+                           const int2* work, int par) {
+  if (mrt && hbb) k_collide<S, Sh, 1, true><<<nwork, P4T, smem, st>>>(desc, work, par);
+  else if (mrt) k_collide<S, Sh, 1, false><<<nwork, P4T, smem, st>>>(desc, work, par);
+  else if (hbb) k_collide<S, Sh, 0, true><<<nwork, P4T, smem, st>>>(desc, work, par);
+  else k_collide<S, Sh, 0, false><<<nwork, P4T, smem, st>>>(desc, work, par);
+}
+
 struct Engine {
   fe_params P{};
   int storage = FE_F64;
@@ -395,8 +406,10 @@ struct Engine {
   int set_attrs() {
     smem_p4 = CollideSmem<Sh, typename S::real>::BYTES;
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 0>, a, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 1>, a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 0, false>, a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 1, false>, a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 0, true>, a, (int)smem_p4));
+    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 1, true>, a, (int)smem_p4));
     return FE_OK;
   }
 
@@ -421,8 +434,7 @@ struct Engine {
     rec(3);
     k_lapmu<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work);
     rec(4);
-    if (hd.prm.use_mrt) k_collide<S, Sh, 1><<<nb, P4T, smem_p4, st>>>(d_desc, d_work, par);
-    else k_collide<S, Sh, 0><<<nb, P4T, smem_p4, st>>>(d_desc, d_work, par);
+    launch_collide<S, Sh>(hd.prm.use_mrt != 0, hd.prm.hbb != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
     launches += 4;
   }
@@ -671,7 +683,7 @@ struct Engine {
 // ---------------------------------------------------------------------------
 struct Batch {
   struct Group {
-    int shape2d = 0, mrt = 0;
+    int shape2d = 0, mrt = 0, hbb = 0;
     int2* d_work = nullptr;
     int nwork = 0;
   };
@@ -815,19 +827,22 @@ struct Batch {
     std::vector<int2> gw;
     std::vector<size_t> offs;
     for (int sh = 0; sh < 2; ++sh)
-      for (int mrt = 0; mrt < 2; ++mrt) {
-        const size_t off = gw.size();
-        for (size_t q = 0; q < mem.size(); ++q)
-          if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0))
-            for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
-        if (gw.size() == off) continue;
-        Group g;
-        g.shape2d = sh;
-        g.mrt = mrt;
-        g.nwork = (int)(gw.size() - off);
-        groups.push_back(g);
-        offs.push_back(off);
-      }
+      for (int mrt = 0; mrt < 2; ++mrt)
+        for (int hbb = 0; hbb < 2; ++hbb) {
+          const size_t off = gw.size();
+          for (size_t q = 0; q < mem.size(); ++q)
+            if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
+                (mem[q]->hd.prm.hbb != 0) == (hbb != 0))
+              for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
+          if (gw.size() == off) continue;
+          Group g;
+          g.shape2d = sh;
+          g.mrt = mrt;
+          g.hbb = hbb;
+          g.nwork = (int)(gw.size() - off);
+          groups.push_back(g);
+          offs.push_back(off);
+        }
     if ((rc = upload_vec(&d_gwork, &cap_gwork, gw))) return rc;
     for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
     if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
@@ -848,8 +863,7 @@ struct Batch {
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {
     const size_t sm = CollideSmem<Sh, typename S::real>::BYTES;
-    if (g.mrt) k_collide<S, Sh, 1><<<g.nwork, P4T, sm, st>>>(d_desc, g.d_work, par);
-    else k_collide<S, Sh, 0><<<g.nwork, P4T, sm, st>>>(d_desc, g.d_work, par);
+    launch_collide<S, Sh>(g.mrt != 0, g.hbb != 0, g.nwork, sm, st, d_desc, g.d_work, par);
   }
   template <class S>
   void launch_step_t(int par, cudaStream_t st) {

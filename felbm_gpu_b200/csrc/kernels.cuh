@@ -600,6 +600,35 @@ __device__ __forceinline__ R bd_val(R f0, R fm, R fp, R fm2, R fp2, bool hbb) {
   if (hbb) return b1 ? R(0.5) * f0 + R(-0.5) * fm : R(0);
   return (b1 && is_site(fm2)) ? R(-1.5) * f0 + R(2.0) * fm + R(-0.5) * fm2 : R(0);
 }
+// The same two stencils for one opposite pair (e, -e) of both tiles, branch
+// free, the near-wall case fixed at compile time by HBB: c and p share their
+// solid positions, so the four neighbour flags are taken once. Outputs the
+// central values of c and p for +e, and the biased values of c and p for +e
+// (a) and -e (b). Same arithmetic as cd_val / bd_val in every case.
+template <bool HBB, class R>
+__device__ __forceinline__ R bd_sel(R f0, R fm, R fp, R fm2, R fp2, bool sm, bool sp, bool sm2, bool sp2) {
+  const R two = R(-1.5) * f0 + R(2.0) * fp + R(-0.5) * fp2;
+  const R one = HBB ? R(-1.5) * f0 + R(1.5) * fp : R(-2.0) * f0 + R(2.0) * fp;
+  const R back = HBB ? (sm ? R(0.5) * f0 + R(-0.5) * fm : R(0))
+                     : ((sm && sm2) ? R(-1.5) * f0 + R(2.0) * fm + R(-0.5) * fm2 : R(0));
+  return sp ? (sp2 ? two : one) : back;
+}
+template <bool HBB, class R>
+__device__ __forceinline__ R cd_sel(R f0, R fm, R fp, bool sm, bool sp) {
+  if (HBB) return R(0.5) * ((sp ? fp : f0) - (sm ? fm : f0));
+  return (sm && sp) ? R(0.5) * (fp - fm) : R(0);
+}
+template <bool HBB, class R>
+__device__ __forceinline__ void pair_derivs(R c0, R cm, R cp, R cm2, R cp2, R p0, R pm, R pp, R pm2, R pp2, R& cdc,
+                                            R& cdp, R& bca, R& bcb, R& bpa, R& bpb) {
+  const bool sm = is_site(cm), sp = is_site(cp), sm2 = is_site(cm2), sp2 = is_site(cp2);
+  cdc = cd_sel<HBB>(c0, cm, cp, sm, sp);
+  cdp = cd_sel<HBB>(p0, pm, pp, sm, sp);
+  bca = bd_sel<HBB>(c0, cm, cp, cm2, cp2, sm, sp, sm2, sp2);
+  bcb = bd_sel<HBB>(c0, cp, cm, cp2, cm2, sp, sm, sp2, sm2);
+  bpa = bd_sel<HBB>(p0, pm, pp, pm2, pp2, sm, sp, sm2, sp2);
+  bpb = bd_sel<HBB>(p0, pp, pm, pp2, pm2, sp, sm, sp2, sm2);
+}
 // Laplacian term of direction k (k_lap_mf), boundary half `bnd`
 template <class R>
 __device__ __forceinline__ R lap_val(R f0, R fm, R fp, R bnd, bool hbb) {
