@@ -18,6 +18,8 @@
 //    pair as E +- O; only g + force_g (19 values) and the 15 relaxed moments
 //    stay live until the g stores.
 #pragma once
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace fe {
@@ -73,7 +75,7 @@ __device__ __forceinline__ void dir_terms(const SiteScal<R>& q, R w, R uk, R fpr
   Z = gk + (q.drho_cs2 * dc - q.u_drm) * wut + (ffk - q.u_fg_f) * G;
 }
 
-template <class S, class Sh, int MRT, bool HBB>
+template <class S, class Sh, int MRT, bool HBB, bool WIDE>
 __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
   using R = typename S::real;
@@ -82,6 +84,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   using F = typename S::fld;
   using T = Tile<Sh, 2>;
   using SM = CollideSmem<Sh, R>;
+  // population offsets: 32-bit while the lattice's arrays stay below 2^32
+  // entries (the host picks WIDE otherwise)
+  using IX = typename std::conditional<WIDE, int64_t, uint32_t>::type;
   __shared__ Head<Sh> s;
   extern __shared__ __align__(16) unsigned char dsm[];
   int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
@@ -127,15 +132,16 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     q.mu = (R)fmu[i];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
     // post-stream g of the site (what P1 read)
-    const int64_t a0 = pbase(i);
+    const IX a0 = (IX)pbase(i);
     R g[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) g[k] = ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg);
     // push target of direction k: slot k of x + e_k, or slot opp(k) of x
     // (halfway bounce-back) when x + e_k is solid
-    auto dst = [&](int k) -> int64_t {
+    auto dst = [&](int k) -> IX {
       const int dn = s_idx[pos + T::off(k)];
-      return dn >= 0 ? pidx(dn, k) : a0 + lat_opp(k) * AOSOA;
+      return dn >= 0 ? (IX)(dn >> 5) * (IX)(Q * AOSOA) + (IX)(k * AOSOA + (dn & (AOSOA - 1)))
+                     : a0 + (IX)(lat_opp(k) * AOSOA);
     };
     // ---- pre-pass: near-wall cases once, the four gradients, stash -----------
     R ecx = 0, ecy = 0, ecz = 0, epx = 0, epy = 0, epz = 0;

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -188,21 +189,47 @@ static int build_layout(const uint8_t* solid, int nx, int ny, int nz, HostLayout
 
 enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
 
-// One launch of the collide pass, the variant chosen by the collision model
-// and the near-wall rule.
-template <class S, class Sh>
-static void launch_collide(bool mrt, bool hbb, int nwork, size_t smem, cudaStream_t st, const LatDesc* desc,
-                           const int2* work, int par) {
-  if (mrt && hbb) k_collide<S, Sh, 1, true><<<nwork, P4T, smem, st>>>(desc, work, par);
-  else if (mrt) k_collide<S, Sh, 1, false><<<nwork, P4T, smem, st>>>(desc, work, par);
-  else if (hbb) k_collide<S, Sh, 0, true><<<nwork, P4T, smem, st>>>(desc, work, par);
-  else k_collide<S, Sh, 0, false><<<nwork, P4T, smem, st>>>(desc, work, par);
+// The collide-pass variants: collision model, near-wall rule, and 64-bit
+// population offsets for lattices whose arrays reach 2^32 entries.
+template <class S, class Sh, int MRT, bool HBB>
+static void launch_collide_w(bool wide, int nwork, size_t smem, cudaStream_t st, const LatDesc* desc,
+                             const int2* work, int par) {
+  if (wide) k_collide<S, Sh, MRT, HBB, true><<<nwork, P4T, smem, st>>>(desc, work, par);
+  else k_collide<S, Sh, MRT, HBB, false><<<nwork, P4T, smem, st>>>(desc, work, par);
 }
+template <class S, class Sh>
+static void launch_collide(bool mrt, bool hbb, bool wide, int nwork, size_t smem, cudaStream_t st,
+                           const LatDesc* desc, const int2* work, int par) {
+  if (mrt && hbb) launch_collide_w<S, Sh, 1, true>(wide, nwork, smem, st, desc, work, par);
+  else if (mrt) launch_collide_w<S, Sh, 1, false>(wide, nwork, smem, st, desc, work, par);
+  else if (hbb) launch_collide_w<S, Sh, 0, true>(wide, nwork, smem, st, desc, work, par);
+  else launch_collide_w<S, Sh, 0, false>(wide, nwork, smem, st, desc, work, par);
+}
+template <class S, class Sh>
+static cudaError_t collide_smem_attr(int bytes) {
+  const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, a, bytes);
+  };
+  set((const void*)k_collide<S, Sh, 0, false, false>);
+  set((const void*)k_collide<S, Sh, 0, false, true>);
+  set((const void*)k_collide<S, Sh, 0, true, false>);
+  set((const void*)k_collide<S, Sh, 0, true, true>);
+  set((const void*)k_collide<S, Sh, 1, false, false>);
+  set((const void*)k_collide<S, Sh, 1, false, true>);
+  set((const void*)k_collide<S, Sh, 1, true, false>);
+  set((const void*)k_collide<S, Sh, 1, true, true>);
+  return e;
+}
+// True when the lattice's population arrays reach 2^32 entries.
+static bool pops_wide(int64_t n) { return (uint64_t)((n + AOSOA - 1) / AOSOA) * AOSOA * Q >= (1ull << 32); }
 
 struct Engine {
   fe_params P{};
   int storage = FE_F64;
   int shape2d = 0;
+  int wide = 0;               // 64-bit population offsets in the collide pass
   int device = 0;
   HostLayout L;
   LatDesc hd{};               // host copy of the descriptor
@@ -319,6 +346,11 @@ struct Engine {
     if (L.n == 0) return fe_fail(FE_ERR_ARG, "geometry has no fluid site");
     if (L.n >= (int64_t)1 << 31) return fe_fail(FE_ERR_ARG, "more than 2^31 sites");
     shape2d = L.shape2d ? 1 : 0;
+    // FELBM_WIDE_OFFSETS=1 takes the 64-bit variant at any size (tests)
+    {
+      const char* w = std::getenv("FELBM_WIDE_OFFSETS");
+      wide = (pops_wide(L.n) || (w && w[0] == '1')) ? 1 : 0;
+    }
     const int nbk = L.nbricks();
     LatDesc& D = hd;
     D.nx = nx; D.ny = ny; D.nz = nz;
@@ -405,11 +437,7 @@ struct Engine {
   template <class S, class Sh>
   int set_attrs() {
     smem_p4 = CollideSmem<Sh, typename S::real>::BYTES;
-    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 0, false>, a, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 1, false>, a, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 0, true>, a, (int)smem_p4));
-    FE_CUDA(cudaFuncSetAttribute(k_collide<S, Sh, 1, true>, a, (int)smem_p4));
+    FE_CUDA((collide_smem_attr<S, Sh>((int)smem_p4)));
     return FE_OK;
   }
 
@@ -434,7 +462,7 @@ struct Engine {
     rec(3);
     k_lapmu<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work);
     rec(4);
-    launch_collide<S, Sh>(hd.prm.use_mrt != 0, hd.prm.hbb != 0, nb, smem_p4, st, d_desc, d_work, par);
+    launch_collide<S, Sh>(hd.prm.use_mrt != 0, hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
     launches += 4;
   }
@@ -683,7 +711,7 @@ struct Engine {
 // ---------------------------------------------------------------------------
 struct Batch {
   struct Group {
-    int shape2d = 0, mrt = 0, hbb = 0;
+    int shape2d = 0, mrt = 0, hbb = 0, wide = 0;
     int2* d_work = nullptr;
     int nwork = 0;
   };
@@ -836,6 +864,10 @@ struct Batch {
               for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
           if (gw.size() == off) continue;
           Group g;
+          for (size_t q = 0; q < mem.size(); ++q)
+            if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
+                (mem[q]->hd.prm.hbb != 0) == (hbb != 0) && mem[q]->wide)
+              g.wide = 1;
           g.shape2d = sh;
           g.mrt = mrt;
           g.hbb = hbb;
@@ -863,7 +895,7 @@ struct Batch {
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {
     const size_t sm = CollideSmem<Sh, typename S::real>::BYTES;
-    launch_collide<S, Sh>(g.mrt != 0, g.hbb != 0, g.nwork, sm, st, d_desc, g.d_work, par);
+    launch_collide<S, Sh>(g.mrt != 0, g.hbb != 0, g.wide != 0, g.nwork, sm, st, d_desc, g.d_work, par);
   }
   template <class S>
   void launch_step_t(int par, cudaStream_t st) {

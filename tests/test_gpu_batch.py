@@ -125,3 +125,38 @@ def test_batch_rejects_mixed_storage(require_gpu):
         b.free()
         a.free()
         c.free()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_wide_offsets_agree_with_narrow(require_gpu, storage, monkeypatch):
+    """The collide pass's 64-bit population offsets (taken for lattices whose
+    arrays reach 2^32 entries; forced here at small size) address the same
+    populations as the 32-bit variant: alone and in a batch, the states agree
+    to rounding (the two instantiations may contract multiply-adds
+    differently)."""
+    steps = 17
+    tol = 1e-12 if storage == "f64" else 2e-6
+    ref = {n: alone(n, storage, steps) for n in MIX}
+    monkeypatch.setenv("FELBM_WIDE_OFFSETS", "1")
+    for n in MIX:
+        h, g, f, s = alone(n, storage, steps)
+        hr, gr, fr, sr = ref[n]
+        d = max(np.max(np.abs(h - hr)), np.max(np.abs(g - gr)))
+        assert d <= tol, (n, d)
+        # the statistics are velocity means and maxima: FP32 rounding of
+        # u ~ 0.05 leaves ~1e-7 noise on the near-zero components
+        assert np.allclose(s, sr, rtol=1e-4, atol=tol if storage == "f64" else 2e-6), (n, s, sr)
+    b = Batch()
+    engines = {n: make_engine(n, storage) for n in MIX}
+    try:
+        for e in engines.values():
+            b.add(e)
+        b.run(steps)
+        for n, e in engines.items():
+            h, g = e.download_state()
+            d = max(np.max(np.abs(h - ref[n][0])), np.max(np.abs(g - ref[n][1])))
+            assert d <= tol, (n, d)
+    finally:
+        b.free()
+        for e in engines.values():
+            e.free()
