@@ -343,9 +343,10 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
 #pragma unroll
     for (int qv = 0; qv < 6; ++qv) part[qv] = st[qv];
     if (bad) atomicOr(&D.ctl->status, 1);
-    __threadfence();
     // the last warp of the launch (per lattice) advances the step counter and
-    // queues the next mass correction
+    // queues the next mass correction; it reads nothing the other warps wrote
+    // (the partials are summed by a later launch), so no fence precedes the
+    // count
     if (atomicAdd(&D.ctl->count4, 1u) == (unsigned)(D.nbricks * P4W) - 1u) {
       Ctl* C = D.ctl;
       C->t += 1;

@@ -458,9 +458,11 @@ struct Engine {
     rec(1);
     if (open_bnd) launch_bc<S>(st);
     rec(2);
-    k_cfield<S, Sh, 0><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
+    if (hd.prm.hbb) k_cfield<S, Sh, 0, true><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
+    else k_cfield<S, Sh, 0, false><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
     rec(3);
-    k_lapmu<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work);
+    if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
+    else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
     rec(4);
     launch_collide<S, Sh>(hd.prm.use_mrt != 0, hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
@@ -647,7 +649,8 @@ struct Engine {
   void fields_launch(FieldOut o) {
     k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
-    k_cfield<S, Sh, OUT><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
+    if (hd.prm.hbb) k_cfield<S, Sh, OUT, true><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
+    else k_cfield<S, Sh, OUT, false><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     launches += 2;
   }
   // Corrected velocity of the current state into node-indexed device grids
@@ -886,11 +889,13 @@ struct Batch {
 
   template <class S, class Sh>
   void launch_group_p2(const Group& g, cudaStream_t st) {
-    k_cfield<S, Sh, 0><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, FieldOut{});
+    if (g.hbb) k_cfield<S, Sh, 0, true><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, FieldOut{});
+    else k_cfield<S, Sh, 0, false><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, FieldOut{});
   }
   template <class S, class Sh>
   void launch_group_p3(const Group& g, cudaStream_t st) {
-    k_lapmu<S, Sh><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work);
+    if (g.hbb) k_lapmu<S, Sh, true><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work);
+    else k_lapmu<S, Sh, false><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work);
   }
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {

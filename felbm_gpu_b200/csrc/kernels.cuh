@@ -639,6 +639,16 @@ __device__ __forceinline__ R lap_val(R f0, R fm, R fp, R bnd, bool hbb) {
   return hbb ? (f1v - f0 - bnd) : (R(2) * f1v - R(2) * f0 - R(2) * bnd);
 }
 
+// lap_val, branch free with the near-wall rule fixed at compile time and the
+// two neighbour flags given.
+template <bool HBB, class R>
+__device__ __forceinline__ R lap_sel(R f0, R fm, R fp, R bnd, bool sm, bool sp) {
+  const R both = fm - R(2) * f0 + fp;
+  const R f1v = sm ? fm : fp;
+  const R one = HBB ? (f1v - f0 - bnd) : (R(2) * f1v - R(2) * f0 - R(2) * bnd);
+  return (sm && sp) ? both : ((sm || sp) ? one : R(0));
+}
+
 // ---------------------------------------------------------------------------
 // P2: grad_cd(c), Laplacian(c) with the wetting term, mu, velocity/pressure
 // correction (reference k_grad_cd_mf :897-913, k_pack_lap_c :159-165,
@@ -670,7 +680,7 @@ __device__ __forceinline__ int64_t node_of(const LatDesc& D, int brick, int slot
   return x + (int64_t)D.nx * (y + (int64_t)D.ny * z);
 }
 
-template <class S, class Sh, int OUT>
+template <class S, class Sh, int OUT, bool HBB>
 __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                  FieldOut out) {
   using R = typename S::real;
@@ -692,7 +702,6 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   const R alpha = R(ALPHA), cs2 = R(CS2);
   const R rho1 = (R)Pm.rho1, drho = (R)Pm.drho, kappa = (R)Pm.kappa, four_beta = (R)Pm.four_beta;
   const R bnd_coeff = (R)Pm.bnd_coeff, ff = (R)s.ff;
-  const bool hbb = Pm.hbb != 0;
   const F* __restrict__ fjx = static_cast<const F*>(D.jx);
   const F* __restrict__ fjy = static_cast<const F*>(D.jy);
   const F* __restrict__ fjz = static_cast<const F*>(D.jz);
@@ -721,11 +730,12 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     for (int k = 1; k < Q; k += 2) {
       const R cm = s_c[pos - T::off(k)], cp = s_c[pos + T::off(k)];
       const R aw2 = R(2) * alpha * weight<R>(k);
-      const R cdv = cd_val(c0, cm, cp, hbb);
+      const bool sm = is_site(cm), sp = is_site(cp);
+      const R cdv = cd_sel<HBB>(c0, cm, cp, sm, sp);
       if (lat_cx(k)) gx += aw2 * R(lat_cx(k)) * cdv;
       if (lat_cy(k)) gy += aw2 * R(lat_cy(k)) * cdv;
       if (lat_cz(k)) gz += aw2 * R(lat_cz(k)) * cdv;
-      lap += aw2 * lap_val(c0, cm, cp, bnd, hbb);
+      lap += aw2 * lap_sel<HBB>(c0, cm, cp, bnd, sm, sp);
     }
     const R rho = rho1 + drho * c0;
     const R mu = four_beta * (c0 * (R(1) - c0)) * (R(0.5) - c0) + (-kappa * lap);
@@ -752,7 +762,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
 // P3: Laplacian of mu, boundary half zero (reference k_pack_lap_zero :168-173
 // + k_lap_mf); symmetric within an opposite pair.
 // ---------------------------------------------------------------------------
-template <class S, class Sh>
+template <class S, class Sh, bool HBB>
 __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
   using R = typename S::real;
   using F = typename S::fld;
@@ -769,7 +779,6 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
     stage<Sh, 1, 1>(src, dst, false, 0.0, s_idx);
   }
   __syncthreads();
-  const bool hbb = D.prm.hbb != 0;
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
   const int first = s.first, cnt = s.cnt;
@@ -778,8 +787,10 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
     const R m0 = s_m[pos];
     R lap = 0;
 #pragma unroll
-    for (int k = 1; k < Q; k += 2)
-      lap += R(2) * alpha * weight<R>(k) * lap_val(m0, s_m[pos - T::off(k)], s_m[pos + T::off(k)], R(0), hbb);
+    for (int k = 1; k < Q; k += 2) {
+      const R mm = s_m[pos - T::off(k)], mp = s_m[pos + T::off(k)];
+      lap += R(2) * alpha * weight<R>(k) * lap_sel<HBB>(m0, mm, mp, R(0), is_site(mm), is_site(mp));
+    }
     flm[first + r] = (F)lap;
   }
 }
