@@ -72,7 +72,8 @@ class FeFields(C.Structure):
 
 
 class FeTracerConfig(C.Structure):
-    _fields_ = [("substeps", C.c_int), ("order", C.c_int), ("velocity_skip", C.c_int), ("seed", C.c_uint64)]
+    _fields_ = [("substeps", C.c_int), ("order", C.c_int), ("velocity_skip", C.c_int), ("seed", C.c_uint64),
+                ("stretching", C.c_int), ("phase_split", C.c_int), ("stretching_seed", C.c_uint64)]
 
 
 class FeServerConfig(C.Structure):
@@ -157,6 +158,10 @@ SIGNATURES = {
     "fe_tracers_destroy": (C.c_int, [_vp]),
     "fe_tracers_step": (C.c_int, [_vp]),
     "fe_tracers_download": (C.c_int, [_vp, _dp, _dp]),
+    "fe_tracers_stretch_rows": (C.c_int, [_vp, _dp, C.c_int64, _i64p]),
+    "fe_tracers_stretch_state": (C.c_int, [_vp, _dp, _dp]),
+    "fe_tracers_set_stretch_state": (C.c_int, [_vp, _dp, _dp]),
+    "fe_tracers_set_velocity": (C.c_int, [_vp, _dp, _dp]),
     "fe_tracers_seed": (C.c_int, [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int64,
                                   C.c_uint64, _dp, _i32p]),
     "fe_write_fields_h5": (C.c_int, [_vp, C.c_char_p, C.c_int]),
@@ -164,7 +169,9 @@ SIGNATURES = {
     "fe_checkpoint_write": (C.c_int, [_vp, C.c_char_p, C.c_uint32]),
     "fe_settle_mass_correction": (C.c_int, [_vp]),
     "fe_checkpoint_read": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_uint32)]),
-    "fe_write_particles_h5": (C.c_int, [C.c_char_p, C.c_int64, _dp, _dp, _i64p, _dp, _i32p]),
+    "fe_write_particles_h5": (C.c_int, [C.c_char_p, C.c_int64, _dp, _dp, _i64p, _dp, _i32p, _dp, _dp]),
+    "fe_write_series": (C.c_int, [C.c_char_p, C.c_int, C.c_uint32, _dp, C.c_int64]),
+    "fe_write_stretching": (C.c_int, [C.c_char_p, C.c_int, _dp, C.c_int64]),
     "fe_h5_read_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _i64p, C.POINTER(C.c_int),
                                      C.c_void_p, C.c_int64]),
     "fe_server_create": (C.c_int, [C.POINTER(FeServerConfig), C.POINTER(C.c_void_p)]),

@@ -257,6 +257,7 @@ struct Engine {
   double* h_stats = nullptr;  // pinned [6]
   double target_mass_host = 0.0;
   struct Batch* owner = nullptr;  // batch the engine is a member of
+  std::vector<struct Tracers*> tracer_sets;  // tracers advected on this engine (detached at destroy)
 
   ~Engine() { release(); }
   void release() {
@@ -655,10 +656,10 @@ struct Engine {
   }
   // Corrected velocity of the current state into node-indexed device grids
   // (solid nodes are left as they are), on the engine stream.
-  int velocity_grid(double* ux, double* uy, double* uz) {
+  int velocity_grid(double* ux, double* uy, double* uz, double* c = nullptr) {
     int rc;
     if ((rc = set_ctl_mode(0, ff_manual))) return rc;
-    FieldOut o{nullptr, nullptr, ux, uy, uz, nullptr, nullptr};
+    FieldOut o{nullptr, c, ux, uy, uz, nullptr, nullptr};
     FE_DISPATCH(*this, (fields_launch<S FE_COMMA Sh FE_COMMA 2>(o)));
     FE_CUDA(cudaGetLastError());
     double zero = 0.0;  // as fields(): the step recomputes lambda
@@ -1040,11 +1041,28 @@ struct Tracers {
   int velocity_skip = 1;
   int64_t step = 0;             // tracer steps taken
   bool have_u = false;
+  bool frozen = false;          // a caller-given velocity snapshot (fe_tracers_set_velocity)
   cudaStream_t stream = nullptr;
+  // stretching time series: rows 1..step, ring of ROWCAP rows on the device
+  static constexpr int ROWCAP = 65536;
+  double* ring = nullptr;
+  int64_t drained = 0;          // rows handed out by rows()
+  int blocks = 0;
 
   ~Tracers() {
+    if (E) {
+      auto& v = E->tracer_sets;
+      v.erase(std::remove(v.begin(), v.end(), this), v.end());
+    }
     if (stream) cudaStreamSynchronize(stream);
     for (void* a : allocs) cudaFree(a);
+  }
+  // The engine is going away: finish the queued work on its stream and drop
+  // both; later calls fail with FE_ERR_STATE.
+  void detach() {
+    if (stream) cudaStreamSynchronize(stream);
+    stream = nullptr;
+    E = nullptr;
   }
   template <class T_>
   int alloc(T_** p, size_t count) {
@@ -1061,6 +1079,7 @@ struct Tracers {
              const int64_t* id) {
     E = e;
     stream = e->stream;
+    e->tracer_sets.push_back(this);
     T.n = n;
     T.nx = e->hd.nx;
     T.ny = e->hd.ny;
@@ -1068,6 +1087,8 @@ struct Tracers {
     T.substeps = cfg->substeps;
     T.order = cfg->order;
     T.seed = cfg->seed;
+    T.stretch = cfg->stretching ? 1 : 0;
+    blocks = (int)((n + TRC - 1) / TRC);
     velocity_skip = cfg->velocity_skip > 0 ? cfg->velocity_skip : 1;
     const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
     double *p, *v, *d, *u;
@@ -1103,23 +1124,94 @@ struct Tracers {
     T.id = ids;
     T.solid = sol;
     for (int a = 0; a < 3; ++a) T.u[a] = u + a * nodes;
+    if (T.stretch) {
+      double *rh, *lr, *part, *cg = nullptr;
+      if ((rc = alloc(&rh, 3 * n)) || (rc = alloc(&lr, n)) || (rc = alloc(&part, (size_t)blocks * NSTR)) ||
+          (rc = alloc(&ring, (size_t)ROWCAP * NROW)) || (cfg->phase_split && (rc = alloc(&cg, nodes))))
+        return rc;
+      if (cg) FE_CUDA(cudaMemset(cg, 0xFF, nodes * sizeof(double)));  // NaN on solid nodes
+      T.rho_hat = rh;
+      T.log_rho = lr;
+      T.part = part;
+      T.cgrid = cg;
+      if (n > 0) k_stretch_init<<<(unsigned)((n + TRC - 1) / TRC), TRC, 0, stream>>>(T, cfg->stretching_seed);
+      FE_CUDA(cudaGetLastError());
+      FE_CUDA(cudaStreamSynchronize(stream));
+    }
     return FE_OK;
   }
   int refresh() {
     double* u = const_cast<double*>(T.u[0]);
     const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
-    int rc = E->velocity_grid(u, u + nodes, u + 2 * nodes);
+    int rc = E->velocity_grid(u, u + nodes, u + 2 * nodes, const_cast<double*>(T.cgrid));
     if (!rc) have_u = true;
     return rc;
+  }
+  // A caller-given node-indexed velocity [3][nodes] (and order parameter
+  // [nodes], optional) used from now on instead of the engine's; u == NULL
+  // returns to the engine's velocity.
+  int set_velocity(const double* u, const double* c) {
+    const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
+    if (!u) {
+      frozen = false;
+      have_u = false;
+      return FE_OK;
+    }
+    FE_CUDA(cudaMemcpyAsync(const_cast<double*>(T.u[0]), u, 3 * nodes * sizeof(double), cudaMemcpyHostToDevice,
+                            stream));
+    if (c && T.cgrid)
+      FE_CUDA(cudaMemcpyAsync(const_cast<double*>(T.cgrid), c, nodes * sizeof(double), cudaMemcpyHostToDevice,
+                              stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
+    frozen = true;
+    have_u = true;
+    return FE_OK;
   }
   // One lattice step of the tracers on the engine's current velocity.
   int advance() {
     int rc;
-    if (!have_u || step % velocity_skip == 0)
+    if (!frozen && (!have_u || step % velocity_skip == 0))
       if ((rc = refresh())) return rc;
-    if (T.n > 0) k_tracers<<<(unsigned)((T.n + 127) / 128), 128, 0, stream>>>(T, step);
+    if (T.n > 0) {
+      k_tracers<<<(unsigned)blocks, TRC, 0, stream>>>(T, step);
+      if (T.stretch) k_stretch_row<<<1, 256, 0, stream>>>(T.part, blocks, T.substeps, T.n, step + 1, ring, ROWCAP);
+    }
     FE_CUDA(cudaGetLastError());
     ++step;
+    return FE_OK;
+  }
+  // Rows produced since the last call (oldest first), at most max_rows.
+  int rows(double* out, int64_t max_rows, int64_t* count) {
+    *count = 0;
+    if (!T.stretch) return fe_fail(FE_ERR_STATE, "tracers created without stretching");
+    const int64_t made = T.n > 0 ? step : 0;
+    if (made - drained > ROWCAP) {
+      const int64_t lost = made - drained - ROWCAP;
+      drained = made - ROWCAP;
+      return fe_fail(FE_ERR_STATE, "stretching rows overwritten before they were read (" + std::to_string(lost) +
+                                       " lost; read them at least every " + std::to_string(ROWCAP) + " steps)");
+    }
+    const int64_t k = std::min<int64_t>(made - drained, std::max<int64_t>(max_rows, 0));
+    for (int64_t r = 0; r < k; ++r) {
+      const int64_t row = drained + 1 + r;  // rows are numbered from 1
+      FE_CUDA(cudaMemcpyAsync(out + r * NROW, ring + (row % ROWCAP) * NROW, NROW * sizeof(double),
+                              cudaMemcpyDeviceToHost, stream));
+    }
+    FE_CUDA(cudaStreamSynchronize(stream));
+    drained += k;
+    *count = k;
+    return FE_OK;
+  }
+  int stretch_state(double* rho_hat, double* log_rho, bool upload) {
+    if (!T.stretch) return fe_fail(FE_ERR_STATE, "tracers created without stretching");
+    const auto dir = upload ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    if (rho_hat)
+      FE_CUDA(upload ? cudaMemcpyAsync(T.rho_hat, rho_hat, 3 * T.n * sizeof(double), dir, stream)
+                     : cudaMemcpyAsync(rho_hat, T.rho_hat, 3 * T.n * sizeof(double), dir, stream));
+    if (log_rho)
+      FE_CUDA(upload ? cudaMemcpyAsync(T.log_rho, log_rho, T.n * sizeof(double), dir, stream)
+                     : cudaMemcpyAsync(log_rho, T.log_rho, T.n * sizeof(double), dir, stream));
+    FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
   }
   int download(double* pos, double* vel) {
@@ -1190,6 +1282,8 @@ int fe_engine_create(const fe_params* p, int nx, int ny, int nz, const uint8_t* 
 int fe_engine_destroy(fe_engine* e) {
   if (!e) return FE_OK;
   if (e->e.owner) e->e.owner->remove(&e->e);
+  for (fe::Tracers* t : std::vector<fe::Tracers*>(e->e.tracer_sets)) t->detach();
+  e->e.tracer_sets.clear();
   cudaStreamSynchronize(e->e.stream);
   delete e;
   return FE_OK;
@@ -1624,13 +1718,47 @@ int fe_tracers_destroy(fe_tracers* t) {
 
 int fe_tracers_step(fe_tracers* t) {
   if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  if (!t->t.E) return fe_fail(FE_ERR_STATE, "the tracers' engine was destroyed");
   if (t->t.E->owner && t->t.E->owner->inflight) return fe_fail(FE_ERR_STATE, "engine's batch steps in flight");
   return t->t.advance();
 }
 
 int fe_tracers_download(fe_tracers* t, double* pos, double* vel) {
   if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  if (!t->t.E) return fe_fail(FE_ERR_STATE, "the tracers' engine was destroyed");
   return t->t.download(pos, vel);
+}
+
+int fe_tracers_stretch_rows(fe_tracers* t, double* rows, int64_t max_rows, int64_t* count) {
+  if (!t || !count || (max_rows > 0 && !rows)) return fe_fail(FE_ERR_ARG, "fe_tracers_stretch_rows: bad arguments");
+  if (!t->t.E) return fe_fail(FE_ERR_STATE, "the tracers' engine was destroyed");
+  return t->t.rows(rows, max_rows, count);
+}
+
+int fe_tracers_stretch_state(fe_tracers* t, double* rho_hat, double* log_rho) {
+  if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  if (!t->t.E) return fe_fail(FE_ERR_STATE, "the tracers' engine was destroyed");
+  return t->t.stretch_state(rho_hat, log_rho, false);
+}
+
+int fe_tracers_set_stretch_state(fe_tracers* t, const double* rho_hat, const double* log_rho) {
+  if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  if (!t->t.E) return fe_fail(FE_ERR_STATE, "the tracers' engine was destroyed");
+  if (rho_hat)
+    for (int64_t p = 0; p < t->t.T.n; ++p) {
+      const int64_t n = t->t.T.n;
+      const double g = std::sqrt(rho_hat[p] * rho_hat[p] + rho_hat[n + p] * rho_hat[n + p] +
+                                 rho_hat[2 * n + p] * rho_hat[2 * n + p]);
+      if (!(std::fabs(g - 1.0) <= 1e-6)) return fe_fail(FE_ERR_ARG, "rho_hat is not a unit vector");
+    }
+  return t->t.stretch_state(const_cast<double*>(rho_hat), const_cast<double*>(log_rho), true);
+}
+
+int fe_tracers_set_velocity(fe_tracers* t, const double* u, const double* c) {
+  if (!t) return fe_fail(FE_ERR_ARG, "null tracers");
+  if (!t->t.E) return fe_fail(FE_ERR_STATE, "the tracers' engine was destroyed");
+  if (t->t.E->owner && t->t.E->owner->inflight) return fe_fail(FE_ERR_STATE, "engine's batch steps in flight");
+  return t->t.set_velocity(u, c);
 }
 
 int fe_batch_launch_count(const fe_batch* b, int64_t* count) {

@@ -3,6 +3,8 @@
 // checkpoint, and particles_<step>.h5. Same dataset names, shapes and types;
 // no gzip (contiguous datasets: the reference's fast default is gzip off).
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -111,7 +113,7 @@ int fe_checkpoint_read(fe_engine* e, const char* path, uint32_t* step) {
 }
 
 int fe_write_particles_h5(const char* path, int64_t n, const double* pos, const double* vel, const int64_t* id,
-                          const double* dm, const int32_t* plane_id) {
+                          const double* dm, const int32_t* plane_id, const double* rho_hat, const double* log_rho) {
   if (!path || n < 1 || !pos) return fe_fail(FE_ERR_ARG, "fe_write_particles_h5: bad arguments");
   std::vector<double> p(3 * n), v;
   for (int64_t q = 0; q < n; ++q)
@@ -128,7 +130,52 @@ int fe_write_particles_h5(const char* path, int64_t n, const double* pos, const 
   sets.push_back({"id", fe::h5::I32, {(uint64_t)n}, ids.data()});
   if (dm) sets.push_back({"Dm", fe::h5::F64, {(uint64_t)n}, dm});
   if (plane_id) sets.push_back({"plane_id", fe::h5::I32, {(uint64_t)n}, plane_id});
+  std::vector<double> rh;
+  if (rho_hat) {
+    rh.resize(3 * n);
+    for (int64_t q = 0; q < n; ++q)
+      for (int a = 0; a < 3; ++a) rh[3 * q + a] = rho_hat[a * n + q];
+    sets.push_back({"rho_hat", fe::h5::F64, {(uint64_t)n, 3}, rh.data()});
+  }
+  if (log_rho) sets.push_back({"log_rho", fe::h5::F64, {(uint64_t)n}, log_rho});
   return fe::h5::write(path, sets);
+}
+
+// Text time series of the reference driver (felbm_gpu_main.cu:600-698): one
+// line per call, the header first when `header` (the file is then truncated).
+int fe_write_series(const char* path, int header, uint32_t iter, const double stats[6], int64_t n) {
+  if (!path || !stats || n < 1) return fe_fail(FE_ERR_ARG, "fe_write_series: bad arguments");
+  FILE* f = std::fopen(path, header ? "w" : "a");
+  if (!f) return fe_fail(FE_ERR_IO, std::string("cannot open ") + path);
+  if (header) std::fprintf(f, "# iter   max_speed   mean_ux   mean_uy   mean_uz   mean_v2   total_order_parameter\n");
+  const double inv = 1.0 / (double)n;
+  std::fprintf(f, "%u  %.10g  %.10g  %.10g  %.10g  %.10g  %.10g\n", iter, std::sqrt(stats[5]), stats[0] * inv,
+               stats[1] * inv, stats[2] * inv, stats[3] * inv, stats[4]);
+  const int bad = std::ferror(f);
+  std::fclose(f);
+  return bad ? fe_fail(FE_ERR_IO, std::string("write failed: ") + path) : FE_OK;
+}
+
+int fe_write_stretching(const char* path, int header, const double* rows, int64_t nrows) {
+  if (!path || nrows < 0 || (nrows > 0 && !rows)) return fe_fail(FE_ERR_ARG, "fe_write_stretching: bad arguments");
+  FILE* f = std::fopen(path, header ? "w" : "a");
+  if (!f) return fe_fail(FE_ERR_IO, std::string("cannot open ") + path);
+  if (header)
+    std::fprintf(f,
+                 "# Stretching of the tracers' material line elements, one row per tracer step.\n"
+                 "# lambda: mean of rho_hat . (grad u) rho_hat over the active tracers and substeps;\n"
+                 "# mean_log_rho, var_log_rho: over all tracers; n_active: tracers with no rejected\n"
+                 "# substep; lambda_w / lambda_nw: the same mean split by phase (c < 0.5 wetting),\n"
+                 "# nan when the phase has no sample; n_w, n_nw: phase samples / substeps.\n"
+                 "# step   lambda   mean_log_rho   var_log_rho   n_active   lambda_w   lambda_nw   n_w   n_nw\n");
+  for (int64_t r = 0; r < nrows; ++r) {
+    const double* v = rows + 9 * r;
+    std::fprintf(f, "%lld  %.10g  %.10g  %.10g  %lld  %.10g  %.10g  %.10g  %.10g\n", (long long)v[0], v[1], v[2],
+                 v[3], (long long)v[4], v[5], v[6], v[7], v[8]);
+  }
+  const int bad = std::ferror(f);
+  std::fclose(f);
+  return bad ? fe_fail(FE_ERR_IO, std::string("write failed: ") + path) : FE_OK;
 }
 
 // Generic read of one dataset of a file written here (tests, tools): the

@@ -121,6 +121,9 @@ class MultiPhaseGPU:
     # -- lifecycle --------------------------------------------------------
     def free(self):
         if self._h:
+            # tracers on this engine use its stream: they go first
+            for t in list(getattr(self, "_tracers", ())):
+                t.free()
             lib.fe_engine_destroy(self._h)
             self._h = None
 

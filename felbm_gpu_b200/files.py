@@ -34,7 +34,7 @@ def read_checkpoint(engine, path: str) -> int:
     return st.value
 
 
-def write_particles(path: str, pos, vel=None, ids=None, dm=None, plane_id=None):
+def write_particles(path: str, pos, vel=None, ids=None, dm=None, plane_id=None, rho_hat=None, log_rho=None):
     pos = np.ascontiguousarray(pos, np.float64).reshape(3, -1)
     n = pos.shape[1]
     keep = [pos]
@@ -47,7 +47,21 @@ def write_particles(path: str, pos, vel=None, ids=None, dm=None, plane_id=None):
         return a.ctypes.data_as(t)
     check(lib.fe_write_particles_h5(path.encode(), n, pos.ctypes.data_as(_dp), ptr(vel, np.float64, _dp),
                                     ptr(ids, np.int64, _i64), ptr(dm, np.float64, _dp),
-                                    ptr(plane_id, np.int32, _i32)))
+                                    ptr(plane_id, np.int32, _i32), ptr(rho_hat, np.float64, _dp),
+                                    ptr(log_rho, np.float64, _dp)))
+
+
+def write_series(path: str, iteration: int, stats, n_sites: int, header: bool = False):
+    """One line of series.txt from the six flow-statistics sums (header:
+    truncate and write the column line first)."""
+    st = np.ascontiguousarray(stats, np.float64)
+    check(lib.fe_write_series(path.encode(), int(header), int(iteration), st.ctypes.data_as(_dp), int(n_sites)))
+
+
+def write_stretching(path: str, rows, header: bool = False):
+    """Rows (k, 9) of Tracers.stretch_rows() appended to stretching.txt."""
+    r = np.ascontiguousarray(rows, np.float64).reshape(-1, 9)
+    check(lib.fe_write_stretching(path.encode(), int(header), r.ctypes.data_as(_dp), len(r)))
 
 
 def read_dataset(path: str, name: str) -> np.ndarray:

@@ -380,6 +380,9 @@ typedef struct fe_tracer_config {
   int order;                  /* 1 or 2 */
   int velocity_skip;          /* refresh the velocity every this many steps */
   uint64_t seed;
+  int stretching;             /* 1: material line elements (particles_stretching) */
+  int phase_split;            /* 1: split lambda by phase (particles_phase_split) */
+  uint64_t stretching_seed;   /* initial orientations (particles_stretching_seed) */
 } fe_tracer_config;
 /* n tracers at pos [3][n] with diffusivities dm [n] and ids [n] (NULL: 0..n-1;
  * the random stream of a tracer depends on its id). */
@@ -390,6 +393,32 @@ int fe_tracers_step(fe_tracers* t);
 /* pos, vel: [3][n] host arrays (either may be NULL); vel is the velocity
  * interpolated at each tracer's position at the end of the last step. */
 int fe_tracers_download(fe_tracers* t, double* pos, double* vel);
+/* Lagrangian stretching (reference README "Lagrangian stretching"; its
+ * ParticleManager half is in the absent felbm_local tree, the method is the
+ * one docs/HANDOFF_stretching.md section 2 states). Each tracer carries a unit
+ * orientation rho_hat (isotropic at creation, from stretching_seed) and
+ * log_rho (0 at creation); per accepted substep, with J the gradient of the
+ * interpolated velocity at the substep's start: lambda_s = rho_hat.J rho_hat
+ * (Eq. 12), r = rho_hat + dt J rho_hat, log_rho += log|r|,
+ * rho_hat = r / |r|. Every step leaves one row of the stretching.txt
+ * time series (felbm_gpu_main.cu:643-655): step (1, 2, ... since creation),
+ * lambda (mean over the active tracers and their substeps), mean_log_rho,
+ * var_log_rho (over all tracers), n_active (tracers with no rejected
+ * substep), lambda_w, lambda_nw (split by the phase of the nearest node,
+ * c < 1/2 wetting; NaN when that phase has no sample or phase_split is off),
+ * n_w, n_nw (samples / substeps; n_w + n_nw = n_active with phase_split).
+ * fe_tracers_stretch_rows hands out the rows made since its last call, oldest
+ * first, at most max_rows of 9 doubles; the device keeps the last 65536. */
+int fe_tracers_stretch_rows(fe_tracers* t, double* rows, int64_t max_rows, int64_t* count);
+/* rho_hat [3][n] and log_rho [n] (either may be NULL), for particle files
+ * and restarts; the setter checks that rho_hat holds unit vectors. */
+int fe_tracers_stretch_state(fe_tracers* t, double* rho_hat, double* log_rho);
+int fe_tracers_set_stretch_state(fe_tracers* t, const double* rho_hat, const double* log_rho);
+/* Advect on a caller-given node-indexed velocity u [3][nodes] (solid nodes 0)
+ * and, with phase_split, order parameter c [nodes] (may be NULL), held until
+ * the next call, instead of the engine's; u == NULL returns to the engine's
+ * velocity. (A frozen field, or an analytic one for tests.) */
+int fe_tracers_set_velocity(fe_tracers* t, const double* u, const double* c);
 /* Seeding (reference particles_init_mode): mode 0 uniform in the fluid
  * volume (count tracers); mode 1 planes normal to `axis` at the coordinates
  * offsets[0..nplanes-1], count tracers per plane, each plane resampled until
@@ -418,9 +447,19 @@ int fe_checkpoint_write(fe_engine* e, const char* path, uint32_t step);
 int fe_settle_mass_correction(fe_engine* e);
 int fe_checkpoint_read(fe_engine* e, const char* path, uint32_t* step);
 /* particles_<step>.h5: position [n][3], velocity [n][3] (if vel), id, Dm (if
- * dm), plane_id (if plane_id); pos and vel as [3][n] (fe_tracers_download). */
+ * dm), plane_id (if plane_id), rho_hat [n][3] and log_rho [n] (if given);
+ * pos, vel and rho_hat as [3][n] (fe_tracers_download). */
 int fe_write_particles_h5(const char* path, int64_t n, const double* pos, const double* vel, const int64_t* id,
-                          const double* dm, const int32_t* plane_id);
+                          const double* dm, const int32_t* plane_id, const double* rho_hat, const double* log_rho);
+/* The driver's text time series (felbm_gpu_main.cu:600-698), one line per
+ * call; header != 0 truncates the file and writes the column line first.
+ * series.txt (timeseries_file): iter max_speed mean_ux mean_uy mean_uz mean_v2
+ * total_order_parameter, from the six fe_flow_stats sums of n sites.
+ * stretching.txt (particles_stretching_file): nrows rows of
+ * fe_tracers_stretch_rows (step lambda mean_log_rho var_log_rho n_active
+ * lambda_w lambda_nw n_w n_nw). */
+int fe_write_series(const char* path, int header, uint32_t iter, const double stats[6], int64_t n);
+int fe_write_stretching(const char* path, int header, const double* rows, int64_t nrows);
 /* One dataset of a file written here: type 0 double, 1 float, 2 int32,
  * 3 uint32; dims[rank]; raw bytes into data (NULL: shape only). */
 int fe_h5_read_dataset(const char* path, const char* name, int* type, int64_t* dims, int* rank, void* data,

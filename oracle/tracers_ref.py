@@ -8,7 +8,10 @@ periodic wrap, Euler or Heun substeps, Brownian kicks sqrt(2 Dm dt) N(0,1)
 from Philox4x32-10 (Salmon et al. 2011) with counter (id, step, substep,
 draw) and the seed as key, Box-Muller normals from 53-bit uniforms, no z kick
 in 2-D (where tracers do not move along z at all), moves onto solid nodes
-rejected.
+rejected; optional Lagrangian stretching (unit orientation rho_hat and
+log_rho per tracer, lambda_s = rho_hat . J rho_hat per accepted substep with J
+the gradient of the trilinear interpolant, Benettin renormalisation, the
+step's row of the stretching time series).
 """
 from __future__ import annotations
 
@@ -84,6 +87,38 @@ def interp(u, shape, x, y, z):
     return out
 
 
+def interp_grad(u, shape, x, y, z):
+    """Velocity (3 arrays) and its gradient J[a][b] = d u_a / d x_b of the
+    trilinear interpolant."""
+    nz, ny, nx = shape
+    fx, fy, fz = np.floor(x), np.floor(y), np.floor(z)
+    ax, ay, az = x - fx, y - fy, z - fz
+    x0, y0, z0 = fx.astype(np.int64) % nx, fy.astype(np.int64) % ny, fz.astype(np.int64) % nz
+    xs, ys, zs = (x0, (x0 + 1) % nx), (y0, (y0 + 1) % ny), (z0, (z0 + 1) % nz)
+    wx, wy, wz = (1 - ax, ax), (1 - ay, ay), (1 - az, az)
+    v = interp(u, shape, x, y, z)
+    J = [[np.zeros_like(x) for _ in range(3)] for _ in range(3)]
+    for q in range(8):
+        bx, by, bz = q & 1, (q >> 1) & 1, q >> 2
+        idx = xs[bx] + nx * (ys[by] + ny * zs[bz])
+        sx, sy, sz = (1.0 if bx else -1.0), (1.0 if by else -1.0), (1.0 if bz else -1.0)
+        for a in range(3):
+            uq = u[a][idx]
+            J[a][0] = J[a][0] + sx * wy[by] * wz[bz] * uq
+            J[a][1] = J[a][1] + sy * wx[bx] * wz[bz] * uq
+            J[a][2] = J[a][2] + sz * wx[bx] * wy[by] * uq
+    return v, J
+
+
+def orientations(ids, seed: int):
+    """Isotropic unit vectors (3, n): three Philox normals per tracer (counter
+    id, step 2^32 - 1, draws 0 and 1), normalised."""
+    a, b = normal_pair(seed, ids, 0xFFFFFFFF, 0, 0)
+    c, _ = normal_pair(seed, ids, 0xFFFFFFFF, 0, 1)
+    g = np.sqrt(a * a + b * b + c * c)
+    return np.stack([a / g, b / g, c / g])
+
+
 def blocked(solid_flat, shape, x, y, z):
     nz, ny, nx = shape
     ix = np.floor(x + 0.5).astype(np.int64) % nx
@@ -92,17 +127,31 @@ def blocked(solid_flat, shape, x, y, z):
     return solid_flat[ix + nx * (iy + ny * iz)] != 0
 
 
-def step(pos, dm, ids, u, solid, step_index: int, substeps: int = 1, order: int = 2, seed: int = 0):
-    """One lattice step of all tracers; returns (pos, vel), each (3, n)."""
+def step(pos, dm, ids, u, solid, step_index: int, substeps: int = 1, order: int = 2, seed: int = 0, stretch=None,
+         cgrid=None):
+    """One lattice step of all tracers; returns (pos, vel), each (3, n). With
+    stretch = (rho_hat (3, n), log_rho (n,)) also the new rho_hat, log_rho and
+    the step's row (step_index + 1, lambda, mean_log_rho, var_log_rho,
+    n_active, lambda_w, lambda_nw, n_w, n_nw); cgrid: node-indexed order
+    parameter for the phase split (c < 0.5 wetting), or None."""
     shape = solid.shape
     nz, ny, nx = shape
     sf = np.ascontiguousarray(solid, np.uint8).reshape(-1)
     x, y, z = (np.array(pos[a], np.float64) for a in range(3))
+    n = len(x)
     dt = 1.0 / substeps
     kick = np.where(dm > 0.0, np.sqrt(2.0 * np.maximum(dm, 0.0) * dt), 0.0)
     move = kick > 0.0
+    if stretch is not None:
+        rh = np.array(stretch[0], np.float64).reshape(3, n)
+        lr = np.array(stretch[1], np.float64)
+        active = np.ones(n, bool)
+        lam, lw, lnw, cw, cnw = (np.zeros(n) for _ in range(5))
     for s in range(substeps):
-        k1 = interp(u, shape, x, y, z)
+        if stretch is not None:
+            k1, J = interp_grad(u, shape, x, y, z)
+        else:
+            k1 = interp(u, shape, x, y, z)
         if order == 1:
             nxp, nyp, nzp = x + dt * k1[0], y + dt * k1[1], z + dt * k1[2]
         else:
@@ -120,6 +169,32 @@ def step(pos, dm, ids, u, solid, step_index: int, substeps: int = 1, order: int 
         nxp, nyp = _wrap(nxp, nx), _wrap(nyp, ny)
         nzp = _wrap(nzp, nz) if nz > 1 else z  # 2-D: no motion along z
         ok = ~blocked(sf, shape, nxp, nyp, nzp)
+        if stretch is not None:
+            active &= ok
+            jr = [J[i][0] * rh[0] + J[i][1] * rh[1] + J[i][2] * rh[2] for i in range(3)]
+            ls = rh[0] * jr[0] + rh[1] * jr[1] + rh[2] * jr[2]
+            lam = np.where(ok, lam + ls, lam)
+            if cgrid is not None:
+                ix = np.floor(x + 0.5).astype(np.int64) % nx
+                iy = np.floor(y + 0.5).astype(np.int64) % ny
+                iz = np.floor(z + 0.5).astype(np.int64) % nz
+                cv = np.asarray(cgrid)[ix + nx * (iy + ny * iz)]
+                w, nw = ok & (cv < 0.5), ok & (cv >= 0.5)
+                lw, cw = np.where(w, lw + ls, lw), cw + w
+                lnw, cnw = np.where(nw, lnw + ls, lnw), cnw + nw
+            r = [rh[i] + dt * jr[i] for i in range(3)]
+            g = np.sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2])
+            lr = np.where(ok, lr + np.log(g), lr)
+            rh = np.where(ok, np.stack([r[0] / g, r[1] / g, r[2] / g]), rh)
         x, y, z = np.where(ok, nxp, x), np.where(ok, nyp, y), np.where(ok, nzp, z)
     vel = interp(u, shape, x, y, z)
-    return np.stack([x, y, z]), np.stack(vel)
+    if stretch is None:
+        return np.stack([x, y, z]), np.stack(vel)
+    nact = float(active.sum())
+    S = float(substeps)
+    sw, sn = float(cw[active].sum()), float(cnw[active].sum())
+    mean = lr.sum() / n
+    row = np.array([step_index + 1, lam[active].sum() / (nact * S) if nact else np.nan, mean,
+                    (lr * lr).sum() / n - mean * mean, nact,
+                    lw[active].sum() / sw if sw else np.nan, lnw[active].sum() / sn if sn else np.nan, sw / S, sn / S])
+    return np.stack([x, y, z]), np.stack(vel), rh, lr, row

@@ -92,3 +92,33 @@ def test_reader_rejects_other_files(tmp_path):
         raise AssertionError("no error")
     except Exception as ex:
         assert "not an HDF5 file" in str(ex)
+
+
+def test_series_and_stretching_text(tmp_path):
+    p = str(tmp_path / "series.txt")
+    st = np.array([2.0, -4.0, 6.0, 8.0, 123.5, 0.25])
+    files.write_series(p, 0, st, 4, header=True)
+    files.write_series(p, 10, st * 2, 4)
+    lines = open(p).read().splitlines()
+    assert lines[0].split()[1:] == ["iter", "max_speed", "mean_ux", "mean_uy", "mean_uz", "mean_v2",
+                                    "total_order_parameter"]
+    d = np.loadtxt(p)
+    assert np.allclose(d[0], [0, 0.5, 0.5, -1.0, 1.5, 2.0, 123.5])
+    assert np.allclose(d[1], [10, np.sqrt(0.5), 1.0, -2.0, 3.0, 4.0, 247.0])
+    q = str(tmp_path / "stretching.txt")
+    rows = np.array([[1, 0.1, 0.01, 0.001, 50, 0.12, np.nan, 50, 0], [2, 0.2, 0.02, 0.002, 49, 0.3, 0.1, 20, 29]])
+    files.write_stretching(q, rows[:1], header=True)
+    files.write_stretching(q, rows[1:])
+    cols = [l for l in open(q).read().splitlines() if l.startswith("#")][-1].split()[1:]
+    assert cols == ["step", "lambda", "mean_log_rho", "var_log_rho", "n_active", "lambda_w", "lambda_nw", "n_w",
+                    "n_nw"]
+    assert np.allclose(np.loadtxt(q), rows, equal_nan=True)
+
+
+def test_particles_with_line_elements(tmp_path):
+    rng = np.random.default_rng(3)
+    pos, rh, lr = rng.random((3, 9)), rng.random((3, 9)), rng.random(9)
+    p = str(tmp_path / "particles_5.h5")
+    files.write_particles(p, pos, rho_hat=rh, log_rho=lr)
+    assert np.array_equal(files.read_dataset(p, "rho_hat"), rh.T)
+    assert np.array_equal(files.read_dataset(p, "log_rho"), lr)

@@ -77,3 +77,74 @@ def test_oracle_2d_no_z_kick():
     for t in range(5):
         pos, _ = tr.step(pos, np.full(50, 0.1), np.arange(50), u, solid, t)
     assert np.all(pos[2] == 0.0) and np.std(pos[0]) > 0
+
+
+def _fluid_box(nx=40, ny=40, nz=8):
+    return np.zeros((nz, ny, nx), np.uint8)
+
+
+def _linear_field(solid, fn):
+    nz, ny, nx = solid.shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ux, uy, uz = fn(x.astype(float), y.astype(float), z.astype(float))
+    return np.stack([np.broadcast_to(a, solid.shape).reshape(-1) for a in (ux, uy, uz)]).astype(np.float64)
+
+
+def test_stretching_uniform_shear_is_exact():
+    """u = (g y, 0, 0): J is nilpotent, so the Euler update of the line
+    element is exact and log|rho| = log|rho0 + t J rho0| (reference analytic
+    test, docs/HANDOFF_stretching.md section 3.3: shear error ~4e-15)."""
+    solid = _fluid_box()
+    gam = 0.01
+    u = _linear_field(solid, lambda x, y, z: (gam * y, 0 * y, 0 * y))
+    n = 64
+    rng = np.random.default_rng(1)
+    pos = np.stack([rng.uniform(5, 10, n), rng.uniform(8, 30, n), rng.uniform(2, 5, n)])
+    ids = np.arange(n)
+    rh0 = tr.orientations(ids, 5)
+    rh, lr = rh0.copy(), np.zeros(n)
+    steps, subs = 20, 3
+    for s in range(steps):
+        pos, _, rh, lr, row = tr.step(pos, np.zeros(n), ids, u, solid, s, substeps=subs, order=1, stretch=(rh, lr))
+    J = np.array([[0, gam, 0], [0, 0, 0], [0, 0, 0]])
+    want = np.log(np.linalg.norm(rh0 + steps * (J @ rh0), axis=0))
+    assert np.max(np.abs(lr - want)) < 1e-13, np.max(np.abs(lr - want))
+    assert np.max(np.abs(np.linalg.norm(rh, axis=0) - 1.0)) < 1e-14
+    assert row[0] == steps and row[4] == n
+    # Eq. (12) of the last step: mean of gamma rho_x rho_y over tracers and substeps
+    assert np.isfinite(row[1]) and np.isnan(row[5]) and np.isnan(row[6])
+
+
+def test_stretching_rotation_has_zero_lambda():
+    """Solid-body rotation: J antisymmetric, so Eq. (12) is zero to rounding
+    while explicit Euler inflates |rho| (the reference's rotation case)."""
+    solid = _fluid_box()
+    om = 0.02
+    u = _linear_field(solid, lambda x, y, z: (-om * (y - 20), om * (x - 20), 0 * z))
+    n = 50
+    rng = np.random.default_rng(2)
+    pos = np.stack([rng.uniform(17, 23, n), rng.uniform(17, 23, n), rng.uniform(2, 5, n)])
+    ids = np.arange(n)
+    rh, lr = tr.orientations(ids, 9), np.zeros(n)
+    for s in range(10):
+        pos, _, rh, lr, row = tr.step(pos, np.zeros(n), ids, u, solid, s, substeps=2, order=2, stretch=(rh, lr))
+        assert abs(row[1]) < 1e-16
+    assert np.all(lr > 0) and np.max(lr) < 10 * 2 * 0.5 * np.log1p((om * 0.5) ** 2) + 1e-15
+
+
+def test_stretching_phase_split_recombines():
+    """n_w + n_nw = n_active and (n_w lambda_w + n_nw lambda_nw) / n_active =
+    lambda (reference checks, docs/HANDOFF_stretching.md section 4)."""
+    solid = geometry.spheres((12, 30, 30), 2.5, 6, 2.0, 3)
+    nz, ny, nx = solid.shape
+    u = _linear_field(solid, lambda x, y, z: (0.01 * np.sin(y / 5.0), 0.004 * np.cos(x / 4.0), 0.002 * np.sin(z)))
+    u[:, solid.reshape(-1) != 0] = 0.0
+    cg = _linear_field(solid, lambda x, y, z: (0.5 + 0.5 * np.sin(x / 3.0), 0 * x, 0 * x))[0]
+    pos, _ = seed(solid, 300, rng_seed=4)
+    ids = np.arange(300)
+    rh, lr = tr.orientations(ids, 1), np.zeros(300)
+    for s in range(6):
+        pos, _, rh, lr, row = tr.step(pos, np.full(300, 1e-3), ids, u, solid, s, substeps=2, stretch=(rh, lr),
+                                      cgrid=cg)
+        assert row[7] + row[8] == row[4]
+        assert abs((row[7] * row[5] + row[8] * row[6]) / row[4] - row[1]) < 1e-14

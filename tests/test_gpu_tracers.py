@@ -113,3 +113,89 @@ def test_2d_tracers_stay_in_plane(require_gpu):
     finally:
         e.free()
     assert np.all(p[2] == 0.0) and np.max(np.abs(p[:2] - pos0[:2])) > 0
+
+
+def _cgrid(solid, f):
+    nodes = geometry.site_nodes(solid)
+    c = np.full(solid.size, np.nan)
+    c[nodes] = f["c"]
+    return c
+
+
+def test_stretching_matches_restatement_on_engine_velocity(require_gpu):
+    """Material line elements and the stretching rows (lambda, <log rho>,
+    its variance, n_active, phase split) against the restatement, step for
+    step on the engine's own velocity and order parameter, FP64, 1e-10."""
+    case = make_case("spheres_mrt_wet", gx=2e-4)
+    e = MultiPhaseGPU(with_storage(case.params, "f64"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        n = 240
+        pos0, _ = seed(case.solid, n, rng_seed=6)
+        dm = np.where(np.arange(n) % 3 == 0, 2e-3, 0.0)
+        ids = np.arange(n) + 7
+        t = Tracers(e, pos0, dm, ids=ids, substeps=2, order=2, rng_seed=11, stretching=True, stretching_seed=77)
+        rh, lr = t.stretch_state()
+        assert np.max(np.abs(rh - tr.orientations(ids, 77))) <= 1e-13 and np.all(lr == 0.0)
+        pos, rows = pos0.copy(), []
+        for s in range(25):
+            e.run(1)
+            t.step()
+            f = e.download()
+            pos, _, rh, lr, row = tr.step(pos, dm, ids, grid(case.solid, f), case.solid, s, substeps=2, order=2,
+                                          seed=11, stretch=(rh, lr), cgrid=_cgrid(case.solid, f))
+            rows.append(row)
+        got = t.stretch_rows()
+        grh, glr = t.stretch_state()
+        gp, _ = t.download()
+        t.free()
+    finally:
+        e.free()
+    want = np.array(rows)
+    assert got.shape == want.shape
+    assert np.array_equal(got[:, 0], np.arange(1, 26)) and np.array_equal(got[:, 4], want[:, 4])
+    assert np.allclose(got, want, rtol=1e-9, atol=1e-12, equal_nan=True), np.nanmax(np.abs(got - want))
+    assert np.all(got[:, 7] + got[:, 8] == got[:, 4])
+    assert np.max(np.abs(gp - pos)) <= 1e-10
+    assert np.max(np.abs(grh - rh)) <= 1e-10 and np.max(np.abs(glr - lr)) <= 1e-10
+    assert np.max(np.abs(np.linalg.norm(grh, axis=0) - 1.0)) <= 1e-14
+    assert np.max(np.abs(glr)) > 1e-6          # the elements stretched
+
+
+def test_stretching_uniform_shear_exact_on_frozen_field(require_gpu):
+    """A frozen analytic shear u = (g y, 0, 0): the line elements follow
+    log|rho0 + t J rho0| to rounding; trajectories equal those without
+    stretching bit for bit."""
+    solid = np.zeros((8, 40, 40), np.uint8)
+    case = make_case("fluid_bgk")
+    e = MultiPhaseGPU(with_storage(case.params, "f64"), solid)
+    gam = 0.01
+    z, y, x = np.meshgrid(np.arange(8), np.arange(40), np.arange(40), indexing="ij")
+    u = np.stack([(gam * y).reshape(-1), np.zeros(solid.size), np.zeros(solid.size)]).astype(np.float64)
+    n = 64
+    rng = np.random.default_rng(1)
+    pos0 = np.stack([rng.uniform(5, 10, n), rng.uniform(8, 30, n), rng.uniform(2, 5, n)])
+    try:
+        t = Tracers(e, pos0, 0.0, substeps=3, order=1, stretching=True, stretching_seed=5)
+        plain = Tracers(e, pos0, 0.0, substeps=3, order=1)
+        rh0, _ = t.stretch_state()
+        for tt in (t, plain):
+            tt.set_velocity(u)
+        for _ in range(20):
+            t.step()
+            plain.step()
+        _, lr = t.stretch_state()
+        p1, v1 = t.download()
+        p2, v2 = plain.download()
+        rows = t.stretch_rows(max_rows=8)
+        rest = t.stretch_rows()
+        t.free()
+        plain.free()
+    finally:
+        e.free()
+    J = np.array([[0, gam, 0], [0, 0, 0], [0, 0, 0]])
+    want = np.log(np.linalg.norm(rh0 + 20 * (J @ rh0), axis=0))
+    assert np.max(np.abs(lr - want)) < 1e-13
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+    assert len(rows) == 8 and len(rest) == 12 and np.array_equal(np.r_[rows[:, 0], rest[:, 0]], np.arange(1, 21))
+    assert np.all(rows[:, 4] == n) and np.all(np.isnan(rows[:, 5]))
