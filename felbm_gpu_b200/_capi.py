@@ -170,6 +170,8 @@ SIGNATURES = {
     "fe_settle_mass_correction": (C.c_int, [_vp]),
     "fe_checkpoint_read": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_uint32)]),
     "fe_write_particles_h5": (C.c_int, [C.c_char_p, C.c_int64, _dp, _dp, _i64p, _dp, _i32p, _dp, _dp]),
+    "fe_geom_tiff_stack": (C.c_int, [C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _u8p,
+                                     C.c_int64]),
     "fe_write_series": (C.c_int, [C.c_char_p, C.c_int, C.c_uint32, _dp, C.c_int64]),
     "fe_write_stretching": (C.c_int, [C.c_char_p, C.c_int, _dp, C.c_int64]),
     "fe_h5_read_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _i64p, C.POINTER(C.c_int),

@@ -72,6 +72,34 @@ def open_lists(solid: np.ndarray, flow_axis: int, buffer_layers: int, split_axis
     return inl, outl, bv, br, coord
 
 
+def tiff_stack(source, extension: str = "tif", solid_nonzero: bool = True, invert: bool = False,
+               coarsening_levels: int = 0, subvolume=None) -> np.ndarray:
+    """Solid mask (nz, ny, nx) of a segmented TIFF stack (reference
+    domain_geometry = 3d_image). source: a directory (every *.extension file
+    in it, in name order, as the reference's image_dir) or a list of files.
+    subvolume: (x0, y0, z0, sx, sy, sz) in full-resolution voxels."""
+    import os
+    if isinstance(source, (str, os.PathLike)) and os.path.isdir(source):
+        files = sorted(os.path.join(source, f) for f in os.listdir(source) if f.endswith("." + extension))
+    elif isinstance(source, (str, os.PathLike)):
+        files = [str(source)]
+    else:
+        files = [str(f) for f in source]
+    if not files:
+        raise ValueError(f"no *.{extension} file in {source}")
+    arr = (C.c_char_p * len(files))(*[f.encode() for f in files])
+    sub = None
+    if subvolume is not None:
+        sub = (C.c_int32 * 6)(*[int(v) for v in subvolume])
+    dims = (C.c_int32 * 3)()
+    args = (arr, len(files), int(solid_nonzero), int(invert), int(coarsening_levels), sub, dims)
+    check(lib.fe_geom_tiff_stack(*args, None, 0))
+    nx, ny, nz = dims
+    out = np.empty((nz, ny, nx), np.uint8)
+    check(lib.fe_geom_tiff_stack(*args, out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size))
+    return out
+
+
 def site_nodes(solid: np.ndarray) -> np.ndarray:
     solid = np.ascontiguousarray(solid, np.uint8)
     nz, ny, nx = solid.shape

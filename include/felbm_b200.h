@@ -231,6 +231,17 @@ int fe_geom_pad_open(const uint8_t* medium, int mx, int my, int mz, int flow_axi
 int fe_geom_open_lists(const uint8_t* solid, int nx, int ny, int nz, int flow_axis, int buffer_layers,
                        int split_axis, int32_t* n_counts, int32_t* inlet, int32_t* outlet,
                        int32_t* buf_verts, int32_t* buf_refs, double* inlet_coord);
+/* Segmented TIFF stack (reference domain_geometry = 3d_image; keys of
+ * cfg/3d_image/domain.cfg). paths: the files in z order (each page one z
+ * slice; baseline TIFF, either byte order, grey 1/8/16 bits, uncompressed or
+ * PackBits). Solid where the voxel is nonzero (solid_nonzero, the
+ * interface_solid key) or zero, inverted when invert (invert_image).
+ * subvolume (x0, y0, z0, sx, sy, sz in full-resolution voxels, or NULL:
+ * use_subvolume) is cut first; then coarsening_levels halvings of every axis
+ * longer than 1 (trailing odd layer dropped; solid when at least half the
+ * fine voxels are). dims out: nx, ny, nz; solid NULL asks for dims only. */
+int fe_geom_tiff_stack(const char* const* paths, int npaths, int solid_nonzero, int invert, int coarsening_levels,
+                       const int* subvolume, int* dims, uint8_t* solid, int64_t capacity);
 /* Site count and node index of each site (SubDomain::idx_to_coords). */
 int fe_geom_sites(const uint8_t* solid, int nx, int ny, int nz, int64_t* n, int64_t* nodes);
 /* Order parameter per site: kind 0 uniform, 1 slab_interface, 2 spherical_droplet. */
