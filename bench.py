@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the served sweep and request stream")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the layout autotuner (default bricks, two steps per graph launch)")
+    ap.add_argument("--brick", default="auto", choices=["auto", "8x8x8", "8x8x4", "16x8x8"],
+                    help="force a brick shape (skips the autotuner)")
     ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per solve of the 64-solve sweep")
     ap.add_argument("--stream-seconds", type=float, default=15.0, help="arrival window of the request stream")
     ap.add_argument("--stream-rate", type=float, default=4.0, help="Poisson arrival rate (requests / s)")
@@ -154,14 +158,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(storage: str, size: int):
-    """Per-launch DRAM bytes of the collide kernel from the committed ncu
-    summary (profiles/collide_traffic.json), scaled to this lattice."""
+def profiled_traffic(storage: str, size: int, brick: str = "8x8x8"):
+    """Per-site DRAM bytes of the collide kernel with this brick from the
+    committed ncu summary (profiles/collide_traffic.json), to be scaled to
+    this lattice; None when that layout was not captured."""
     path = os.path.join(ROOT, "profiles", "collide_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        rec = d.get(storage)
+        rec = (d.get(storage) or {}).get(brick)
         if rec:
             return rec["bytes_per_site"]
     except Exception:
@@ -395,8 +400,17 @@ def main():
     from felbm_gpu_b200 import _capi
     solid, por, p, h0, g0 = workload(args.size, seed=2024 + rank)
     p.storage = _capi.STORAGE[args.storage]
+    tuned = None
+    if args.brick != "auto":
+        p.brick = _capi.BRICK[args.brick]
+    elif not args.no_autotune:
+        # the layout autotuner on this lattice (outside the timed region); the
+        # engine below (brick "auto") takes its choice
+        from felbm_gpu_b200.engine import autotune
+        tuned = autotune(p, solid, steps=30, device=lrank)
     eng = MultiPhaseGPU(p, solid, device=lrank)
     n = eng.n
+    brick, graph_steps = eng.layout()
     eng.upload_state(h0, g0)
     eng.record_target_mass()
     eng.run(max(args.warmup, 3))
@@ -429,7 +443,7 @@ def main():
     peak, peak_kind = measured_peak()
     t_p4 = kms[4] / 1e3
     achieved = B_P4[args.storage] * n / t_p4 / 1e9
-    tr = profiled_traffic(args.storage, args.size)
+    tr = profiled_traffic(args.storage, args.size, brick)
     roof = {"bound": "hbm", "kernel": "k_collide (P4: equilibria + Guo force + MRT, push streaming)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind,
@@ -489,7 +503,9 @@ def main():
                                        f"periodic, body force 1e-6, fused MRT, theta 45, correct_op_mass, "
                                        f"slab IC, {args.storage} populations",
                            "sites": int(n), "porosity": por, "parallelism": f"replicas x{ws}",
-                           "l2": "inputs larger than L2 (state > 1 GB), no flush"},
+                           "l2": "inputs larger than L2 (state > 1 GB), no flush",
+                           "layout": {"brick": brick, "graph_steps": graph_steps,
+                                      "autotune": tuned["candidates"] if tuned else None}},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk.summary(), "serving": serving}
         print(json.dumps(line), flush=True)

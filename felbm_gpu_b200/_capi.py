@@ -43,6 +43,7 @@ class FeParams(C.Structure):
         ("mrt_fast_transform", C.c_int), ("stream_inplace", C.c_int),
         ("storage", C.c_int),
         ("c_ref", C.c_double), ("p_ref", C.c_double),
+        ("brick", C.c_int), ("graph_steps", C.c_int),
     ]
 
 
@@ -69,6 +70,14 @@ _dp = C.POINTER(C.c_double)
 
 class FeFields(C.Structure):
     _fields_ = [("rho", _dp), ("c", _dp), ("ux", _dp), ("uy", _dp), ("uz", _dp), ("p", _dp), ("mu", _dp)]
+
+
+class FeTuneReport(C.Structure):
+    _fields_ = [("brick", C.c_int), ("graph_steps", C.c_int), ("ncand", C.c_int), ("cand_brick", C.c_int * 8),
+                ("cand_graph_steps", C.c_int * 8), ("cand_mlups", C.c_double * 8)]
+
+
+BRICK = {"auto": 0, "8x8x8": 1, "16x16x1": 2, "8x8x4": 3, "16x8x8": 4}
 
 
 class FeTracerConfig(C.Structure):
@@ -172,6 +181,12 @@ SIGNATURES = {
     "fe_write_particles_h5": (C.c_int, [C.c_char_p, C.c_int64, _dp, _dp, _i64p, _dp, _i32p, _dp, _dp]),
     "fe_geom_tiff_stack": (C.c_int, [C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _u8p,
                                      C.c_int64]),
+    "fe_autotune": (C.c_int, [C.POINTER(FeParams), C.c_int, C.c_int, C.c_int, _u8p, C.c_int, C.c_int,
+                              C.POINTER(FeTuneReport)]),
+    "fe_engine_layout": (C.c_int, [_vp, _i32p, _i32p]),
+    "fe_tune_save": (C.c_int, [C.c_char_p]),
+    "fe_tune_load": (C.c_int, [C.c_char_p]),
+    "fe_tune_clear": (C.c_int, []),
     "fe_write_series": (C.c_int, [C.c_char_p, C.c_int, C.c_uint32, _dp, C.c_int64]),
     "fe_write_stretching": (C.c_int, [C.c_char_p, C.c_int, _dp, C.c_int64]),
     "fe_h5_read_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _i64p, C.POINTER(C.c_int),

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/felbm_b200.h"
@@ -42,23 +43,55 @@ void fe_clear_error() { g_last_error.clear(); }
   } while (0)
 
 // Run CALL with S (storage traits) and Sh (brick shape) bound to the engine's.
-// Inside CALL, write template argument commas as FE_COMMA.
+// Inside CALL, write template argument commas as FE_COMMA. Shapes: 0 8x8x8,
+// 1 16x16x1, 2 8x8x4, 3 16x8x8; the last two exist for FP64 and FP32 only.
 #define FE_COMMA ,
-#define FE_DISPATCH(E, CALL)                                                   \
-  switch ((E).storage * 2 + (E).shape2d) {                                     \
-    case 0: { using S = StF64; using Sh = Shape3D; CALL; } break;              \
-    case 1: { using S = StF64; using Sh = Shape2D; CALL; } break;              \
-    case 2: { using S = StF32; using Sh = Shape3D; CALL; } break;              \
-    case 3: { using S = StF32; using Sh = Shape2D; CALL; } break;              \
-    case 4: { using S = StF16S; using Sh = Shape3D; CALL; } break;             \
-    case 5: { using S = StF16S; using Sh = Shape2D; CALL; } break;             \
-    case 6: { using S = StBF16S; using Sh = Shape3D; CALL; } break;            \
-    case 7: { using S = StBF16S; using Sh = Shape2D; CALL; } break;            \
-    case 8: { using S = StF16G; using Sh = Shape3D; CALL; } break;             \
-    case 9: { using S = StF16G; using Sh = Shape2D; CALL; } break;             \
-    case 10: { using S = StBF16G; using Sh = Shape3D; CALL; } break;           \
-    default: { using S = StBF16G; using Sh = Shape2D; CALL; } break;           \
+#define FE_SHAPES_ALL(E, ...)                                                  \
+  switch ((E).shape) {                                                         \
+    case 1: { using Sh = Shape2D; __VA_ARGS__; } break;                       \
+    case 2: { using Sh = Shape3D_H; __VA_ARGS__; } break;                     \
+    case 3: { using Sh = Shape3D_W; __VA_ARGS__; } break;                     \
+    default: { using Sh = Shape3D; __VA_ARGS__; } break;                      \
   }
+#define FE_SHAPES_BASE(E, ...)                                                 \
+  if ((E).shape == 1) { using Sh = Shape2D; __VA_ARGS__; }                    \
+  else { using Sh = Shape3D; __VA_ARGS__; }
+#define FE_DISPATCH(E, ...)                                                    \
+  switch ((E).storage) {                                                       \
+    case FE_F64: { using S = StF64; FE_SHAPES_ALL(E, __VA_ARGS__) } break;     \
+    case FE_F32: { using S = StF32; FE_SHAPES_ALL(E, __VA_ARGS__) } break;     \
+    case FE_F16S: { using S = StF16S; FE_SHAPES_BASE(E, __VA_ARGS__) } break;  \
+    case FE_BF16S: { using S = StBF16S; FE_SHAPES_BASE(E, __VA_ARGS__) } break; \
+    case FE_F16G: { using S = StF16G; FE_SHAPES_BASE(E, __VA_ARGS__) } break;  \
+    default: { using S = StBF16G; FE_SHAPES_BASE(E, __VA_ARGS__) } break;      \
+  }
+
+template <class Sh>
+struct ShTag {
+  using type = Sh;
+};
+template <class S, class Fn>
+static void with_shape(int shape, Fn&& fn);
+
+// Storages with the alternative 3-D bricks compiled.
+template <class S>
+constexpr bool kAllShapes = std::is_same<S, StF64>::value || std::is_same<S, StF32>::value;
+constexpr int NSHAPE = 4;
+// log2 of the brick extents per shape
+constexpr int kShapeLb[NSHAPE][3] = {{3, 3, 3}, {4, 4, 0}, {3, 3, 2}, {4, 3, 3}};
+// Call fn(ShTag<Sh>) with the brick shape of index `shape`.
+template <class S, class Fn>
+static void with_shape(int shape, Fn&& fn) {
+  if (shape == 1) {
+    fn(ShTag<Shape2D>{});
+  } else if (shape == 2) {
+    if constexpr (kAllShapes<S>) fn(ShTag<Shape3D_H>{});
+  } else if (shape == 3) {
+    if constexpr (kAllShapes<S>) fn(ShTag<Shape3D_W>{});
+  } else {
+    fn(ShTag<Shape3D>{});
+  }
+}
 
 static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   auto spread = [](uint64_t v) {
@@ -76,7 +109,8 @@ static uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
 // Host copy of one lattice's brick layout.
 struct HostLayout {
   int nx, ny, nz, lb[3], nb[3], words;
-  bool shape2d;
+  int shape;
+  bool shape2d;  // no halo along z (16x16x1 bricks of a one-layer lattice)
   int64_t n;
   std::vector<int32_t> brick_grid, base, brick_xyz, ref_of, site_of_ref, node_of;
   std::vector<uint64_t> mask;
@@ -84,15 +118,14 @@ struct HostLayout {
   int nbricks() const { return (int)brick_xyz.size() / 3; }
 };
 
-// Brick shape: 8x8x8 (Shape3D) for 3-D lattices, 16x16x1 (Shape2D) for
-// quasi-2-D ones (nz == 1). Axes shorter than the brick simply leave slots
+// Brick shape (kShapeLb): 16x16x1 for quasi-2-D lattices (nz == 1), one of
+// the 3-D bricks otherwise. Axes shorter than the brick simply leave slots
 // empty; tile positions wrap periodically, so any extent works.
-static int build_layout(const uint8_t* solid, int nx, int ny, int nz, HostLayout& L) {
+static int build_layout(const uint8_t* solid, int nx, int ny, int nz, int shape, HostLayout& L) {
   L.nx = nx; L.ny = ny; L.nz = nz;
-  L.shape2d = nz == 1;
-  L.lb[0] = L.shape2d ? 4 : 3;
-  L.lb[1] = L.shape2d ? 4 : 3;
-  L.lb[2] = L.shape2d ? 0 : 3;
+  L.shape = shape;
+  L.shape2d = shape == 1;
+  for (int a = 0; a < 3; ++a) L.lb[a] = kShapeLb[shape][a];
   const int B[3] = {1 << L.lb[0], 1 << L.lb[1], 1 << L.lb[2]};
   const int N[3] = {nx, ny, nz};
   for (int a = 0; a < 3; ++a) L.nb[a] = (N[a] + B[a] - 1) / B[a];
@@ -229,6 +262,8 @@ struct Engine {
   fe_params P{};
   int storage = FE_F64;
   int shape2d = 0;
+  int shape = 0;              // kShapeLb index
+  int graph_steps = 2;        // steps per graph launch of fe_run
   int wide = 0;               // 64-bit population offsets in the collide pass
   int device = 0;
   HostLayout L;
@@ -330,6 +365,33 @@ struct Engine {
     return FE_OK;
   }
 
+  // Brick shape and graph length: as requested in the parameters, else the
+  // autotuner's choice for this size class, else 8x8x8 (3-D) / 16x16x1
+  // (nz == 1) and two steps per graph.
+  int choose_layout(int nx, int ny, int nz, const uint8_t* solid) {
+    const int64_t nodes = (int64_t)nx * ny * nz;
+    int64_t fluid = 0;
+    for (int64_t q = 0; q < nodes; ++q) fluid += solid[q] == 0;
+    int brick = P.brick, gs = P.graph_steps;
+    int tb = 0, tg = 0;
+    if ((brick == FE_BRICK_AUTO || gs <= 0) &&
+        tune_lookup(nz == 1, storage, P.use_mrt != 0, P.use_halfway_bb != 0, (double)fluid / (double)nodes, fluid,
+                    &tb, &tg)) {
+      if (brick == FE_BRICK_AUTO) brick = tb;
+      if (gs <= 0) gs = tg;
+    }
+    if (brick == FE_BRICK_AUTO) brick = nz == 1 ? FE_BRICK_16x16x1 : FE_BRICK_8x8x8;
+    if (brick < FE_BRICK_8x8x8 || brick > FE_BRICK_16x8x8) return fe_fail(FE_ERR_ARG, "unknown brick shape");
+    if ((nz == 1) != (brick == FE_BRICK_16x16x1))
+      return fe_fail(FE_ERR_ARG, "16x16x1 bricks are for lattices with nz == 1, and only they");
+    if (brick >= FE_BRICK_8x8x4 && storage != FE_F64 && storage != FE_F32)
+      return fe_fail(FE_ERR_ARG, "8x8x4 and 16x8x8 bricks exist for FP64 and FP32 storage");
+    shape = brick - 1;
+    graph_steps = gs > 0 ? gs : 2;
+    if (graph_steps > 1024) return fe_fail(FE_ERR_ARG, "graph_steps above 1024");
+    return FE_OK;
+  }
+
   int create(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid, int dev) {
     P = *p;
     storage = P.storage;
@@ -342,8 +404,9 @@ struct Engine {
     if (dev >= 0) FE_CUDA(cudaSetDevice(dev));
     FE_CUDA(cudaGetDevice(&device));
     FE_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    int rc = build_layout(solid, nx, ny, nz, L);
-    if (rc) return rc;
+    int rc;
+    if ((rc = choose_layout(nx, ny, nz, solid))) return rc;
+    if ((rc = build_layout(solid, nx, ny, nz, shape, L))) return rc;
     if (L.n == 0) return fe_fail(FE_ERR_ARG, "geometry has no fluid site");
     if (L.n >= (int64_t)1 << 31) return fe_fail(FE_ERR_ARG, "more than 2^31 sites");
     shape2d = L.shape2d ? 1 : 0;
@@ -514,7 +577,8 @@ struct Engine {
         cudaGraph_t g;
         FE_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         const int64_t saved = launches;
-        for (int s = 0; s < len; ++s) launch_step(p ^ (s & 1), stream);
+        const int steps = len == 1 ? 1 : graph_steps;
+        for (int s = 0; s < steps; ++s) launch_step(p ^ (s & 1), stream);
         launches = saved;
         cudaError_t e1 = cudaStreamEndCapture(stream, &g);
         if (e1 != cudaSuccess) return fe_fail(FE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e1));
@@ -542,10 +606,11 @@ struct Engine {
     const int kps = kernels_per_step();
     int s = 0;
     while (s < nsteps) {
-      if (nsteps - s >= 2) {
+      if (graph_steps > 1 && nsteps - s >= graph_steps) {
         FE_CUDA(cudaGraphLaunch(graph2[parity], stream));
-        s += 2;  // two steps: parity unchanged
-        launches += 2 * kps;
+        s += graph_steps;
+        parity ^= graph_steps & 1;
+        launches += (int64_t)graph_steps * kps;
       } else {
         FE_CUDA(cudaGraphLaunch(graph1[parity], stream));
         parity ^= 1;
@@ -715,7 +780,7 @@ struct Engine {
 // ---------------------------------------------------------------------------
 struct Batch {
   struct Group {
-    int shape2d = 0, mrt = 0, hbb = 0, wide = 0;
+    int shape = 0, mrt = 0, hbb = 0, wide = 0;
     int2* d_work = nullptr;
     int nwork = 0;
   };
@@ -734,7 +799,7 @@ struct Batch {
   bool dirty = true;
   int inflight = 0;                 // steps launched by fe_batch_launch, not yet waited for
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
-  cudaGraphExec_t graph2[2] = {nullptr, nullptr};
+  cudaGraphExec_t graph2[2] = {nullptr, nullptr};  // graph_steps steps
   int64_t launches = 0;
 
   ~Batch() {
@@ -858,21 +923,21 @@ struct Batch {
     }
     std::vector<int2> gw;
     std::vector<size_t> offs;
-    for (int sh = 0; sh < 2; ++sh)
+    for (int sh = 0; sh < NSHAPE; ++sh)
       for (int mrt = 0; mrt < 2; ++mrt)
         for (int hbb = 0; hbb < 2; ++hbb) {
           const size_t off = gw.size();
           for (size_t q = 0; q < mem.size(); ++q)
-            if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
+            if (mem[q]->shape == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
                 (mem[q]->hd.prm.hbb != 0) == (hbb != 0))
               for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
           if (gw.size() == off) continue;
           Group g;
           for (size_t q = 0; q < mem.size(); ++q)
-            if (mem[q]->shape2d == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
+            if (mem[q]->shape == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
                 (mem[q]->hd.prm.hbb != 0) == (hbb != 0) && mem[q]->wide)
               g.wide = 1;
-          g.shape2d = sh;
+          g.shape = sh;
           g.mrt = mrt;
           g.hbb = hbb;
           g.nwork = (int)(gw.size() - off);
@@ -914,18 +979,12 @@ struct Batch {
       if (nb) k_bc_buffers<S><<<(nb + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
       if (nall) k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
     }
-    for (const Group& g : groups) {
-      if (g.shape2d) launch_group_p2<S, Shape2D>(g, st);
-      else launch_group_p2<S, Shape3D>(g, st);
-    }
-    for (const Group& g : groups) {
-      if (g.shape2d) launch_group_p3<S, Shape2D>(g, st);
-      else launch_group_p3<S, Shape3D>(g, st);
-    }
-    for (const Group& g : groups) {
-      if (g.shape2d) launch_group_p4<S, Shape2D>(g, par, st);
-      else launch_group_p4<S, Shape3D>(g, par, st);
-    }
+    for (const Group& g : groups)
+      with_shape<S>(g.shape, [&](auto t) { launch_group_p2<S, typename decltype(t)::type>(g, st); });
+    for (const Group& g : groups)
+      with_shape<S>(g.shape, [&](auto t) { launch_group_p3<S, typename decltype(t)::type>(g, st); });
+    for (const Group& g : groups)
+      with_shape<S>(g.shape, [&](auto t) { launch_group_p4<S, typename decltype(t)::type>(g, par, st); });
   }
   void launch_step(int par, cudaStream_t st) {
     switch (storage) {
@@ -1286,6 +1345,13 @@ int fe_engine_destroy(fe_engine* e) {
   e->e.tracer_sets.clear();
   cudaStreamSynchronize(e->e.stream);
   delete e;
+  return FE_OK;
+}
+
+int fe_engine_layout(const fe_engine* e, int* brick, int* graph_steps) {
+  FE_GUARD(e);
+  if (brick) *brick = e->e.shape + 1;
+  if (graph_steps) *graph_steps = e->e.graph_steps;
   return FE_OK;
 }
 

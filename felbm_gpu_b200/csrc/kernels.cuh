@@ -185,6 +185,11 @@ struct BrickShape {
 };
 using Shape3D = BrickShape<8, 8, 8>;
 using Shape2D = BrickShape<16, 16, 1>;
+// Alternative 3-D bricks the autotuner chooses from (FP64 and FP32 storage):
+// half height (256 slots, one collide-pass iteration for any fill) and
+// double width (1024 slots, a shorter per-site prologue for sparse media).
+using Shape3D_H = BrickShape<8, 8, 4>;
+using Shape3D_W = BrickShape<16, 8, 8>;
 
 template <class Sh, int H>
 struct Tile {

@@ -36,6 +36,8 @@ def default_params(**kw) -> capi.FeParams:
     for k, v in kw.items():
         if k == "storage" and isinstance(v, str):
             v = capi.STORAGE[v]
+        if k == "brick" and isinstance(v, str):
+            v = capi.BRICK[v]
         if k in ("mrt_rate_mode", "mrt_rate_value"):
             arr = getattr(p, k)
             for i, x in v.items() if isinstance(v, dict) else enumerate(v):
@@ -46,6 +48,33 @@ def default_params(**kw) -> capi.FeParams:
         setattr(p, k, v)
     check(lib.fe_params_derive(C.byref(p)))
     return p
+
+
+def autotune(params, solid: np.ndarray, steps: int = 20, device: int = 0) -> dict:
+    """Time the brick shapes and graph lengths this lattice can use and record
+    the fastest for its size class (fe_autotune); engines created afterwards
+    with brick = "auto" in that class take it. Returns the choice and the
+    per-candidate MLUPS."""
+    solid = np.ascontiguousarray(solid, np.uint8)
+    nz, ny, nx = solid.shape
+    r = capi.FeTuneReport()
+    check(lib.fe_autotune(C.byref(params), nx, ny, nz, solid.ctypes.data_as(C.POINTER(C.c_uint8)), device, steps,
+                          C.byref(r)))
+    names = {v: k for k, v in capi.BRICK.items()}
+    return {"brick": names[r.brick], "graph_steps": r.graph_steps,
+            "candidates": [(names[r.cand_brick[i]], r.cand_graph_steps[i], r.cand_mlups[i]) for i in range(r.ncand)]}
+
+
+def tune_save(path: str):
+    check(lib.fe_tune_save(path.encode()))
+
+
+def tune_load(path: str):
+    check(lib.fe_tune_load(path.encode()))
+
+
+def tune_clear():
+    check(lib.fe_tune_clear())
 
 
 @dataclass
@@ -203,6 +232,12 @@ class MultiPhaseGPU:
         f = capi.FeFields(*[_dptr(out[k]) for k in ("rho", "c", "ux", "uy", "uz", "p", "mu")])
         check(lib.fe_download_fields(self._h, C.byref(f)))
         return out
+
+    def layout(self):
+        """(brick name, steps per graph launch) this engine runs with."""
+        b, g = C.c_int32(), C.c_int32()
+        check(lib.fe_engine_layout(self._h, C.byref(b), C.byref(g)))
+        return {v: k for k, v in capi.BRICK.items()}[b.value], g.value
 
     def flow_stats(self) -> np.ndarray:
         out = np.empty(6, np.float64)

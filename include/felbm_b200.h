@@ -98,7 +98,21 @@ typedef struct fe_params {
   int storage;
   /* reference scale of the FE_F16S/FE_BF16S deviations (ignored otherwise) */
   double c_ref, p_ref;
+  /* layout of this library (no reference counterpart): the brick shape,
+   * FE_BRICK_AUTO = the autotuner's choice for the size class (fe_autotune)
+   * or the default, and the steps per CUDA-graph launch of fe_run (0 = the
+   * tuned or default 2) */
+  int brick;
+  int graph_steps;
 } fe_params;
+
+/* Brick shapes. 16x16x1 is the one for lattices with nz == 1; the 3-D
+ * alternatives 8x8x4 and 16x8x8 exist for FE_F64 and FE_F32 storage. */
+#define FE_BRICK_AUTO 0
+#define FE_BRICK_8x8x8 1
+#define FE_BRICK_16x16x1 2
+#define FE_BRICK_8x8x4 3
+#define FE_BRICK_16x8x8 4
 
 /* Open inlet/outlet (reference MultiPhaseGPU::set_open_bnd,
  * multiphase_gpu.cuh:369-400, plus the DevParams open-boundary block
@@ -480,6 +494,32 @@ int fe_h5_read_dataset(const char* path, const char* name, int* type, int64_t* d
 /* Time nsteps of fe_run with CUDA events on the engine's stream; ms_total is
  * the device time. */
 int fe_time_run(fe_engine* e, int nsteps, float* ms_total);
+
+/* ---- autotuner (no reference counterpart) -------------------------------
+ * Times the brick shapes this lattice can use (3-D: 8x8x8, and for FP64/FP32
+ * storage 8x8x4 and 16x8x8; nz == 1: 16x16x1), then 2, 8 and 32 steps per
+ * graph launch with the fastest brick, each on its own engine over the given
+ * geometry (steps timed after 3 warm-up steps, CUDA events), and records the
+ * fastest pair for the size class: dimensionality, storage, collision,
+ * near-wall rule, porosity in 0.05 bins, site count in powers of two.
+ * Engines created afterwards with brick = FE_BRICK_AUTO (graph_steps = 0) in
+ * that class take it. The table lives in the process; fe_tune_save/load keep
+ * it in a text file. */
+typedef struct fe_tune_report {
+  int brick;                  /* chosen FE_BRICK_* */
+  int graph_steps;            /* chosen steps per graph launch */
+  int ncand;                  /* candidates timed */
+  int cand_brick[8];
+  int cand_graph_steps[8];
+  double cand_mlups[8];
+} fe_tune_report;
+/* The brick (FE_BRICK_*) and graph length an engine was created with. */
+int fe_engine_layout(const fe_engine* e, int* brick, int* graph_steps);
+int fe_autotune(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid, int device, int steps,
+                fe_tune_report* out);
+int fe_tune_save(const char* path);
+int fe_tune_load(const char* path);
+int fe_tune_clear(void);
 int fe_time_kernels(fe_engine* e, int nsteps, float* ms_per_kernel, int nkernels);
 /* Number of kernels the engine launched since creation. */
 int fe_launch_count(const fe_engine* e, int64_t* count);

@@ -106,3 +106,24 @@ def test_equilibrium_moments():
     assert np.allclose(h.reshape(19, -1).sum(0), c, atol=1e-15)
     assert np.allclose(g.reshape(19, -1).sum(0), 0.7, atol=1e-15)
     del m
+
+
+def test_autotune_table_round_trip(tmp_path):
+    """The autotune table's text form: loaded entries are saved back as read;
+    a malformed file is refused."""
+    from felbm_gpu_b200.engine import tune_clear, tune_load, tune_save
+    p = tmp_path / "tune.txt"
+    rows = ["0 1 1 1 7 23 3 8", "1 1 1 1 12 16 2 32"]
+    p.write_text("# a table\n" + "\n".join(rows) + "\n")
+    tune_clear()
+    tune_load(str(p))
+    q = tmp_path / "out.txt"
+    tune_save(str(q))
+    got = [l for l in q.read_text().splitlines() if not l.startswith("#")]
+    assert sorted(got) == sorted(rows)
+    p.write_text("0 1 1 1 7 23 9 8\n")
+    import pytest
+    from felbm_gpu_b200._capi import FeError
+    with pytest.raises(FeError):
+        tune_load(str(p))
+    tune_clear()

@@ -2,6 +2,8 @@
 status, and creation reports the missing device instead of crashing."""
 import ctypes as C
 
+import pytest
+
 import torch
 
 from felbm_gpu_b200 import _capi
@@ -36,9 +38,25 @@ def test_server_arguments():
         assert lib.fe_server_create(C.byref(ok), C.byref(h)) == _capi.FE_ERR_NO_DEVICE
 
 
-def test_struct_sizes_match_header():
-    # sizes of the C structs (gcc, x86-64): a mismatch would corrupt requests
-    assert C.sizeof(_capi.FeRequest) == 456
-    assert C.sizeof(_capi.FeResult) == 328
-    assert C.sizeof(_capi.FeServerStats) == 112
-    assert C.sizeof(_capi.FeServerConfig) == 32
+def test_struct_sizes_match_header(tmp_path):
+    """The ctypes mirrors have the C structs' sizes (a mismatch would corrupt
+    requests): the header compiled by the host C compiler tells."""
+    import os
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    names = {"fe_request": _capi.FeRequest, "fe_result": _capi.FeResult, "fe_server_stats": _capi.FeServerStats,
+             "fe_server_config": _capi.FeServerConfig, "fe_params": _capi.FeParams,
+             "fe_tracer_config": _capi.FeTracerConfig, "fe_tune_report": _capi.FeTuneReport,
+             "fe_fields": _capi.FeFields, "fe_open_bnd": _capi.FeOpenBnd}
+    src = tmp_path / "sizes.c"
+    src.write_text("#include <stdio.h>\n#include \"felbm_b200.h\"\nint main(void){\n" +
+                   "".join('printf("%%zu\\n", sizeof(%s));\n' % n for n in names) + "return 0;}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    for (n, cls), size in zip(names.items(), got):
+        assert C.sizeof(cls) == size, n
