@@ -797,6 +797,7 @@ struct Batch {
   int ncwork = 0;
   int64_t since_build = 0;          // steps since the last rebuild
   bool dirty = true;
+  int64_t same_members = 0;  // launches since the last membership change
   int inflight = 0;                 // steps launched by fe_batch_launch, not yet waited for
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
   cudaGraphExec_t graph2[2] = {nullptr, nullptr};  // graph_steps steps
@@ -1030,20 +1031,30 @@ struct Batch {
       if (mem[q]->parity != (join_parity[q] ^ (int)(since_build & 1))) dirty = true;
     if (dirty) {
       if ((rc = rebuild())) return rc;
+      same_members = 0;
     } else {
       for (Engine* e : mem) {
         FE_CUDA(cudaStreamSynchronize(e->stream));
         if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;
       }
+      ++same_members;
     }
-    if (!graph1[0] && (rc = build_graphs())) return rc;
+    // graphs pay off once a membership is launched again (a request loop
+    // changes members often; capturing and instantiating four graphs costs
+    // more than the plain launches of one chunk)
+    if (!graph1[0] && same_members >= 1 && (rc = build_graphs())) return rc;
     return FE_OK;
   }
-  // graph launches of nsteps on the batch stream (after prepare)
+  // nsteps on the batch stream (after prepare): graph launches, or plain
+  // launches while the membership is new
   int run_async(int nsteps) {
     const int64_t kps = launches_per_step();
     int par = (int)(since_build & 1);
     int s = 0;
+    if (!graph1[0]) {
+      for (; s < nsteps; ++s, par ^= 1) launch_step(par, stream);
+      launches += (int64_t)nsteps * kps;
+    }
     while (s < nsteps) {
       if (nsteps - s >= 2) {
         FE_CUDA(cudaGraphLaunch(graph2[par], stream));
@@ -1741,6 +1752,7 @@ int fe_batch_time_run(fe_batch* b, int nsteps, float* ms) {
   int rc;
   // graphs and descriptors ready before the timed region
   if ((rc = B.prepare())) return rc;
+  if (!B.graph1[0] && (rc = B.build_graphs())) return rc;
   cudaEvent_t e0, e1;
   FE_CUDA(cudaEventCreate(&e0));
   FE_CUDA(cudaEventCreate(&e1));

@@ -1,17 +1,19 @@
 // Serving: a request loop over the public C-ABI (fe_engine_*, fe_batch_*).
 // No counterpart in the reference, which runs one solve per process
-// (felbm_gpu_main.cu). One host thread owns the device work:
-//  * admission: queued solves become resident (engine created, state
-//    uploaded) while a slot is free and their footprint fits the budget;
+// (felbm_gpu_main.cu). One host thread owns the batch:
+//  * admission: queued solves are admitted while a slot is free and their
+//    footprint fits the budget; creator threads then make them resident
+//    (engine created, state uploaded) and hands them to the loop;
 //  * scheduling: each chunk runs the resident solves with the least
 //    remaining work, up to fill_sites sites, as one batch (the GPU's
 //    throughput saturates at a few million sites, so adding more solves to a
 //    chunk only slows every member's step rate);
 //  * overlap: a prep thread builds initial states on the host ahead of
-//    admission; a chunk is launched asynchronously, and while it runs the
-//    loop reads back the solves that retired in the previous chunk and admits
-//    new ones (their work goes on their own engine streams); retired engines
-//    are freed after the chunk (freeing device memory waits for the GPU);
+//    admission, creator threads build engines and a finisher thread
+//    reads back retired solves, all on their engines' own streams while
+//    chunks run, so the loop thread only launches chunks and changes batch
+//    membership; retired engines are freed by the loop after a chunk
+//    (freeing device memory waits for the GPU);
 //  * retirement: after the step count, or the convergence test.
 // Submission and polling only touch the queues under a mutex.
 #include <cuda_runtime.h>
@@ -90,15 +92,21 @@ struct fe_server {
   fe_server_config cfg{};
   fe_batch* batch = nullptr;
   Clock::time_point t0;
-  std::thread th, prep;
+  std::thread th, finisher;
+  std::vector<std::thread> preps, creators;  // host work of several solves at once
   std::mutex mu;
-  std::condition_variable cv;       // a prepared solve is queued / stop
+  std::condition_variable cv;       // loop: a prepared solve is queued, a solve was created or read back / stop
   std::condition_variable cv_prep;  // a solve needs its initial state / stop
+  std::condition_variable cv_make;  // creator: an admitted solve waits for its engine / stop
+  std::condition_variable cv_read;  // finisher: a retired solve waits to be read back / stop
   std::condition_variable cv_idle;  // queue and resident set drained
   std::deque<Req> queue;
-  std::vector<Live> live;           // resident solves (loop thread only)
-  std::vector<Live> retiring;       // stepped out, results not read back yet
-  std::vector<Live> to_free;        // read back; engines freed after the chunk
+  std::vector<Live> live;           // resident solves in the loop (loop thread only)
+  std::deque<Live> to_create;       // admitted, engine not built yet (under mu)
+  std::vector<Live> created;        // engine built, not yet in the loop (under mu)
+  std::deque<Live> to_read;         // stepped out, results not read back yet (under mu)
+  std::vector<Live> to_free;        // read back; engines freed after the chunk (under mu)
+  int64_t holding = 0;              // admitted solves whose memory is not released (under mu)
   std::vector<fe_result> finished;
   bool stop = false;
   double budget = 0.0, committed = 0.0, reserve = 0.0;
@@ -131,8 +139,10 @@ struct fe_server {
   void release(Live& L) {
     if (L.e) fe_engine_destroy(L.e);  // leaves the batch first
     L.e = nullptr;
+    std::lock_guard<std::mutex> g(mu);
     committed -= L.bytes;
     L.bytes = 0.0;
+    --holding;
   }
 
   void fail(Live& L, int status) {
@@ -223,8 +233,8 @@ struct fe_server {
     }
   }
 
-  bool fits(int64_t sites) {
-    if (cfg.max_active > 0 && (int)(live.size() + retiring.size()) >= cfg.max_active) return false;
+  bool fits(int64_t sites) {  // under mu
+    if (cfg.max_active > 0 && holding >= cfg.max_active) return false;
     const double need = footprint(sites, cfg.storage);
     if (committed + need > budget) return false;
     size_t fr = 0, tot = 0;  // memory other users took since the server started
@@ -235,44 +245,77 @@ struct fe_server {
     return (double)fr - need >= reserve;
   }
 
-  // Admits queued solves (oldest first) while they fit.
-  void admit() {
-    for (;;) {
-      Req q;
-      {
-        std::lock_guard<std::mutex> g(mu);
-        if (stop || queue.empty() || !queue.front().ready) return;
-        // with nothing resident, the oldest solve is admitted even if its
-        // estimate exceeds the budget: engine creation then reports an
-        // out-of-memory failure for it instead of a queue that never moves
-        if (!fits(queue.front().sites) && !(live.empty() && retiring.empty())) return;
-        q = std::move(queue.front());
-        queue.pop_front();
-        ++admitted;
-        ++active;
-        peak_active = std::max(peak_active, active);
-      }
+  // Admits queued solves (oldest first) while they fit: their memory is
+  // charged and the creator thread builds their engines. Under mu.
+  void admit_locked() {
+    while (!stop && !queue.empty() && queue.front().ready) {
+      // with nothing held, the oldest solve is admitted even if its estimate
+      // exceeds the budget: engine creation then reports an out-of-memory
+      // failure for it instead of a queue that never moves
+      if (!fits(queue.front().sites) && holding > 0) return;
       Live L;
-      L.q = std::move(q);
+      L.q = std::move(queue.front());
+      queue.pop_front();
+      ++admitted;
+      ++active;
+      peak_active = std::max(peak_active, active);
       L.t_admit = now();
       L.bytes = footprint(L.q.sites, cfg.storage);
       committed += L.bytes;
-      if (make_resident(L)) live.push_back(std::move(L));
+      ++holding;
+      to_create.push_back(std::move(L));
+      cv_make.notify_all();
     }
   }
 
-  // Reads back retired solves; their engines are freed by free_retired()
-  // (freeing device memory waits for the GPU, so not while a chunk runs).
-  void drain_retiring() {
-    for (Live& L : retiring) {
-      read_back(L);
-      to_free.push_back(std::move(L));
+  void creator_loop() {
+    cudaSetDevice(cfg.device);
+    for (;;) {
+      Live L;
+      {
+        std::unique_lock<std::mutex> g(mu);
+        cv_make.wait(g, [&] { return stop || !to_create.empty(); });
+        if (stop) return;
+        L = std::move(to_create.front());
+        to_create.pop_front();
+      }
+      if (make_resident(L)) {
+        std::lock_guard<std::mutex> g(mu);
+        created.push_back(std::move(L));
+        cv.notify_all();
+      } else {
+        std::lock_guard<std::mutex> g(mu);
+        cv.notify_all();
+      }
     }
-    retiring.clear();
   }
+
+  void finisher_loop() {
+    cudaSetDevice(cfg.device);
+    for (;;) {
+      Live L;
+      {
+        std::unique_lock<std::mutex> g(mu);
+        cv_read.wait(g, [&] { return stop || !to_read.empty(); });
+        if (stop) return;
+        L = std::move(to_read.front());
+        to_read.pop_front();
+      }
+      read_back(L);
+      std::lock_guard<std::mutex> g(mu);
+      to_free.push_back(std::move(L));
+      cv.notify_all();
+    }
+  }
+
+  // Engines of read-back solves (loop thread, outside a running chunk).
   void free_retired() {
-    for (Live& L : to_free) release(L);
-    to_free.clear();
+    std::vector<Live> v;
+    {
+      std::lock_guard<std::mutex> g(mu);
+      v.swap(to_free);
+    }
+    for (Live& L : v) release(L);
   }
 
   // The chunk's running set: least remaining work first, up to fill_sites.
@@ -296,23 +339,24 @@ struct fe_server {
     {
       size_t fr = 0, tot = 0;
       if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) cudaGetLastError();
+      std::lock_guard<std::mutex> g(mu);
       reserve = cfg.hbm_reserve_frac * (double)tot;
       budget = (double)fr - reserve;
     }
     for (;;) {
+      free_retired();
       {
-        std::lock_guard<std::mutex> g(mu);
+        std::unique_lock<std::mutex> g(mu);
         if (stop) break;
-      }
-      if (live.empty()) {
-        drain_retiring();
-        free_retired();
-        admit();
+        admit_locked();
+        for (Live& L : created) live.push_back(std::move(L));
+        created.clear();
         if (live.empty()) {
-          std::unique_lock<std::mutex> g(mu);
-          if (stop) break;
-          if (queue.empty()) cv_idle.notify_all();
-          cv.wait(g, [&] { return stop || (!queue.empty() && queue.front().ready); });
+          if (queue.empty() && to_create.empty() && to_read.empty() && active == 0) cv_idle.notify_all();
+          cv.wait(g, [&] {
+            return stop || !created.empty() || !to_free.empty() ||
+                   (!queue.empty() && queue.front().ready && (holding == 0 || fits(queue.front().sites)));
+          });
           continue;
         }
       }
@@ -339,13 +383,12 @@ struct fe_server {
       chunk = std::max<int64_t>(chunk, 1);
       const double tb = now();
       int rc = fe_batch_launch(batch, (int)chunk);
-      // while the chunk runs: results of the last retirements, new solves
-      drain_retiring();
-      admit();
-      sel.resize(live.size(), 0);  // solves admitted meanwhile did not run
+      {  // while the chunk runs: admit what fits now
+        std::lock_guard<std::mutex> g(mu);
+        admit_locked();
+      }
       if (!rc) rc = fe_batch_wait(batch);
       const double te = now();
-      free_retired();
       if (rc) {  // the batch failed: report every solve of the chunk
         for (int q : run) live[q].status = rc;
       } else {
@@ -378,16 +421,19 @@ struct fe_server {
         if (ret) {
           fe_batch_remove(batch, L.e);
           L.in_batch = false;
-          retiring.push_back(std::move(L));
+          std::lock_guard<std::mutex> g(mu);
+          to_read.push_back(std::move(L));
+          cv_read.notify_all();
         } else {
           keep.push_back(std::move(L));
         }
       }
       live.swap(keep);
     }
-    drain_retiring();
-    free_retired();
-    for (Live& L : live) release(L);
+    for (Live& L : live) {
+      if (L.in_batch) fe_batch_remove(batch, L.e);
+      release(L);
+    }
     live.clear();
     std::lock_guard<std::mutex> g(mu);
     cv_idle.notify_all();
@@ -413,7 +459,9 @@ int fe_server_create(const fe_server_config* cfg, fe_server** out) {
   }
   s->t0 = Clock::now();
   s->th = std::thread([s] { s->loop(); });
-  s->prep = std::thread([s] { s->prep_loop(); });
+  for (int k = 0; k < 1; ++k) s->preps.emplace_back([s] { s->prep_loop(); });
+  for (int k = 0; k < 1; ++k) s->creators.emplace_back([s] { s->creator_loop(); });
+  s->finisher = std::thread([s] { s->finisher_loop(); });
   *out = s;
   return FE_OK;
 }
@@ -504,9 +552,17 @@ int fe_server_destroy(fe_server* s) {
     s->stop = true;
     s->cv.notify_all();
     s->cv_prep.notify_all();
+    s->cv_make.notify_all();
+    s->cv_read.notify_all();
   }
   if (s->th.joinable()) s->th.join();
-  if (s->prep.joinable()) s->prep.join();
+  for (std::thread& t : s->preps) t.join();
+  for (std::thread& t : s->creators) t.join();
+  if (s->finisher.joinable()) s->finisher.join();
+  // solves caught between the threads at shutdown
+  for (Live& L : s->created) s->release(L);
+  for (Live& L : s->to_read) s->release(L);
+  for (Live& L : s->to_free) s->release(L);
   for (fe_result& r : s->finished) fe_server_free_result(&r);
   fe_batch_destroy(s->batch);
   delete s;
