@@ -23,6 +23,7 @@
 #include "collide.cuh"
 #include "fe_internal.hpp"
 #include "kernels.cuh"
+#include "staging.hpp"
 #include "tracers.cuh"
 
 namespace fe {
@@ -670,10 +671,20 @@ struct Engine {
                                                                                   d_tmp + Vn, apply)));
     ++launches;
     FE_CUDA(cudaGetLastError());
-    FE_CUDA(cudaMemcpyAsync(h, d_tmp, Vn * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    FE_CUDA(cudaMemcpyAsync(g, d_tmp + Vn, Vn * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    FE_CUDA(copy_to_host(h, d_tmp, Vn * sizeof(double)));
+    FE_CUDA(copy_to_host(g, d_tmp + Vn, Vn * sizeof(double)));
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
+  }
+  // Large transfers through the pinned staging buffers (plain copies if
+  // those cannot be allocated).
+  cudaError_t copy_to_host(void* dst, const void* src, size_t bytes) {
+    Staging* s = bytes >= (size_t(4) << 20) ? Staging::get() : nullptr;
+    return s ? s->to_host(dst, src, bytes, stream) : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream);
+  }
+  cudaError_t copy_to_device(void* dst, const void* src, size_t bytes) {
+    Staging* s = bytes >= (size_t(4) << 20) ? Staging::get() : nullptr;
+    return s ? s->to_device(dst, src, bytes, stream) : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
   }
 
   // A queued mass correction written into the stored h now (instead of at
@@ -697,8 +708,8 @@ struct Engine {
     const int64_t Vn = (int64_t)Q * hd.n;
     int rc;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
-    FE_CUDA(cudaMemcpyAsync(d_tmp, h, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
-    FE_CUDA(cudaMemcpyAsync(d_tmp + Vn, g, Vn * sizeof(double), cudaMemcpyHostToDevice, stream));
+    FE_CUDA(copy_to_device(d_tmp, h, Vn * sizeof(double)));
+    FE_CUDA(copy_to_device(d_tmp + Vn, g, Vn * sizeof(double)));
     FE_DISPATCH(*this, (k_upload_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
                                                                                 d_tmp + Vn)));
     ++launches;
@@ -743,7 +754,7 @@ struct Engine {
     FE_CUDA(cudaGetLastError());
     double* dst[7] = {f->rho, f->c, f->ux, f->uy, f->uz, f->p, f->mu};
     for (int q = 0; q < 7; ++q)
-      if (dst[q]) FE_CUDA(cudaMemcpyAsync(dst[q], d_tmp + q * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      if (dst[q]) FE_CUDA(copy_to_host(dst[q], d_tmp + q * n, n * sizeof(double)));
     FE_CUDA(cudaStreamSynchronize(stream));
     double zero = 0.0;
     return write_ctl_field(offsetof(Ctl, lambda), &zero, 8);
