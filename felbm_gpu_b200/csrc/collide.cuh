@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   const DevPrm& Pm = D.prm;
   const R cs2 = R(CS2), alpha = R(ALPHA);
   const R rho1 = (R)Pm.rho1, drho = (R)Pm.drho;
-  const R tau0 = (R)Pm.tau0, tau1 = (R)Pm.tau1, ffac = (R)s.ff;
+  // per-lattice reciprocals once per brick: the site formulas multiply
+  const R itau0 = (R)(1.0 / Pm.tau0), itau1 = (R)(1.0 / Pm.tau1), ffac = (R)s.ff;
   const R gxa = (R)Pm.gx, gya = (R)Pm.gy, gza = (R)Pm.gz;
   const R fxa = (R)Pm.fx * ffac, fya = (R)Pm.fy * ffac, fza = (R)Pm.fz * ffac;
   const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
@@ -176,10 +177,11 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       }
     }
     const R rho = rho1 + drho * q.c;
+    const R irho = R(1) / rho;
     const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : q.c;
     // relaxation rate (reference k_moments :130-132)
     const R cpc = cm_ < R(0) ? R(0) : (cm_ > R(1) ? R(1) : cm_);
-    const R tau = R(1) / (cpc / tau0 + (R(1) - cpc) / tau1);
+    const R tau = R(1) / (cpc * itau0 + (R(1) - cpc) * itau1);
     const R s0 = R(1) / (tau + R(0.5));
     // corrected velocity (k_moments + k_vel_press_corr)
     R ux, uy, uz;
@@ -194,11 +196,11 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
         if (lat_cy(k)) jy += R(lat_cy(k)) * g[k];
         if (lat_cz(k)) jz += R(lat_cz(k)) * g[k];
       }
-      const R inv = R(1) / (cs2 * rho);
-      const R mor = q.mu / rho;
-      ux = jx * inv + R(0.5) * (gxa + fxa / rho + mor * ecx);
-      uy = jy * inv + R(0.5) * (gya + fya / rho + mor * ecy);
-      uz = jz * inv + R(0.5) * (gza + fza / rho + mor * ecz);
+      const R inv = irho * R(1.0 / CS2);
+      const R mor = q.mu * irho;
+      ux = jx * inv + R(0.5) * (gxa + fxa * irho + mor * ecx);
+      uy = jy * inv + R(0.5) * (gya + fya * irho + mor * ecy);
+      uz = jz * inv + R(0.5) * (gza + fza * irho + mor * ecz);
     }
     // open-boundary overwrite of g by the plain equilibrium (apply_open_bnd)
     if (flag & BC_G_OVER) {
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     }
     // site scalars (device_engine.cuh:563-583)
     q.rho_cs2 = rho * cs2;
-    q.c_over = q.c / q.rho_cs2;
+    q.c_over = q.c * irho * R(1.0 / CS2);
     q.drho_cs2 = drho * cs2;
     q.mob = (R)Pm.mobility;
     const R bfx = rho * gxa + fxa, bfy = rho * gya + fya, bfz = rho * gza + fza;
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     }
     if (MRT) {
       // rates (reference device_engine.cuh:623-625, with per-kind modes)
-      const R taus = R(1) / s0 - R(0.5);
+      const R taus = tau;  // 1 / s0 - 1/2
       const R s1 = R(2) * taus / (R(2) * (R)Pm.mrt_lambda + taus);
       R srate[7];
 #pragma unroll
