@@ -181,8 +181,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : q.c;
     // relaxation rate (reference k_moments :130-132)
     const R cpc = cm_ < R(0) ? R(0) : (cm_ > R(1) ? R(1) : cm_);
-    const R tau = R(1) / (cpc * itau0 + (R(1) - cpc) * itau1);
-    const R s0 = R(1) / (tau + R(0.5));
+    // 1/tau = cpc/tau0 + (1-cpc)/tau1; s0 = 1/(tau + 1/2) = itau / (1 + itau/2)
+    const R itau = cpc * itau0 + (R(1) - cpc) * itau1;
+    const R s0 = itau / (R(1) + R(0.5) * itau);
     // corrected velocity (k_moments + k_vel_press_corr)
     R ux, uy, uz;
     if (flag & BC_SITE) {
@@ -294,8 +295,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     }
     if (MRT) {
       // rates (reference device_engine.cuh:623-625, with per-kind modes)
-      const R taus = tau;  // 1 / s0 - 1/2
-      const R s1 = R(2) * taus / (R(2) * (R)Pm.mrt_lambda + taus);
+      // s1 = 2 tau / (2 Lambda + tau) with tau = 1 / s0 - 1/2 = 1 / itau
+      const R s1 = R(2) / (R(2) * (R)Pm.mrt_lambda * itau + R(1));
       R srate[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k)

@@ -748,11 +748,12 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     // the correction changes p only through drho (k_vel_press_corr :194-195);
     // u is needed here only for that, or for output
     if (Pm.drho != 0.0 || OUT) {
-      const R inv = R(1) / (cs2 * rho);
-      const R mor = mu / rho;
-      const R ux = (R)fjx[i] * inv + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff / rho + mor * gx);
-      const R uy = (R)fjy[i] * inv + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff / rho + mor * gy);
-      const R uz = (R)fjz[i] * inv + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
+      const R irho = R(1) / rho;
+      const R inv = irho * R(1.0 / CS2);
+      const R mor = mu * irho;
+      const R ux = (R)fjx[i] * inv + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff * irho + mor * gx);
+      const R uy = (R)fjy[i] * inv + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff * irho + mor * gy);
+      const R uz = (R)fjz[i] * inv + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff * irho + mor * gz);
       const R p = (R)fp[i] + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
       if (Pm.drho != 0.0) fp[i] = (F)p;
       if (OUT) {
