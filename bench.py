@@ -384,6 +384,19 @@ def run_reference_arm(args, ws, rank):
     return 0
 
 
+def reduce_ranks(dist, ms: float, n: int, device: str):
+    """Whole-job timing over the replicas: the slowest rank's time and the
+    sites of all ranks (identity without a process group)."""
+    if dist is None:
+        return ms, n
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    nt = torch.tensor([float(n)], dtype=torch.float64, device=device)
+    dist.all_reduce(nt)
+    return float(t.item()), int(nt.item())
+
+
 def main():
     args = parse()
     ws, rank, lrank = dist_env()
@@ -428,15 +441,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
     launches = eng.launch_count() - l0
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        nt = torch.tensor([float(n)], device="cuda")
-        dist.all_reduce(nt)
-        n_total = nt.item()
-    else:
-        n_total = n
+    ms, n_total = reduce_ranks(dist, ms, n, "cuda")
     value = n_total * args.steps / (ms / 1e3) / 1e6
     # per-kernel device times (plain launches, CUDA events on the engine stream)
     kms = eng.time_kernels(max(10, min(args.steps, 50))) / max(10, min(args.steps, 50))
