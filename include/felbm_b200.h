@@ -107,7 +107,8 @@ typedef struct fe_params {
 } fe_params;
 
 /* Brick shapes. 16x16x1 is the one for lattices with nz == 1; the 3-D
- * alternatives 8x8x4 and 16x8x8 exist for FE_F64 and FE_F32 storage. */
+ * alternatives 8x8x4 and 16x8x8 exist for FE_F64 and FE_F32 storage. Without
+ * a tuned choice, 3-D lattices get 16x8x8 (FP64, FP32) or 8x8x8. */
 #define FE_BRICK_AUTO 0
 #define FE_BRICK_8x8x8 1
 #define FE_BRICK_16x16x1 2
