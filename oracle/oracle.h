@@ -14,8 +14,8 @@
  * reference's own kernels (device_engine.cuh compiled unmodified for sm_100a
  * by oracle/ref/build_ref.sh) through golden vectors in tests/golden/.
  * Semantics that live only in felbm_local (site set, is_known, streaming rows,
- * MRT matrix values, initial conditions) are this project's definitions and
- * are unpinned; they are listed in DESIGN.md.
+ * MRT matrix values, initial conditions) are this project's definitions,
+ * written once in the kernels and once here, and are unpinned.
  */
 #ifndef FE_ORACLE_H
 #define FE_ORACLE_H

@@ -52,7 +52,7 @@ def make_case(name: str, **over) -> Case:
         h, g = _ic(solid, p, "droplet", 4.0, centre=(8, 8, 8), radius=4.0)
         return Case(name, solid, p, h, g)
     if name == "cyl2d_mrt":           # quasi-2-D cylinder pack, slab, body force
-        # rates: the BASELINE's explicit s_e = s_eps = 1.19, s_q = 1.2 (nu from tau),
+        # rates: the production configuration's explicit s_e = s_eps = 1.19, s_q = 1.2 (nu from tau),
         # or with ref_rates=True the reference's own assignment (device_engine.cuh:625),
         # which is what the reference's kernels can run
         ref_rates = bool(over.pop("ref_rates", False))
