@@ -1,4 +1,4 @@
-// Minimal HDF5 files without libhdf5 (absent from this build's toolchain):
+// Minimal HDF5 files without libhdf5 (no HDF5 library to link against):
 // the file-format specification's version-0 superblock, one root group held
 // as a symbol table (v1 B-tree + local heap + one symbol-table node), and
 // datasets with version-1 object headers, contiguous layout, no filters.

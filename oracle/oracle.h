@@ -5,7 +5,7 @@
  * include/felbm_gpu/device_engine.cuh + multiphase_gpu.cuh) in the reference's
  * own data layout (f[k*n+i]) and with the reference's own neighbour/case
  * tables. Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline
- * leg use it, as the checker; the product never links or calls it.
+ * leg use it, to compare against; the product never links or calls it.
  *
  * Parity pin: the reference's CPU engine (felbm_local EngineMultiPhase) is not
  * part of the reference snapshot, so this oracle restates the reference's GPU

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (liboracle.so) — TEST INFRASTRUCTURE ONLY.
 
-Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the
-checker; the product never imports it. The struct layouts are the C-ABI's
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg to
+compare against; the product never imports it. The struct layouts are the C-ABI's
 (include/felbm_b200.h), taken from felbm_gpu_b200._capi.
 """
 from __future__ import annotations
