@@ -294,6 +294,13 @@ struct Engine {
   double target_mass_host = 0.0;
   struct Batch* owner = nullptr;  // batch the engine is a member of
   std::vector<struct Tracers*> tracer_sets;  // tracers advected on this engine (detached at destroy)
+  // The tracer set whose velocity snapshot P2 writes on every step: its
+  // advance after step t is deferred to the next single step, whose P2 forms
+  // the velocity of that state anyway (tracers.cuh, Tracers::advance).
+  struct Tracers* fused = nullptr;
+  int64_t state_id = 0;       // bumps whenever the populations change
+  int base_need_j = 0;        // need_j without the snapshot
+  int tracer_hook(int nsteps, int64_t before, bool after);  // defined after Tracers
 
   ~Engine() { release(); }
   void release() {
@@ -567,6 +574,8 @@ struct Engine {
 
   int step(int nsteps) {
     int rc;
+    const int64_t before = state_id;
+    if ((rc = tracer_hook(nsteps, before, false))) return rc;
     if ((rc = set_ctl_mode(0, ff_manual))) return rc;
     for (int s = 0; s < nsteps; ++s) {
       launch_step(parity, stream);
@@ -574,7 +583,8 @@ struct Engine {
     }
     FE_CUDA(cudaGetLastError());
     t_host += nsteps;
-    return FE_OK;
+    state_id += nsteps;
+    return tracer_hook(nsteps, before, true);
   }
 
   int build_graphs() {
@@ -607,6 +617,8 @@ struct Engine {
 
   int run(int nsteps) {
     int rc;
+    const int64_t before = state_id;
+    if ((rc = tracer_hook(nsteps, before, false))) return rc;
     if ((rc = set_ctl_mode(1, ff_manual))) return rc;
     if (!graph1[0] && (rc = build_graphs())) return rc;
     const int kps = kernels_per_step();
@@ -625,8 +637,9 @@ struct Engine {
       }
     }
     t_host += nsteps;
+    state_id += nsteps;
     FE_CUDA(cudaGetLastError());
-    return FE_OK;
+    return tracer_hook(nsteps, before, true);
   }
 
   int ensure_tmp(int64_t len) {
@@ -697,6 +710,7 @@ struct Engine {
   int settle_correction() {
     Ctl c;
     int rc;
+    if ((rc = tracer_hook(-1, state_id, false))) return rc;
     if ((rc = read_ctl(&c))) return rc;
     if (!c.pending || !hd.prm.correct_mass) return FE_OK;
     if ((rc = mass_pass())) return rc;
@@ -712,6 +726,8 @@ struct Engine {
   int upload(const double* h, const double* g) {
     const int64_t Vn = (int64_t)Q * hd.n;
     int rc;
+    if ((rc = tracer_hook(-1, state_id, false))) return rc;  // deferred tracer advances see the old state
+    ++state_id;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
     FE_CUDA(copy_to_device(d_tmp, h, Vn * sizeof(double)));
     FE_CUDA(copy_to_device(d_tmp + Vn, g, Vn * sizeof(double)));
@@ -867,6 +883,8 @@ struct Batch {
     if (e->owner) return fe_fail(FE_ERR_STATE, "engine is a member of another batch");
     if (e->device != device) return fe_fail(FE_ERR_ARG, "engine and batch on different devices");
     if (storage >= 0 && e->storage != storage) return fe_fail(FE_ERR_ARG, "a batch holds one storage type");
+    int rc;
+    if ((rc = e->tracer_hook(-1, e->state_id, false))) return rc;  // batch steps do not run tracer advances
     storage = e->storage;
     cudaStreamSynchronize(e->stream);
     e->owner = this;
@@ -1088,7 +1106,10 @@ struct Batch {
   }
   int finish(int nsteps) {
     since_build += nsteps;
-    for (Engine* e : mem) e->t_host += nsteps;
+    for (Engine* e : mem) {
+      e->t_host += nsteps;
+      e->state_id += nsteps;
+    }
     settle();
     return FE_OK;
   }
@@ -1102,6 +1123,9 @@ struct Batch {
     if (inflight) return fe_fail(FE_ERR_STATE, "batch steps already in flight");
     if (mem.empty() || nsteps == 0) return FE_OK;
     int rc;
+    // deferred tracer advances of members use the state before these steps
+    for (Engine* e : mem)
+      if ((rc = e->tracer_hook(-1, e->state_id, false))) return rc;
     if ((rc = prepare())) return rc;
     if ((rc = run_async(nsteps))) return rc;
     inflight = nsteps;
@@ -1128,6 +1152,8 @@ struct Tracers {
   int64_t step = 0;             // tracer steps taken
   bool have_u = false;
   bool frozen = false;          // a caller-given velocity snapshot (fe_tracers_set_velocity)
+  bool pending = false;         // an advance waits for the engine's next single step
+  int64_t grid_for = -1;        // engine state whose velocity the snapshot holds
   cudaStream_t stream = nullptr;
   // stretching time series: rows 1..step, ring of ROWCAP rows on the device
   static constexpr int ROWCAP = 65536;
@@ -1139,6 +1165,7 @@ struct Tracers {
     if (E) {
       auto& v = E->tracer_sets;
       v.erase(std::remove(v.begin(), v.end(), this), v.end());
+      unfuse();
     }
     if (stream) cudaStreamSynchronize(stream);
     for (void* a : allocs) cudaFree(a);
@@ -1149,6 +1176,24 @@ struct Tracers {
     if (stream) cudaStreamSynchronize(stream);
     stream = nullptr;
     E = nullptr;
+  }
+  // Let the engine's field pass write this set's velocity snapshot on every
+  // step (velocity_skip 1, one set per engine, not while in a batch).
+  int fuse() {
+    if (E->fused || E->owner || velocity_skip != 1 || T.n == 0) return FE_OK;
+    E->fused = this;
+    for (int a = 0; a < 3; ++a) E->hd.snap_u[a] = const_cast<double*>(T.u[a]);
+    E->hd.snap_c = const_cast<double*>(T.cgrid);
+    E->hd.prm.need_j = 1;
+    return E->upload_desc();
+  }
+  void unfuse() {
+    if (!E || E->fused != this) return;
+    E->fused = nullptr;
+    for (int a = 0; a < 3; ++a) E->hd.snap_u[a] = nullptr;
+    E->hd.snap_c = nullptr;
+    E->hd.prm.need_j = (E->P.rho0 != E->P.rho1 || E->open_bnd) ? 1 : 0;
+    E->upload_desc();
   }
   template <class T_>
   int alloc(T_** p, size_t count) {
@@ -1224,25 +1269,38 @@ struct Tracers {
       FE_CUDA(cudaGetLastError());
       FE_CUDA(cudaStreamSynchronize(stream));
     }
-    return FE_OK;
+    return fuse();
   }
   int refresh() {
     double* u = const_cast<double*>(T.u[0]);
     const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
     int rc = E->velocity_grid(u, u + nodes, u + 2 * nodes, const_cast<double*>(T.cgrid));
-    if (!rc) have_u = true;
+    if (!rc) {
+      have_u = true;
+      grid_for = E->state_id;
+    }
     return rc;
+  }
+  // A deferred advance now, on a snapshot of the current state.
+  int flush() {
+    if (!pending) return FE_OK;
+    pending = false;
+    int rc = refresh();
+    return rc ? rc : launch_advance();
   }
   // A caller-given node-indexed velocity [3][nodes] (and order parameter
   // [nodes], optional) used from now on instead of the engine's; u == NULL
   // returns to the engine's velocity.
   int set_velocity(const double* u, const double* c) {
     const int64_t nodes = (int64_t)T.nx * T.ny * T.nz;
+    int rc;
+    if ((rc = flush())) return rc;
     if (!u) {
       frozen = false;
       have_u = false;
       return FE_OK;
     }
+    unfuse();  // the engine must not overwrite the caller's field
     FE_CUDA(cudaMemcpyAsync(const_cast<double*>(T.u[0]), u, 3 * nodes * sizeof(double), cudaMemcpyHostToDevice,
                             stream));
     if (c && T.cgrid)
@@ -1254,10 +1312,28 @@ struct Tracers {
     return FE_OK;
   }
   // One lattice step of the tracers on the engine's current velocity.
+  // One lattice step of the tracers on the engine's current velocity. A
+  // fused set defers it: the engine's next single step forms that velocity
+  // in its field pass, and the advance runs right after it on the engine's
+  // stream (same values as a refresh now; anything that needs the tracers
+  // earlier flushes the deferred advance through a refresh).
   int advance() {
     int rc;
+    if (!frozen && E->fused == this) {
+      if (grid_for != E->state_id) {
+        if ((rc = flush())) return rc;
+        if (grid_for != E->state_id) {
+          pending = true;
+          return FE_OK;
+        }
+      }
+      return launch_advance();
+    }
     if (!frozen && (!have_u || step % velocity_skip == 0))
       if ((rc = refresh())) return rc;
+    return launch_advance();
+  }
+  int launch_advance() {
     if (T.n > 0) {
       k_tracers<<<(unsigned)blocks, TRC, 0, stream>>>(T, step);
       if (T.stretch) k_stretch_row<<<1, 256, 0, stream>>>(T.part, blocks, T.substeps, T.n, step + 1, ring, ROWCAP);
@@ -1269,6 +1345,8 @@ struct Tracers {
   // Rows produced since the last call (oldest first), at most max_rows.
   int rows(double* out, int64_t max_rows, int64_t* count) {
     *count = 0;
+    int rc;
+    if ((rc = flush())) return rc;
     if (!T.stretch) return fe_fail(FE_ERR_STATE, "tracers created without stretching");
     const int64_t made = T.n > 0 ? step : 0;
     if (made - drained > ROWCAP) {
@@ -1290,6 +1368,8 @@ struct Tracers {
   }
   int stretch_state(double* rho_hat, double* log_rho, bool upload) {
     if (!T.stretch) return fe_fail(FE_ERR_STATE, "tracers created without stretching");
+    int rc;
+    if ((rc = flush())) return rc;
     const auto dir = upload ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
     if (rho_hat)
       FE_CUDA(upload ? cudaMemcpyAsync(T.rho_hat, rho_hat, 3 * T.n * sizeof(double), dir, stream)
@@ -1301,12 +1381,27 @@ struct Tracers {
     return FE_OK;
   }
   int download(double* pos, double* vel) {
+    int rc;
+    if ((rc = flush())) return rc;
     if (pos) FE_CUDA(cudaMemcpyAsync(pos, T.pos, 3 * T.n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     if (vel) FE_CUDA(cudaMemcpyAsync(vel, T.vel, 3 * T.n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
   }
 };
+
+// Deferred tracer advances around an engine step (Engine::fused).
+int Engine::tracer_hook(int nsteps, int64_t before, bool after) {
+  Tracers* t = fused;
+  if (!t || !t->pending) return FE_OK;
+  if (!after) return nsteps == 1 ? FE_OK : t->flush();
+  if (nsteps != 1) return FE_OK;
+  // this step's field pass wrote the velocity of the state it started from
+  t->pending = false;
+  t->grid_for = before;
+  t->have_u = true;
+  return t->launch_advance();
+}
 
 }  // namespace fe
 
@@ -1668,8 +1763,10 @@ int fe_time_kernels(fe_engine* e, int nsteps, float* ms, int nk) {
   cudaEvent_t ev[6];
   for (auto& x : ev) FE_CUDA(cudaEventCreate(&x));
   for (int q = 0; q < fe::K_N; ++q) ms[q] = 0.f;
-  int rc = E.set_ctl_mode(1, E.ff_manual);
+  int rc = E.tracer_hook(-1, E.state_id, false);
+  if (!rc) rc = E.set_ctl_mode(1, E.ff_manual);
   if (rc) return rc;
+  E.state_id += nsteps;
   for (int s = 0; s < nsteps; ++s) {
     E.launch_step(E.parity, E.stream, ev);
     E.parity ^= 1;

@@ -724,6 +724,13 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
         const F* ub = static_cast<const F*>(D.u_bc);
         out.put(q, (double)c0, (double)(rho1 + drho * c0), (double)ub[i], (double)ub[D.n + i],
                 (double)ub[2 * D.n + i], (double)fp[i], (double) static_cast<const F*>(D.mu)[i]);
+      } else if (D.snap_u[0]) {
+        const int64_t q = node_of<Sh>(D, wk.y, s.slot_of[r]);
+        const F* ub = static_cast<const F*>(D.u_bc);
+        D.snap_u[0][q] = (double)ub[i];
+        D.snap_u[1][q] = (double)ub[D.n + i];
+        D.snap_u[2][q] = (double)ub[2 * D.n + i];
+        if (D.snap_c) D.snap_c[q] = (double)c0;
       }
       continue;  // fields resolved by the open-boundary kernels
     }
@@ -746,8 +753,8 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     const R mu = four_beta * (c0 * (R(1) - c0)) * (R(0.5) - c0) + (-kappa * lap);
     fmu[i] = (F)mu;
     // the correction changes p only through drho (k_vel_press_corr :194-195);
-    // u is needed here only for that, or for output
-    if (Pm.drho != 0.0 || OUT) {
+    // u is needed here only for that, for output, or for the tracers' snapshot
+    if (Pm.drho != 0.0 || OUT || D.snap_u[0]) {
       const R irho = R(1) / rho;
       const R inv = irho * R(1.0 / CS2);
       const R mor = mu * irho;
@@ -759,6 +766,12 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
       if (OUT) {
         const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, s.slot_of[r]) : (int64_t)D.ref_of[i];
         out.put(q, (double)c0, (double)rho, (double)ux, (double)uy, (double)uz, (double)p, (double)mu);
+      } else if (D.snap_u[0]) {
+        const int64_t q = node_of<Sh>(D, wk.y, s.slot_of[r]);
+        D.snap_u[0][q] = (double)ux;
+        D.snap_u[1][q] = (double)uy;
+        D.snap_u[2][q] = (double)uz;
+        if (D.snap_c) D.snap_c[q] = (double)c0;
       }
     }
   }

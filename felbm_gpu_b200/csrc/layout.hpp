@@ -118,6 +118,10 @@ struct LatDesc {
   const int32_t* bcsrc;
   void* c_raw_bc;
   void* u_bc;                  // [3][n]
+  // node-indexed velocity (and order parameter) snapshot that P2 writes on
+  // every step while tracers are attached (null: none)
+  double* snap_u[3];
+  double* snap_c;
   const int32_t* bc_list;      // inlet sites, then outlet sites
   const int32_t* bc_xyz;       // node coordinates of inlet, outlet, buffer sites [3 each]
   const double* bc_coord;      // inlet coordinate along the split axis

@@ -199,3 +199,33 @@ def test_stretching_uniform_shear_exact_on_frozen_field(require_gpu):
     assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
     assert len(rows) == 8 and len(rest) == 12 and np.array_equal(np.r_[rows[:, 0], rest[:, 0]], np.arange(1, 21))
     assert np.all(rows[:, 4] == n) and np.all(np.isnan(rows[:, 5]))
+
+
+def test_fused_snapshot_equals_refresh(require_gpu):
+    """The first tracer set of an engine (velocity_skip 1) takes its velocity
+    from the engine's next step; a second set refreshes the snapshot itself.
+    Same tracers, same streams: identical trajectories and line elements, bit
+    for bit, through solo steps, several steps at once and downloads."""
+    case = flow_case("spheres_mrt_wet")
+    e = MultiPhaseGPU(with_storage(case.params, "f32"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        pos0, _ = seed(case.solid, 150, rng_seed=8)
+        kw = dict(substeps=2, order=2, rng_seed=5, stretching=True)
+        fused = Tracers(e, pos0, 1e-3, **kw)
+        plain = Tracers(e, pos0, 1e-3, **kw)
+        for s in range(12):
+            e.run(1 if s % 4 else 3)
+            fused.step()
+            plain.step()
+            if s == 6:
+                assert np.array_equal(fused.download()[0], plain.download()[0])
+        p1, v1 = fused.download()
+        p2, v2 = plain.download()
+        r1, r2 = fused.stretch_rows(), plain.stretch_rows()
+        fused.free()
+        plain.free()
+    finally:
+        e.free()
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+    assert np.array_equal(r1, r2, equal_nan=True) and len(r1) == 12
