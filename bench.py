@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the served sweep and request stream")
+    ap.add_argument("--no-tracers", action="store_true", help="skip the production loop with 12,000 tracers")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the layout autotuner (default bricks, two steps per graph launch)")
     ap.add_argument("--brick", default="auto", choices=["auto", "8x8x8", "8x8x4", "16x8x8"],
@@ -493,6 +494,33 @@ def main():
                "d2h_bytes_per_step": (state_bytes + ke * 48 + 16) / ke, "steps": ke,
                "what": "one job: fe_upload_state (host FP64 state) + K x (fe_set_forcing_factor, fe_step, "
                        "fe_apply_mass_correction, fe_flow_stats) + fe_download_state, host wall clock"}
+    production = None
+    if not args.no_tracers:
+        # the production loop: 12,000 GPU tracers (diffusivity ladder
+        # 1e-5..1e-1, uniform in the fluid) advanced after every step, flow
+        # statistics every 100 steps; device synchronised around the loop
+        from felbm_gpu_b200.tracers import Tracers, seed
+        pos, _ = seed(solid, 12000, rng_seed=17)
+        tr = Tracers(eng, pos, np.logspace(-5, -1, 12000), rng_seed=3)
+        for _ in range(3):
+            eng.run(1)
+            tr.step()
+        kp = max(100, (args.steps // 100) * 100)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in range(1, kp + 1):
+            eng.run(1)
+            tr.step()
+            if s % 100 == 0:
+                eng.flow_stats()
+        tr.download()
+        torch.cuda.synchronize()
+        dtp = time.perf_counter() - t0
+        tr.free()
+        production = {"workload": "the benched lattice + 12,000 tracers (Dm ladder 1e-5..1e-1), flow statistics "
+                                  "every 100 steps; driver loop fe_run(1) + fe_tracers_step per step",
+                      "steps": kp, "mlups": n * kp / dtp / 1e6, "ms_per_step": dtp * 1e3 / kp,
+                      "tracer_ms_per_step": dtp * 1e3 / kp - ms / args.steps}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample_mlups(args.storage)
@@ -512,7 +540,7 @@ def main():
                            "layout": {"brick": brick, "graph_steps": graph_steps,
                                       "autotune": tuned["candidates"] if tuned else None}},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "serving": serving}
+                "clocks": clk.summary(), "production": production, "serving": serving}
         print(json.dumps(line), flush=True)
     eng.free()
     if dist:
