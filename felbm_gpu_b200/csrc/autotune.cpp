@@ -89,7 +89,7 @@ int fe_autotune(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid
   std::vector<int> bricks;
   if (nz == 1) bricks = {FE_BRICK_16x16x1};
   else if (p->storage == FE_F64 || p->storage == FE_F32) bricks = {FE_BRICK_8x8x8, FE_BRICK_8x8x4, FE_BRICK_16x8x8};
-  else bricks = {FE_BRICK_8x8x8};
+  else bricks = {FE_BRICK_8x8x8, FE_BRICK_16x8x8};
   int best_brick = 0, best_graph = 2, rc;
   double best = -1.0;
   auto add = [&](int brick, int gs, double v) {

@@ -45,7 +45,7 @@ void fe_clear_error() { g_last_error.clear(); }
 
 // Run CALL with S (storage traits) and Sh (brick shape) bound to the engine's.
 // Inside CALL, write template argument commas as FE_COMMA. Shapes: 0 8x8x8,
-// 1 16x16x1, 2 8x8x4, 3 16x8x8; the last two exist for FP64 and FP32 only.
+// 1 16x16x1, 2 8x8x4 (FP64 and FP32 only), 3 16x8x8.
 #define FE_COMMA ,
 #define FE_SHAPES_ALL(E, ...)                                                  \
   switch ((E).shape) {                                                         \
@@ -55,8 +55,11 @@ void fe_clear_error() { g_last_error.clear(); }
     default: { using Sh = Shape3D; __VA_ARGS__; } break;                      \
   }
 #define FE_SHAPES_BASE(E, ...)                                                 \
-  if ((E).shape == 1) { using Sh = Shape2D; __VA_ARGS__; }                    \
-  else { using Sh = Shape3D; __VA_ARGS__; }
+  switch ((E).shape) {                                                         \
+    case 1: { using Sh = Shape2D; __VA_ARGS__; } break;                       \
+    case 3: { using Sh = Shape3D_W; __VA_ARGS__; } break;                     \
+    default: { using Sh = Shape3D; __VA_ARGS__; } break;                      \
+  }
 #define FE_DISPATCH(E, ...)                                                    \
   switch ((E).storage) {                                                       \
     case FE_F64: { using S = StF64; FE_SHAPES_ALL(E, __VA_ARGS__) } break;     \
@@ -74,7 +77,7 @@ struct ShTag {
 template <class S, class Fn>
 static void with_shape(int shape, Fn&& fn);
 
-// Storages with the alternative 3-D bricks compiled.
+// Storages with the 8x8x4 brick compiled.
 template <class S>
 constexpr bool kAllShapes = std::is_same<S, StF64>::value || std::is_same<S, StF32>::value;
 constexpr int NSHAPE = 4;
@@ -88,7 +91,7 @@ static void with_shape(int shape, Fn&& fn) {
   } else if (shape == 2) {
     if constexpr (kAllShapes<S>) fn(ShTag<Shape3D_H>{});
   } else if (shape == 3) {
-    if constexpr (kAllShapes<S>) fn(ShTag<Shape3D_W>{});
+    fn(ShTag<Shape3D_W>{});
   } else {
     fn(ShTag<Shape3D>{});
   }
@@ -374,9 +377,8 @@ struct Engine {
   }
 
   // Brick shape and graph length: as requested in the parameters, else the
-  // autotuner's choice for this size class, else the default brick (16x8x8
-  // for FP64/FP32, 8x8x8 for the 16-bit storages, 16x16x1 when nz == 1) and
-  // two steps per graph.
+  // autotuner's choice for this size class, else the default brick (16x8x8,
+  // 16x16x1 when nz == 1) and two steps per graph.
   int choose_layout(int nx, int ny, int nz, const uint8_t* solid) {
     const int64_t nodes = (int64_t)nx * ny * nz;
     int64_t fluid = 0;
@@ -390,15 +392,14 @@ struct Engine {
       if (gs <= 0) gs = tg;
     }
     // 16x8x8 measured fastest for FP64 and FP32 at every porosity from 0.2 to
-    // fully fluid (128^3 and 300^3); 8x8x8 is the brick of the 16-bit storages
-    if (brick == FE_BRICK_AUTO)
-      brick = nz == 1 ? FE_BRICK_16x16x1
-                      : ((storage == FE_F64 || storage == FE_F32) ? FE_BRICK_16x8x8 : FE_BRICK_8x8x8);
+    // fully fluid (128^3 and 300^3), and for the 16-bit storages by 16-19 %
+    // over 8x8x8 at 300^3
+    if (brick == FE_BRICK_AUTO) brick = nz == 1 ? FE_BRICK_16x16x1 : FE_BRICK_16x8x8;
     if (brick < FE_BRICK_8x8x8 || brick > FE_BRICK_16x8x8) return fe_fail(FE_ERR_ARG, "unknown brick shape");
     if ((nz == 1) != (brick == FE_BRICK_16x16x1))
       return fe_fail(FE_ERR_ARG, "16x16x1 bricks are for lattices with nz == 1, and only they");
-    if (brick >= FE_BRICK_8x8x4 && storage != FE_F64 && storage != FE_F32)
-      return fe_fail(FE_ERR_ARG, "8x8x4 and 16x8x8 bricks exist for FP64 and FP32 storage");
+    if (brick == FE_BRICK_8x8x4 && storage != FE_F64 && storage != FE_F32)
+      return fe_fail(FE_ERR_ARG, "8x8x4 bricks exist for FP64 and FP32 storage");
     shape = brick - 1;
     graph_steps = gs > 0 ? gs : 2;
     if (graph_steps > 1024) return fe_fail(FE_ERR_ARG, "graph_steps above 1024");

@@ -106,9 +106,9 @@ typedef struct fe_params {
   int graph_steps;
 } fe_params;
 
-/* Brick shapes. 16x16x1 is the one for lattices with nz == 1; the 3-D
- * alternatives 8x8x4 and 16x8x8 exist for FE_F64 and FE_F32 storage. Without
- * a tuned choice, 3-D lattices get 16x8x8 (FP64, FP32) or 8x8x8. */
+/* Brick shapes. 16x16x1 is the one for lattices with nz == 1; 8x8x4 exists
+ * for FE_F64 and FE_F32 storage. Without a tuned choice, 3-D lattices get
+ * 16x8x8. */
 #define FE_BRICK_AUTO 0
 #define FE_BRICK_8x8x8 1
 #define FE_BRICK_16x16x1 2
@@ -497,8 +497,8 @@ int fe_h5_read_dataset(const char* path, const char* name, int* type, int64_t* d
 int fe_time_run(fe_engine* e, int nsteps, float* ms_total);
 
 /* ---- autotuner (no reference counterpart) -------------------------------
- * Times the brick shapes this lattice can use (3-D: 8x8x8, and for FP64/FP32
- * storage 8x8x4 and 16x8x8; nz == 1: 16x16x1), then 2, 8 and 32 steps per
+ * Times the brick shapes this lattice can use (3-D: 8x8x8, 16x8x8, and for
+ * FP64/FP32 storage 8x8x4; nz == 1: 16x16x1), then 2, 8 and 32 steps per
  * graph launch with the fastest brick, each on its own engine over the given
  * geometry (steps timed after 3 warm-up steps, CUDA events), and records the
  * fastest pair for the size class: dimensionality, storage, collision,

@@ -123,3 +123,14 @@ def test_bricks_refused_where_not_built(require_gpu):
     c2 = make_case("cyl2d_mrt")
     with pytest.raises(_capi.FeError, match="16x16x1"):
         MultiPhaseGPU(_params(c2, "f32", "8x8x8"), c2.solid)
+
+
+@pytest.mark.parametrize("storage", ["f16g", "f16s", "bf16g"])
+def test_16bit_storages_on_wide_bricks(require_gpu, storage):
+    """16x8x8 bricks for the 16-bit storages: the same per-site arithmetic as
+    on 8x8x8 (only the order of the mass and statistics sums differs)."""
+    case = make_case("grf_mrt_mass")
+    h, g, _, lay = _run(case, storage, 20, "16x8x8")
+    h8, g8, _, _ = _run(case, storage, 20, "8x8x8")
+    assert lay == ("16x8x8", 2)
+    assert maxdiff(h, h8) <= 2e-3 and maxdiff(g, g8) <= 2e-3, (maxdiff(h, h8), maxdiff(g, g8))
