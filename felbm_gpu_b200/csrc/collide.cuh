@@ -4,15 +4,22 @@
 // :89-113, evaluated from shared-memory tiles, and the open-boundary overwrite
 // of g, k_open_bnd / k_open_bnd_buf, :761-798,826-846, folded in).
 //
-// Arithmetic layout (same algebra as the reference, reordered):
-//  * directions are processed in opposite pairs (k, k+1), e_{k+1} = -e_k: the
-//    neighbour values are loaded once per pair, the central-difference value is
-//    exactly antisymmetric (cd_{k+1} = -cd_k), and G_k, G_{k+1} share all
-//    terms but +-alpha w u.e_k;
+// Arithmetic layout (same algebra as the reference, regrouped):
+//  * the work comes in twins, done two lanes at a time (V2: one f32x2
+//    instruction for both lanes in FP32): the pre-pass evaluates the stencils
+//    of c and p together, the main pass the two directions of an opposite
+//    pair (k, k+1), e_{k+1} = -e_k;
+//  * within a pair every quantity is even or odd in e: odd ones (u.e, F.e,
+//    the central difference, exactly antisymmetric) enter as (v, -v), so the
+//    pair needs each of them once;
+//  * the central differences cancel from eq_h + force_h: with
+//    dc = (cd + bd) / 2 and ffk = mu dc + F.e, the bracket of h_k reduces to
+//    c + S_h + mob avg + (1 + c_o mu) bd_c / 2 - c_o bd_p / 2 + c_o F.e / 2
+//    (c_o = c / (rho cs^2)); eq_g splits the same way (see the main pass);
 //  * a pre-pass over the pairs evaluates the near-wall cases once, sums the
-//    four gradients (central / biased, of c and p) and keeps the six
-//    per-pair derivative values in a per-thread shared-memory stash; then all
-//    site scalars are known and the main pass stores h_k at once;
+//    four gradients (central / biased, of c and p) and keeps the five
+//    per-pair values the main pass needs (cd_c, bd_c and bd_p of both
+//    directions) in a per-thread shared-memory stash;
 //  * the MRT transform uses the row parity of the moment basis: even rows see
 //    x_k + x_{k+1}, odd rows x_k - x_{k+1}, and the back transform gives the
 //    pair as E +- O; only g + force_g (19 values) and the 15 relaxed moments
@@ -31,54 +38,37 @@ struct CollideMinBlocks {
   static constexpr int value = 65536 / ((sizeof(typename S::real) == 8 ? 256 : 128) * P4T);
 };
 
-constexpr int NPAIR = (Q - 1) / 2;   // 9 opposite pairs
-constexpr int NSTASH = 6 * NPAIR;    // stashed values per thread
+constexpr int NPAIR = (Q - 1) / 2;  // 9 opposite pairs
 
-// Dynamic shared memory of the collide pass: site indices, c / p / lap(mu)
-// tiles (halo 2) and the per-thread derivative stash.
+// Dynamic shared memory of the collide pass: site indices, the interleaved
+// (c, p) tile and the lap(mu) tile (halo 2), and the per-thread stash (two
+// pairs and one scalar per opposite pair).
 template <class Sh, class R>
 struct CollideSmem {
   using T = Tile<Sh, 2>;
   static constexpr int NT16 = (T::N * 4 + 15) & ~15;
   static constexpr int NTR = (T::N * (int)sizeof(R) + 15) & ~15;
-  static constexpr int STASH = NSTASH * P4T * (int)sizeof(R);
-  static constexpr int BYTES = NT16 + 3 * NTR + STASH;
+  static constexpr int NTV = (T::N * (int)sizeof(V2<R>) + 15) & ~15;
+  static constexpr int STV = 2 * NPAIR * P4T * (int)sizeof(V2<R>);
+  static constexpr int STS = NPAIR * P4T * (int)sizeof(R);
+  static constexpr int BYTES = NT16 + NTV + NTR + STV + STS;
 };
 
 // Per-site scalars shared by every direction of the collision.
 template <class R>
 struct SiteScal {
-  R c, p, mu, rho_cs2, c_over, drho_cs2, mob;
-  R gu2;                  // gamma |u|^2
-  R u_force_g, u_drho;    // u.e_fg, drho cs2 u.grad_cd c
-  R S_h, u_fg_f, u_drm;   // gradient-dependent terms of h and force_g
+  R mu, gu2, mob;
+  R C0;            // c + S_h
+  R hk1, hco;      // (1 + c_o mu) / 2, c_o / 2
+  R A1, A2;        // eq_g: w A1 + A2 w u_term (even part)
+  R hdr, u_drm, u_fg_f, drho_cs2;
 };
-
-// One direction: h_k, and x_k = eq_g,k - g_k, Z_k = g_k + force_g,k. The MRT
-// equilibrium of g carries +(mu dc_k + f_proj) G / 2 where the BGK one carries
-// -(...) (device_engine.cuh:517 vs :598).
-template <class R, int MRT>
-__device__ __forceinline__ void dir_terms(const SiteScal<R>& q, R w, R uk, R fproj, R cdc, R cdp, R bdc, R bdp,
-                                          R avg, R gk, R& h, R& x, R& Z) {
-  const R u_term = uk * (R(ALPHA) + R(BETA) * uk) - q.gu2;
-  const R G = w * (R(1) + u_term);
-  const R wut = G - w;
-  const R dc = R(0.5) * (cdc + bdc), dp = R(0.5) * (cdp + bdp);
-  const R ffk = q.mu * dc + fproj;
-  // eq_h + force_h (device_engine.cuh:596,608)
-  h = G * (q.c + R(0.5) * (-cdc + q.c_over * (cdp - q.mu * cdc - fproj)) + (dc - q.c_over * (dp - ffk)) +
-           q.mob * avg + q.S_h);
-  // eq_g (:597-598) and g + force_g (:609)
-  const R mcf = MRT ? q.mu * cdc + fproj : -(q.mu * cdc + fproj);
-  const R eg = w * q.p + q.rho_cs2 * wut + R(0.5) * ((q.u_drho - q.drho_cs2 * cdc) * wut + (q.u_force_g + mcf) * G);
-  x = eg - gk;
-  Z = gk + (q.drho_cs2 * dc - q.u_drm) * wut + (ffk - q.u_fg_f) * G;
-}
 
 template <class S, class Sh, int MRT, bool HBB, bool WIDE>
 __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
   using R = typename S::real;
+  using V = V2<R>;
   using PH = typename S::hpop;
   using PG = typename S::gpop;
   using F = typename S::fld;
@@ -90,10 +80,10 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   __shared__ Head<Sh> s;
   extern __shared__ __align__(16) unsigned char dsm[];
   int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  R* s_c = reinterpret_cast<R*>(dsm + SM::NT16);
-  R* s_p = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTR);
-  R* s_l = reinterpret_cast<R*>(dsm + SM::NT16 + 2 * SM::NTR);
-  R* s_st = reinterpret_cast<R*>(dsm + SM::NT16 + 3 * SM::NTR) + threadIdx.x;  // [v * P4T]
+  V* s_cp = reinterpret_cast<V*>(dsm + SM::NT16);
+  R* s_l = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTV);
+  V* s_sv = reinterpret_cast<V*>(dsm + SM::NT16 + SM::NTV + SM::NTR) + threadIdx.x;            // [(2 pr + j) P4T]
+  R* s_sc = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTV + SM::NTR + SM::STV) + threadIdx.x;  // [pr P4T]
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
@@ -101,8 +91,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   {
     const F* const src[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
                              static_cast<const F*>(D.lapmu)};
-    R* const dst[3] = {s_c, s_p, s_l};
-    stage<Sh, 2, 3, P4T>(src, dst, true, s.lambda, s_idx);
+    R* const dst[3] = {reinterpret_cast<R*>(s_cp), reinterpret_cast<R*>(s_cp) + 1, s_l};
+    stage<Sh, 2, 3, P4T, true>(src, dst, true, s.lambda, s_idx);
   }
   __syncthreads();
 
@@ -126,17 +116,19 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   for (int r = threadIdx.x; r < cnt; r += P4T) {
     const int64_t i = first + r;
     const int pos = T::pos(s.slot_of[r]);
-    SiteScal<R> q;
-    q.c = s_c[pos];
-    q.p = s_p[pos];
+    const V cp0 = s_cp[pos];
+    const R c = cp0.x(), p = cp0.y();
     const R lmu = s_l[pos];
+    SiteScal<R> q;
     q.mu = (R)fmu[i];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
-    // post-stream g of the site (what P1 read)
+    // post-stream g of the site (what P1 read), the pairs (k, k+1) together
     const IX a0 = (IX)pbase(i);
-    R g[Q];
+    R g0 = ld_pop<GV<S>>(gin, a0, 0, shg);
+    V gp[NPAIR];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) g[k] = ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg);
+    for (int k = 1; k < Q; k += 2)
+      gp[k >> 1] = V(ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg), ld_pop<GV<S>>(gin, a0 + (k + 1) * AOSOA, k + 1, shg));
     // push target of direction k: slot k of x + e_k, or slot opp(k) of x
     // (halfway bounce-back) when x + e_k is solid
     auto dst = [&](int k) -> IX {
@@ -145,40 +137,43 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
                      : a0 + (IX)(lat_opp(k) * AOSOA);
     };
     // ---- pre-pass: near-wall cases once, the four gradients, stash -----------
-    R ecx = 0, ecy = 0, ecz = 0, epx = 0, epy = 0, epz = 0;
-    R bcx = 0, bcy = 0, bcz = 0, bpx = 0, bpy = 0, bpz = 0;
+    // lanes (c, p): ec central sums, eb biased sums, per axis
+    V ec[3] = {V(R(0)), V(R(0)), V(R(0))}, eb[3] = {V(R(0)), V(R(0)), V(R(0))};
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
-      const int o = T::off(k), v = 6 * (k >> 1);
-      const R cm = s_c[pos - o], cp = s_c[pos + o], cm2 = s_c[pos - 2 * o], cp2 = s_c[pos + 2 * o];
-      const R pm = s_p[pos - o], pp = s_p[pos + o], pm2 = s_p[pos - 2 * o], pp2 = s_p[pos + 2 * o];
-      R cdc, cdp, bca, bcb, bpa, bpb;
-      pair_derivs<HBB>(q.c, cm, cp, cm2, cp2, q.p, pm, pp, pm2, pp2, cdc, cdp, bca, bcb, bpa, bpb);
-      s_st[(v + 0) * P4T] = cdc;
-      s_st[(v + 1) * P4T] = cdp;
-      s_st[(v + 2) * P4T] = bca;
-      s_st[(v + 3) * P4T] = bcb;
-      s_st[(v + 4) * P4T] = bpa;
-      s_st[(v + 5) * P4T] = bpb;
+      const int o = T::off(k), pr = k >> 1;
+      const V fm = s_cp[pos - o], fp = s_cp[pos + o], fm2 = s_cp[pos - 2 * o], fp2 = s_cp[pos + 2 * o];
+      V cd, ba, bb;
+      pair_derivs2<HBB>(cp0, fm, fp, fm2, fp2, cd, ba, bb);
+      s_sc[pr * P4T] = cd.x();
+      s_sv[(2 * pr) * P4T] = V(ba.x(), bb.x());
+      s_sv[(2 * pr + 1) * P4T] = V(ba.y(), bb.y());
       // pairs: central terms count twice, biased ones as a difference
       const R aw = alpha * weight<R>(k);
-      const R dbc = bca - bcb, dbp = bpa - bpb;
+      const V db = ba - bb;
       if (lat_cx(k)) {
         const R e = aw * R(lat_cx(k));
-        ecx += R(2) * e * cdc; epx += R(2) * e * cdp; bcx += e * dbc; bpx += e * dbp;
+        ec[0] = fma2(V(R(2) * e), cd, ec[0]);
+        eb[0] = fma2(V(e), db, eb[0]);
       }
       if (lat_cy(k)) {
         const R e = aw * R(lat_cy(k));
-        ecy += R(2) * e * cdc; epy += R(2) * e * cdp; bcy += e * dbc; bpy += e * dbp;
+        ec[1] = fma2(V(R(2) * e), cd, ec[1]);
+        eb[1] = fma2(V(e), db, eb[1]);
       }
       if (lat_cz(k)) {
         const R e = aw * R(lat_cz(k));
-        ecz += R(2) * e * cdc; epz += R(2) * e * cdp; bcz += e * dbc; bpz += e * dbp;
+        ec[2] = fma2(V(R(2) * e), cd, ec[2]);
+        eb[2] = fma2(V(e), db, eb[2]);
       }
     }
-    const R rho = rho1 + drho * q.c;
+    const R ecx = ec[0].x(), ecy = ec[1].x(), ecz = ec[2].x();
+    const R epx = ec[0].y(), epy = ec[1].y(), epz = ec[2].y();
+    const R bcx = eb[0].x(), bcy = eb[1].x(), bcz = eb[2].x();
+    const R bpx = eb[0].y(), bpy = eb[1].y(), bpz = eb[2].y();
+    const R rho = rho1 + drho * c;
     const R irho = R(1) / rho;
-    const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : q.c;
+    const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : c;
     // relaxation rate (reference k_moments :130-132)
     const R cpc = cm_ < R(0) ? R(0) : (cm_ > R(1) ? R(1) : cm_);
     // 1/tau = cpc/tau0 + (1-cpc)/tau1; s0 = 1/(tau + 1/2) = itau / (1 + itau/2)
@@ -190,12 +185,14 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const F* ubc = static_cast<const F*>(D.u_bc);
       ux = (R)ubc[i]; uy = (R)ubc[D.n + i]; uz = (R)ubc[2 * D.n + i];
     } else {
+      // g_k - g_{k+1} per pair carries the pair's momentum
       R jx = 0, jy = 0, jz = 0;
 #pragma unroll
-      for (int k = 0; k < Q; ++k) {
-        if (lat_cx(k)) jx += R(lat_cx(k)) * g[k];
-        if (lat_cy(k)) jy += R(lat_cy(k)) * g[k];
-        if (lat_cz(k)) jz += R(lat_cz(k)) * g[k];
+      for (int k = 1; k < Q; k += 2) {
+        const R dg = gp[k >> 1].x() - gp[k >> 1].y();
+        if (lat_cx(k)) jx += R(lat_cx(k)) * dg;
+        if (lat_cy(k)) jy += R(lat_cy(k)) * dg;
+        if (lat_cz(k)) jz += R(lat_cz(k)) * dg;
       }
       const R inv = irho * R(1.0 / CS2);
       const R mor = q.mu * irho;
@@ -211,73 +208,106 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const R bp = (R) static_cast<const F*>(D.p)[sb];
       const R brho = rho1 + drho * (R) static_cast<const F*>(D.c)[sb];
       const R bu_sq = bux * bux + buy * buy + buz * buz;
+      g0 = weight<R>(0) * (bp - brho * cs2 * R(GAMMA) * bu_sq);
 #pragma unroll
-      for (int k = 0; k < Q; ++k) {
+      for (int k = 1; k < Q; k += 2) {
         const R uk = bux * R(lat_cx(k)) + buy * R(lat_cy(k)) + buz * R(lat_cz(k));
-        const R u_term = uk * (alpha + R(BETA) * uk) - R(GAMMA) * bu_sq;
-        g[k] = weight<R>(k) * (bp + brho * cs2 * u_term);
+        const R ua = uk * (alpha + R(BETA) * uk) - R(GAMMA) * bu_sq;
+        const R ub = -uk * (alpha - R(BETA) * uk) - R(GAMMA) * bu_sq;
+        gp[k >> 1] = V(weight<R>(k) * (bp + brho * cs2 * ua), weight<R>(k) * (bp + brho * cs2 * ub));
       }
     }
     // site scalars (device_engine.cuh:563-583)
-    q.rho_cs2 = rho * cs2;
-    q.c_over = q.c * irho * R(1.0 / CS2);
+    const R rho_cs2 = rho * cs2;
+    const R c_over = c * irho * R(1.0 / CS2);
     q.drho_cs2 = drho * cs2;
+    q.hdr = R(0.5) * q.drho_cs2;
     q.mob = (R)Pm.mobility;
     const R bfx = rho * gxa + fxa, bfy = rho * gya + fya, bfz = rho * gza + fza;
     const R u2 = ux * ux + uy * uy + uz * uz;
     q.gu2 = R(GAMMA) * u2;
     const R efgx = q.mu * ecx + bfx, efgy = q.mu * ecy + bfy, efgz = q.mu * ecz + bfz;
-    const R efhx = ecx - q.c_over * (epx - efgx), efhy = ecy - q.c_over * (epy - efgy),
-            efhz = ecz - q.c_over * (epz - efgz);
+    const R efhx = ecx - c_over * (epx - efgx), efhy = ecy - c_over * (epy - efgy), efhz = ecz - c_over * (epz - efgz);
     const R fdcx = R(0.5) * (ecx + bcx), fdcy = R(0.5) * (ecy + bcy), fdcz = R(0.5) * (ecz + bcz);
     const R fdpx = R(0.5) * (epx + bpx), fdpy = R(0.5) * (epy + bpy), fdpz = R(0.5) * (epz + bpz);
     const R ffgx = q.mu * fdcx + bfx, ffgy = q.mu * fdcy + bfy, ffgz = q.mu * fdcz + bfz;
-    const R ffhx = fdcx - q.c_over * (fdpx - ffgx), ffhy = fdcy - q.c_over * (fdpy - ffgy),
-            ffhz = fdcz - q.c_over * (fdpz - ffgz);
-    q.u_force_g = ux * efgx + uy * efgy + uz * efgz;
-    q.u_drho = q.drho_cs2 * (ux * ecx + uy * ecy + uz * ecz);
-    q.S_h = R(0.5) * (ux * efhx + uy * efhy + uz * efhz) - (ux * ffhx + uy * ffhy + uz * ffhz);
+    const R ffhx = fdcx - c_over * (fdpx - ffgx), ffhy = fdcy - c_over * (fdpy - ffgy),
+            ffhz = fdcz - c_over * (fdpz - ffgz);
+    const R u_force_g = ux * efgx + uy * efgy + uz * efgz;
+    const R u_drho = q.drho_cs2 * (ux * ecx + uy * ecy + uz * ecz);
+    const R S_h = R(0.5) * (ux * efhx + uy * efhy + uz * efhz) - (ux * ffhx + uy * ffhy + uz * ffhz);
     q.u_fg_f = ux * ffgx + uy * ffgy + uz * ffgz;
     q.u_drm = q.drho_cs2 * (ux * fdcx + uy * fdcy + uz * fdcz);
-    st[0] += (double)ux; st[1] += (double)uy; st[2] += (double)uz; st[3] += (double)u2; st[4] += (double)q.c;
+    q.C0 = c + S_h;
+    q.hk1 = R(0.5) * (R(1) + c_over * q.mu);
+    q.hco = R(0.5) * c_over;
+    q.A1 = p + R(0.5) * u_force_g;
+    q.A2 = rho_cs2 + R(0.5) * (u_drho + u_force_g);
+    st[0] += (double)ux; st[1] += (double)uy; st[2] += (double)uz; st[3] += (double)u2; st[4] += (double)c;
     st[5] = fmax(st[5], (double)u2);
     bad |= !(u2 < R(1e30));
 
     // ---- main pass over the pairs ------------------------------------------
-    R Z[Q], mom[Q];
+    R z0, mom[Q];
+    V zp[NPAIR];
 #pragma unroll
     for (int j = 0; j < Q; ++j) mom[j] = R(0);
     {  // rest direction: no derivatives, avg = lap(mu) of the site
-      R h0, x0;
-      dir_terms<R, MRT>(q, weight<R>(0), R(0), R(0), R(0), R(0), R(0), R(0), lmu, g[0], h0, x0, Z[0]);
+      const R w = weight<R>(0);
+      const R wut = -w * q.gu2, G = w + wut;
+      const R h0 = G * (q.C0 + q.mob * lmu);
+      const R x0 = (w * q.A1 + q.A2 * wut) - g0;
+      z0 = g0 - q.u_drm * wut - q.u_fg_f * G;
       st_pop<HV<S>>(hout, a0, 0, h0, shh);
       if (MRT) {
 #pragma unroll
         for (int j = 0; j < Q; ++j)
           if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) mom[j] += R(mrt_M(j, 0)) * x0;
       } else {
-        st_pop<GV<S>>(gout, a0, 0, Z[0] + s0 * x0, shg);
+        st_pop<GV<S>>(gout, a0, 0, z0 + s0 * x0, shg);
       }
     }
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
-      const int o = T::off(k), v = 6 * (k >> 1);
-      const R cdc = s_st[(v + 0) * P4T], cdp = s_st[(v + 1) * P4T];
-      const R bca = s_st[(v + 2) * P4T], bcb = s_st[(v + 3) * P4T];
-      const R bpa = s_st[(v + 4) * P4T], bpb = s_st[(v + 5) * P4T];
+      const int o = T::off(k), pr = k >> 1;
+      const R cdc = s_sc[pr * P4T];
+      const V BC = s_sv[(2 * pr) * P4T], BP = s_sv[(2 * pr + 1) * P4T];
       const R lm = s_l[pos - o], lp = s_l[pos + o];
-      const R avg_a = is_site(lp) ? R(0.5) * (lmu + lp) : lmu;
-      const R avg_b = is_site(lm) ? R(0.5) * (lmu + lm) : lmu;
+      // avg of +e takes the +e neighbour, of -e the -e one
+      const V AVG(is_site(lp) ? R(0.5) * (lmu + lp) : lmu, is_site(lm) ? R(0.5) * (lmu + lm) : lmu);
       const R w = weight<R>(k);
       const R uk = ux * R(lat_cx(k)) + uy * R(lat_cy(k)) + uz * R(lat_cz(k));
       const R fproj = bfx * R(lat_cx(k)) + bfy * R(lat_cy(k)) + bfz * R(lat_cz(k));
-      R ha, hb, xa, xb;
-      dir_terms<R, MRT>(q, w, uk, fproj, cdc, cdp, bca, bpa, avg_a, g[k], ha, xa, Z[k]);
-      dir_terms<R, MRT>(q, w, -uk, -fproj, -cdc, -cdp, bcb, bpb, avg_b, g[k + 1], hb, xb, Z[k + 1]);
-      st_pop<HV<S>>(hout, dst(k), k, ha, shh);
-      st_pop<HV<S>>(hout, dst(k + 1), k + 1, hb, shh);
+      // w u_term of +e and -e: w (beta (u.e)^2 - gamma u^2) +- w alpha u.e
+      const R we = w * (R(BETA) * uk * uk - q.gu2), wa = (w * alpha) * uk;
+      const V WUT(we + wa, we - wa);
+      const V G = WUT + V(w);
+      // eq_h + force_h = G (c + S_h + mob avg + hk1 bd_c - c_o bd_p / 2 +- c_o F.e / 2)
+      const R oh = q.hco * fproj;
+      V hb = fma2(V(q.hk1), BC, V(q.C0 + oh, q.C0 - oh));
+      hb = fma2(V(-q.hco), BP, hb);
+      hb = fma2(V(q.mob), AVG, hb);
+      const V H = G * hb;
+      // eq_g = w A1 + A2 wut +- (w m1 / 2 + (m1 / 2 - drho cs2 cd_c / 2) wut),
+      // m1 = mu cd_c + F.e in the MRT equilibrium, -(mu cd_c + F.e) in the BGK
+      // one (device_engine.cuh:517 vs :598)
+      const R m1 = MRT ? q.mu * cdc + fproj : -(q.mu * cdc + fproj);
+      const R o1 = (R(0.5) * w) * m1, o2 = R(0.5) * m1 - q.hdr * cdc;
+      const R wa1 = w * q.A1;
+      const V EG = fma2(V(q.A2), WUT, fma2(V(o2, -o2), WUT, V(wa1 + o1, wa1 - o1)));
+      const V X = EG - gp[pr];
+      // g + force_g = g + (drho cs2 dc - u.drm) wut + (mu dc +- F.e - u.fg_f) G,
+      // dc = (+-cd_c + bd_c) / 2 (device_engine.cuh:609)
+      const R hc = R(0.5) * cdc;
+      const V DC = fma2(V(R(0.5)), BC, V(hc, -hc));
+      const V T1 = fma2(V(q.drho_cs2), DC, V(-q.u_drm));
+      const V T2 = fma2(V(q.mu), DC, V(fproj - q.u_fg_f, -fproj - q.u_fg_f));
+      const V Zk = fma2(T2, G, fma2(T1, WUT, gp[pr]));
+      st_pop<HV<S>>(hout, dst(k), k, H.x(), shh);
+      st_pop<HV<S>>(hout, dst(k + 1), k + 1, H.y(), shh);
       if (MRT) {
-        const R sx = xa + xb, dx = xa - xb;
+        zp[pr] = Zk;
+        const R sx = X.x() + X.y(), dx = X.x() - X.y();
 #pragma unroll
         for (int j = 0; j < Q; ++j) {
           if (mrt_kind(j) == MK_CONS) continue;
@@ -289,8 +319,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
           else if (mjk != 0) mom[j] += R(mjk) * vv;
         }
       } else {
-        st_pop<GV<S>>(gout, dst(k), k, Z[k] + s0 * xa, shg);
-        st_pop<GV<S>>(gout, dst(k + 1), k + 1, Z[k + 1] + s0 * xb, shg);
+        const V out = fma2(V(s0), X, Zk);
+        st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
+        st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
       }
     }
     if (MRT) {
@@ -308,7 +339,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
 #pragma unroll
       for (int j = 0; j < Q; ++j)
         if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) back0 += R(mrt_M(j, 0)) * mom[j];
-      st_pop<GV<S>>(gout, a0, 0, Z[0] + back0, shg);
+      st_pop<GV<S>>(gout, a0, 0, z0 + back0, shg);
 #pragma unroll
       for (int k = 1; k < Q; k += 2) {
         R E = 0, O = 0;
@@ -322,8 +353,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
           else if (mjk == -1) acc -= mom[j];
           else if (mjk != 0) acc += R(mjk) * mom[j];
         }
-        st_pop<GV<S>>(gout, dst(k), k, Z[k] + (E + O), shg);
-        st_pop<GV<S>>(gout, dst(k + 1), k + 1, Z[k + 1] + (E - O), shg);
+        const V out = zp[k >> 1] + V(E + O, E - O);
+        st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
+        st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
       }
     }
   }

@@ -35,6 +35,7 @@
 #include "d3q19.hpp"
 #include "layout.hpp"
 #include "mrt.hpp"
+#include "pair2.cuh"
 
 namespace fe {
 
@@ -550,7 +551,9 @@ __device__ __forceinline__ R corr_c(R c, double lambda) {
 // reads the site indices of all its positions, then issues all its gathers
 // before the first use, so a CTA waits for one round of L2/HBM latency instead
 // of one per position. The fields are read-only for the kernel (__ldg).
-template <class Sh, int H, int NF, int NT = CTA, class R, class F>
+// With IL, fields 0 and 1 go to one interleaved tile (dst[1] = dst[0] + 1,
+// stride 2), read back as two-lane pairs.
+template <class Sh, int H, int NF, int NT = CTA, bool IL = false, class R, class F>
 __device__ __forceinline__ void stage(const F* const (&src)[NF], R* const (&dst)[NF], bool correct, double lambda,
                                       const int32_t* __restrict__ s_idx) {
   using T = Tile<Sh, H>;
@@ -577,7 +580,7 @@ __device__ __forceinline__ void stage(const F* const (&src)[NF], R* const (&dst)
           x = (R)v[u][f];
           if (f == 0 && correct) x = corr_c<R>(x, lambda);
         }
-        dst[f][t] = x;
+        dst[f][(IL && f < 2) ? 2 * t : t] = x;
       }
     }
   }
@@ -634,6 +637,35 @@ __device__ __forceinline__ void pair_derivs(R c0, R cm, R cp, R cm2, R cp2, R p0
   bpa = bd_sel<HBB>(p0, pm, pp, pm2, pp2, sm, sp, sm2, sp2);
   bpb = bd_sel<HBB>(p0, pp, pm, pp2, pm2, sp, sm, sp2, sm2);
 }
+// cd_sel / bd_sel on two-lane (c, p) pairs: the same cases, both fields per
+// instruction.
+template <bool HBB, class R>
+__device__ __forceinline__ V2<R> cd_sel2(V2<R> f0, V2<R> fm, V2<R> fp, bool sm, bool sp) {
+  using V = V2<R>;
+  if (HBB) return V(R(0.5)) * (sel(sp, fp, f0) - sel(sm, fm, f0));
+  return sel(sm && sp, V(R(0.5)) * (fp - fm), V(R(0)));
+}
+template <bool HBB, class R>
+__device__ __forceinline__ V2<R> bd_sel2(V2<R> f0, V2<R> fm, V2<R> fp, V2<R> fm2, V2<R> fp2, bool sm, bool sp,
+                                         bool sm2, bool sp2) {
+  using V = V2<R>;
+  const V two = fma2(V(R(-0.5)), fp2, fma2(V(R(2)), fp, V(R(-1.5)) * f0));
+  const V one = HBB ? fma2(V(R(1.5)), fp, V(R(-1.5)) * f0) : fma2(V(R(2)), fp, V(R(-2)) * f0);
+  const V back = HBB ? sel(sm, fma2(V(R(-0.5)), fm, V(R(0.5)) * f0), V(R(0)))
+                     : sel(sm && sm2, fma2(V(R(-0.5)), fm2, fma2(V(R(2)), fm, V(R(-1.5)) * f0)), V(R(0)));
+  return sel(sp, sel(sp2, two, one), back);
+}
+// pair_derivs on (c, p) pairs: central value for +e, biased values for +e (ba)
+// and -e (bb); the solid positions are read from the c lane.
+template <bool HBB, class R>
+__device__ __forceinline__ void pair_derivs2(V2<R> f0, V2<R> fm, V2<R> fp, V2<R> fm2, V2<R> fp2, V2<R>& cd,
+                                             V2<R>& ba, V2<R>& bb) {
+  const bool sm = is_site(fm.x()), sp = is_site(fp.x()), sm2 = is_site(fm2.x()), sp2 = is_site(fp2.x());
+  cd = cd_sel2<HBB>(f0, fm, fp, sm, sp);
+  ba = bd_sel2<HBB>(f0, fm, fp, fm2, fp2, sm, sp, sm2, sp2);
+  bb = bd_sel2<HBB>(f0, fp, fm, fp2, fm2, sp, sm, sp2, sm2);
+}
+
 // Laplacian term of direction k (k_lap_mf), boundary half `bnd`
 template <class R>
 __device__ __forceinline__ R lap_val(R f0, R fm, R fp, R bnd, bool hbb) {
