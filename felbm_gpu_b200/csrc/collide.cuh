@@ -20,10 +20,16 @@
 //    four gradients (central / biased, of c and p) and keeps the five
 //    per-pair values the main pass needs (cd_c, bd_c and bd_p of both
 //    directions) in a per-thread shared-memory stash;
-//  * the MRT transform uses the row parity of the moment basis: even rows see
-//    x_k + x_{k+1}, odd rows x_k - x_{k+1}, and the back transform gives the
-//    pair as E +- O; only g + force_g (19 values) and the 15 relaxed moments
-//    stay live until the g stores.
+//  * the MRT transform (MRT == 1) uses the row parity of the moment basis:
+//    even rows see x_k + x_{k+1}, odd rows x_k - x_{k+1}, and the back
+//    transform gives the pair as E +- O; only g + force_g (19 values) and the
+//    15 relaxed moments stay live until the g stores;
+//  * with one rate s_e for every even non-conserved moment and one rate s_o
+//    for every odd one (the reference's own assignment, device_engine.cuh:625),
+//    M^-1 S M is exact in closed form (MRT == 2): the even rows with rho span
+//    the even subspace and the odd rows with j the odd one, so the collision
+//    adds s_e (x+ - sum(x) / 19) + s_o (x- - e.J / 10), x+- = (x_k +- x_{k+1})
+//    / 2 and J = sum_k e_k x_k; the 19x15 transforms become two sums.
 #pragma once
 #include <type_traits>
 
@@ -94,6 +100,15 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     R* const dst[3] = {reinterpret_cast<R*>(s_cp), reinterpret_cast<R*>(s_cp) + 1, s_l};
     stage<Sh, 2, 3, P4T, true>(src, dst, true, s.lambda, s_idx);
   }
+  if (!WIDE) {
+    // from here on the index tile holds each site's AoSoA population base
+    // (below 2^32 - 1 for narrow offsets; 0xffffffff marks no site), so a
+    // push target is one add; every thread rewrites the positions it staged
+    for (int t = threadIdx.x; t < T::N; t += P4T) {
+      const int32_t v = s_idx[t];
+      if (v >= 0) s_idx[t] = (int32_t)((uint32_t)(v >> 5) * (uint32_t)(Q * AOSOA) + (uint32_t)(v & (AOSOA - 1)));
+    }
+  }
   __syncthreads();
 
   const DevPrm& Pm = D.prm;
@@ -132,9 +147,14 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     // push target of direction k: slot k of x + e_k, or slot opp(k) of x
     // (halfway bounce-back) when x + e_k is solid
     auto dst = [&](int k) -> IX {
-      const int dn = s_idx[pos + T::off(k)];
-      return dn >= 0 ? (IX)(dn >> 5) * (IX)(Q * AOSOA) + (IX)(k * AOSOA + (dn & (AOSOA - 1)))
-                     : a0 + (IX)(lat_opp(k) * AOSOA);
+      if constexpr (WIDE) {
+        const int dn = s_idx[pos + T::off(k)];
+        return dn >= 0 ? (IX)(dn >> 5) * (IX)(Q * AOSOA) + (IX)(k * AOSOA + (dn & (AOSOA - 1)))
+                       : a0 + (IX)(lat_opp(k) * AOSOA);
+      } else {
+        const uint32_t b = (uint32_t)s_idx[pos + T::off(k)];
+        return b != 0xffffffffu ? b + (uint32_t)(k * AOSOA) : a0 + (uint32_t)(lat_opp(k) * AOSOA);
+      }
     };
     // ---- pre-pass: near-wall cases once, the four gradients, stash -----------
     // lanes (c, p): ec central sums, eb biased sums, per axis
@@ -248,10 +268,19 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     bad |= !(u2 < R(1e30));
 
     // ---- main pass over the pairs ------------------------------------------
+    const R hl = R(0.5) * lmu;
     R z0, mom[Q];
     V zp[NPAIR];
 #pragma unroll
     for (int j = 0; j < Q; ++j) mom[j] = R(0);
+    // two-rate form: the parity rates, sum(x) and J
+    R hse = R(0), hso = R(0), sumx = R(0), jsx = R(0), jsy = R(0), jsz = R(0);
+    if (MRT == 2) {
+      const R s1 = R(2) / (R(2) * (R)Pm.mrt_lambda * itau + R(1));
+      const int me = Pm.rate_mode[MK_E], mo = Pm.rate_mode[MK_Q];
+      hse = R(0.5) * (me == RATE_S0 ? s0 : (me == RATE_MAGIC ? s1 : (R)Pm.rate_value[MK_E]));
+      hso = R(0.5) * (mo == RATE_S0 ? s0 : (mo == RATE_MAGIC ? s1 : (R)Pm.rate_value[MK_Q]));
+    }
     {  // rest direction: no derivatives, avg = lap(mu) of the site
       const R w = weight<R>(0);
       const R wut = -w * q.gu2, G = w + wut;
@@ -259,10 +288,13 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const R x0 = (w * q.A1 + q.A2 * wut) - g0;
       z0 = g0 - q.u_drm * wut - q.u_fg_f * G;
       st_pop<HV<S>>(hout, a0, 0, h0, shh);
-      if (MRT) {
+      if (MRT == 1) {
 #pragma unroll
         for (int j = 0; j < Q; ++j)
           if (mrt_kind(j) != MK_CONS && mrt_M(j, 0) != 0) mom[j] += R(mrt_M(j, 0)) * x0;
+      } else if (MRT == 2) {
+        sumx = x0;
+        z0 += R(2) * hse * x0;
       } else {
         st_pop<GV<S>>(gout, a0, 0, z0 + s0 * x0, shg);
       }
@@ -274,7 +306,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const V BC = s_sv[(2 * pr) * P4T], BP = s_sv[(2 * pr + 1) * P4T];
       const R lm = s_l[pos - o], lp = s_l[pos + o];
       // avg of +e takes the +e neighbour, of -e the -e one
-      const V AVG(is_site(lp) ? R(0.5) * (lmu + lp) : lmu, is_site(lm) ? R(0.5) * (lmu + lm) : lmu);
+      const V la = fma2(V(R(0.5)), V(lp, lm), V(hl));
+      const V AVG(is_site(lp) ? la.x() : lmu, is_site(lm) ? la.y() : lmu);
       const R w = weight<R>(k);
       const R uk = ux * R(lat_cx(k)) + uy * R(lat_cy(k)) + uz * R(lat_cz(k));
       const R fproj = bfx * R(lat_cx(k)) + bfy * R(lat_cy(k)) + bfz * R(lat_cz(k));
@@ -305,7 +338,15 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const V Zk = fma2(T2, G, fma2(T1, WUT, gp[pr]));
       st_pop<HV<S>>(hout, dst(k), k, H.x(), shh);
       st_pop<HV<S>>(hout, dst(k + 1), k + 1, H.y(), shh);
-      if (MRT) {
+      if (MRT == 2) {
+        const R sx = X.x() + X.y(), dx = X.x() - X.y();
+        sumx += sx;
+        if (lat_cx(k)) jsx += R(lat_cx(k)) * dx;
+        if (lat_cy(k)) jsy += R(lat_cy(k)) * dx;
+        if (lat_cz(k)) jsz += R(lat_cz(k)) * dx;
+        const R te = hse * sx, to = hso * dx;
+        zp[pr] = Zk + V(te + to, te - to);
+      } else if (MRT == 1) {
         zp[pr] = Zk;
         const R sx = X.x() + X.y(), dx = X.x() - X.y();
 #pragma unroll
@@ -324,7 +365,20 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
         st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
       }
     }
-    if (MRT) {
+    if (MRT == 2) {
+      // remove the mass and momentum parts of the relaxation
+      const R mx = R(2) * hse * sumx * R(1.0 / 19.0);
+      const R qx = R(0.2) * hso * jsx, qy = R(0.2) * hso * jsy, qz = R(0.2) * hso * jsz;
+      st_pop<GV<S>>(gout, a0, 0, z0 - mx, shg);
+#pragma unroll
+      for (int k = 1; k < Q; k += 2) {
+        const R ej = qx * R(lat_cx(k)) + qy * R(lat_cy(k)) + qz * R(lat_cz(k));
+        const V out = zp[k >> 1] - V(mx + ej, mx - ej);
+        st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
+        st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
+      }
+    }
+    if (MRT == 1) {
       // rates (reference device_engine.cuh:623-625, with per-kind modes)
       // s1 = 2 tau / (2 Lambda + tau) with tau = 1 / s0 - 1/2 = 1 / itau
       const R s1 = R(2) / (R(2) * (R)Pm.mrt_lambda * itau + R(1));

@@ -226,7 +226,9 @@ static int build_layout(const uint8_t* solid, int nx, int ny, int nz, int shape,
 
 enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
 
-// The collide-pass variants: collision model, near-wall rule, and 64-bit
+// The collide-pass variants: collision model (0 BGK, 1 MRT, 2 MRT in the
+// two-rate form, built for halfway bounce-back with 32-bit offsets only; the
+// general MRT serves every other case), near-wall rule, and 64-bit
 // population offsets for lattices whose arrays reach 2^32 entries.
 template <class S, class Sh, int MRT, bool HBB>
 static void launch_collide_w(bool wide, int nwork, size_t smem, cudaStream_t st, const LatDesc* desc,
@@ -235,9 +237,10 @@ static void launch_collide_w(bool wide, int nwork, size_t smem, cudaStream_t st,
   else k_collide<S, Sh, MRT, HBB, false><<<nwork, P4T, smem, st>>>(desc, work, par);
 }
 template <class S, class Sh>
-static void launch_collide(bool mrt, bool hbb, bool wide, int nwork, size_t smem, cudaStream_t st,
+static void launch_collide(int mrt, bool hbb, bool wide, int nwork, size_t smem, cudaStream_t st,
                            const LatDesc* desc, const int2* work, int par) {
-  if (mrt && hbb) launch_collide_w<S, Sh, 1, true>(wide, nwork, smem, st, desc, work, par);
+  if (mrt == 2 && hbb && !wide) k_collide<S, Sh, 2, true, false><<<nwork, P4T, smem, st>>>(desc, work, par);
+  else if (mrt && hbb) launch_collide_w<S, Sh, 1, true>(wide, nwork, smem, st, desc, work, par);
   else if (mrt) launch_collide_w<S, Sh, 1, false>(wide, nwork, smem, st, desc, work, par);
   else if (hbb) launch_collide_w<S, Sh, 0, true>(wide, nwork, smem, st, desc, work, par);
   else launch_collide_w<S, Sh, 0, false>(wide, nwork, smem, st, desc, work, par);
@@ -257,6 +260,7 @@ static cudaError_t collide_smem_attr(int bytes) {
   set((const void*)k_collide<S, Sh, 1, false, true>);
   set((const void*)k_collide<S, Sh, 1, true, false>);
   set((const void*)k_collide<S, Sh, 1, true, true>);
+  set((const void*)k_collide<S, Sh, 2, true, false>);
   return e;
 }
 // True when the lattice's population arrays reach 2^32 entries.
@@ -350,6 +354,13 @@ struct Engine {
   }
   size_t fld_size() const { return storage == FE_F64 ? 8 : 4; }
 
+  // The collide kernel this lattice runs: 0 BGK, 1 MRT, 2 MRT in the
+  // two-rate form (halfway bounce-back, 32-bit offsets).
+  int collide_variant() const {
+    if (!hd.prm.use_mrt) return 0;
+    return (hd.prm.two_rate && hd.prm.hbb && !wide) ? 2 : 1;
+  }
+
   void fill_prm() {
     DevPrm& d = hd.prm;
     d.rho0 = P.rho0; d.rho1 = P.rho1; d.drho = P.rho0 - P.rho1;
@@ -362,6 +373,17 @@ struct Engine {
       d.rate_value[q] = P.mrt_rate_value[q];
     }
     d.use_mrt = P.use_mrt; d.hbb = P.use_halfway_bb; d.correct_mass = P.correct_op_mass;
+    {
+      // one rate per moment parity (FELBM_GENERAL_MRT=1 keeps the general
+      // transform, for tests)
+      auto same = [&](int a, int b) {
+        return P.mrt_rate_mode[a] == P.mrt_rate_mode[b] &&
+               (P.mrt_rate_mode[a] != FE_RATE_FIXED || P.mrt_rate_value[a] == P.mrt_rate_value[b]);
+      };
+      const char* gm = std::getenv("FELBM_GENERAL_MRT");
+      d.two_rate = same(FE_MRT_E, FE_MRT_EPS) && same(FE_MRT_E, FE_MRT_NU) && same(FE_MRT_E, FE_MRT_PI) &&
+                   same(FE_MRT_Q, FE_MRT_M) && !(gm && gm[0] == '1');
+    }
     d.need_j = (P.rho0 != P.rho1 || open_bnd) ? 1 : 0;
     d.forcing_timedep = P.forcing_timedep; d.forcing_period = P.forcing_period;
     d.c_ref = P.c_ref; d.p_ref = P.p_ref;
@@ -542,7 +564,7 @@ struct Engine {
     if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
     else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
     rec(4);
-    launch_collide<S, Sh>(hd.prm.use_mrt != 0, hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
+    launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
     launches += 4;
   }
@@ -959,19 +981,19 @@ struct Batch {
     }
     std::vector<int2> gw;
     std::vector<size_t> offs;
+    // one group per collide variant, so each member runs the kernel it runs alone
     for (int sh = 0; sh < NSHAPE; ++sh)
-      for (int mrt = 0; mrt < 2; ++mrt)
+      for (int mrt = 0; mrt < 3; ++mrt)
         for (int hbb = 0; hbb < 2; ++hbb) {
           const size_t off = gw.size();
           for (size_t q = 0; q < mem.size(); ++q)
-            if (mem[q]->shape == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
-                (mem[q]->hd.prm.hbb != 0) == (hbb != 0))
+            if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt && (mem[q]->hd.prm.hbb != 0) == (hbb != 0))
               for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
           if (gw.size() == off) continue;
           Group g;
           for (size_t q = 0; q < mem.size(); ++q)
-            if (mem[q]->shape == sh && (mem[q]->hd.prm.use_mrt != 0) == (mrt != 0) &&
-                (mem[q]->hd.prm.hbb != 0) == (hbb != 0) && mem[q]->wide)
+            if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt && (mem[q]->hd.prm.hbb != 0) == (hbb != 0) &&
+                mem[q]->wide)
               g.wide = 1;
           g.shape = sh;
           g.mrt = mrt;
@@ -1002,7 +1024,7 @@ struct Batch {
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {
     const size_t sm = CollideSmem<Sh, typename S::real>::BYTES;
-    launch_collide<S, Sh>(g.mrt != 0, g.hbb != 0, g.wide != 0, g.nwork, sm, st, d_desc, g.d_work, par);
+    launch_collide<S, Sh>(g.mrt, g.hbb != 0, g.wide != 0, g.nwork, sm, st, d_desc, g.d_work, par);
   }
   template <class S>
   void launch_step_t(int par, cudaStream_t st) {

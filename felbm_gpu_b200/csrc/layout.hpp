@@ -70,6 +70,9 @@ struct DevPrm {
   double rate_value[7];
   int rate_mode[7];
   int use_mrt, hbb, correct_mass;
+  // MRT rates that depend on the moment's parity only (every even kind one
+  // rate, every odd kind another): the collide pass may take the two-rate form
+  int two_rate;
   int need_j;  // P1 writes the momentum (drho != 0 or open boundaries)
   int forcing_timedep;
   double forcing_period;

@@ -521,6 +521,8 @@ int fe_autotune(const fe_params* p, int nx, int ny, int nz, const uint8_t* solid
 int fe_tune_save(const char* path);
 int fe_tune_load(const char* path);
 int fe_tune_clear(void);
+/* Device time of each pass summed over nsteps plain steps: [0] moments,
+ * [1] open-boundary kernels, [2] c field, [3] Laplacian of mu, [4] collide. */
 int fe_time_kernels(fe_engine* e, int nsteps, float* ms_per_kernel, int nkernels);
 /* Number of kernels the engine launched since creation. */
 int fe_launch_count(const fe_engine* e, int64_t* count);

@@ -160,3 +160,42 @@ def test_wide_offsets_agree_with_narrow(require_gpu, storage, monkeypatch):
         b.free()
         for e in engines.values():
             e.free()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_two_rate_form_equals_general_transform(require_gpu, storage, monkeypatch):
+    """MRT with one rate per moment parity (the reference's rate assignment)
+    runs the closed two-rate form of M^-1 S M; FELBM_GENERAL_MRT=1 forces the
+    19x15 transform. Both are the same linear map, so the states agree to
+    rounding; cyl2d_mrt's explicit rates always take the general transform,
+    and a batch mixing both forms gives every member its result alone."""
+    steps = 23
+    tol = 1e-12 if storage == "f64" else 2e-6
+    names = ["spheres_mrt", "grf_mrt_mass", "spheres_mrt_wet"]
+    fast = {n: alone(n, storage, steps) for n in names}
+    monkeypatch.setenv("FELBM_GENERAL_MRT", "1")
+    for n in names:
+        h, g, _, _ = alone(n, storage, steps)
+        d = max(np.max(np.abs(h - fast[n][0])), np.max(np.abs(g - fast[n][1])))
+        assert 0 < d <= tol, (n, d)  # 0 would mean the switch changed nothing
+    # engines made under FELBM_GENERAL_MRT=1 keep the general transform
+    general = make_engine("grf_mrt_mass", storage)
+    monkeypatch.delenv("FELBM_GENERAL_MRT")
+    b = Batch()
+    engines = {"general": general, "fast": make_engine("grf_mrt_mass", storage),
+               "cyl2d_mrt": make_engine("cyl2d_mrt", storage)}
+    try:
+        monkeypatch.setenv("FELBM_GENERAL_MRT", "1")
+        ref_general = alone("grf_mrt_mass", storage, steps)
+        monkeypatch.delenv("FELBM_GENERAL_MRT")
+        ref = {"general": ref_general, "fast": fast["grf_mrt_mass"], "cyl2d_mrt": alone("cyl2d_mrt", storage, steps)}
+        for e in engines.values():
+            b.add(e)
+        b.run(steps)
+        for n, e in engines.items():
+            h, g = e.download_state()
+            assert np.array_equal(h, ref[n][0]) and np.array_equal(g, ref[n][1]), n
+    finally:
+        b.free()
+        for e in engines.values():
+            e.free()
