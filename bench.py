@@ -466,7 +466,10 @@ def main():
         # goes host->device (fe_upload_state, FP64 in the reference layout),
         # then the reference driver loop runs K steps (per step the forcing
         # factor goes host->device, step + mass correction, and the flow
-        # statistics come back device->host), and the final state comes back
+        # statistics of every step come back device->host through the
+        # asynchronous form, flow_stats_launch / _collect: step t's are
+        # collected once step t+1 is queued, so the device does not idle
+        # while the host reads them), and the final state comes back
         # (fe_download_state). Host wall clock around all of it.
         ke = args.steps
         torch.cuda.synchronize()
@@ -474,11 +477,14 @@ def main():
         t0 = time.perf_counter()
         eng.upload_state(h0, g0)
         eng.record_target_mass()
-        for _ in range(ke):
+        for t in range(ke):
             eng.set_forcing_factor(1.0)
             eng.step(1)
             eng.apply_mass_correction(want_drift=False)
-            eng.flow_stats()
+            if t:
+                eng.flow_stats_collect()  # step t-1's, read while step t runs
+            eng.flow_stats_launch()
+        eng.flow_stats_collect()
         hd, gd = eng.download_state()
         torch.cuda.synchronize()
         barrier()
@@ -493,7 +499,8 @@ def main():
                "h2d_bytes_per_step": (state_bytes + ke * 8) / ke,
                "d2h_bytes_per_step": (state_bytes + ke * 48 + 16) / ke, "steps": ke,
                "what": "one job: fe_upload_state (host FP64 state) + K x (fe_set_forcing_factor, fe_step, "
-                       "fe_apply_mass_correction, fe_flow_stats) + fe_download_state, host wall clock"}
+                       "fe_apply_mass_correction, fe_flow_stats_launch, and step t-1's "
+                       "fe_flow_stats_collect) + fe_download_state, host wall clock"}
     production = None
     if not args.no_tracers:
         # the production loop: 12,000 GPU tracers (diffusivity ladder

@@ -224,6 +224,9 @@ static int build_layout(const uint8_t* solid, int nx, int ny, int nz, int shape,
   return FE_OK;
 }
 
+// Sets the control block's correction flag (fe_apply_mass_correction).
+__global__ void k_queue_correction(Ctl* c) { c->pending = 1; }
+
 enum KernelId { K_P1 = 0, K_BC = 1, K_P2 = 2, K_P3 = 3, K_P4 = 4, K_N = 5 };
 
 // The collide-pass variants: collision model (0 BGK, 1 MRT, 2 MRT in the
@@ -681,6 +684,15 @@ struct Engine {
 
   int mass_pass() {
     FE_DISPATCH(*this, (k_mass<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_partm)));
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    return FE_OK;
+  }
+
+  // Queue the order-parameter mass correction for the next step: the flag is
+  // set by a one-thread kernel in stream order, so the host does not wait.
+  int queue_correction() {
+    k_queue_correction<<<1, 1, 0, stream>>>(d_ctl);
     ++launches;
     FE_CUDA(cudaGetLastError());
     return FE_OK;
@@ -1669,9 +1681,8 @@ int fe_apply_mass_correction(fe_engine* e, double* drift) {
     if (drift) *drift = 0.0;
     return FE_OK;
   }
-  int32_t one = 1;
   int rc;
-  if ((rc = E.write_ctl_field(offsetof(fe::Ctl, pending), &one, 4))) return rc;
+  if ((rc = E.queue_correction())) return rc;
   if (!drift) return FE_OK;
   // form M and lambda now so that the drift can be returned
   if ((rc = E.mass_pass())) return rc;
