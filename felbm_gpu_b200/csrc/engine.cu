@@ -288,6 +288,7 @@ struct Engine {
   double* d_tmp = nullptr;    // state/field transfer buffer
   int64_t tmp_len = 0;
   double* d_partm = nullptr;
+  double* d_stats_blk = nullptr;  // [STATS_BLOCKS][6] block sums of k_stats_finalize
   int parity = 0;             // buffer holding the current state
   int64_t t_host = 0;
   int64_t launches = 0;
@@ -493,6 +494,7 @@ struct Engine {
     if ((rc = alloc(&D.part4, (size_t)nbk * P4W * 6))) return rc;
     FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * P4W * 6 * 8));
     if ((rc = alloc(&d_partm, (size_t)D.nchunks * 2))) return rc;
+    if ((rc = alloc(&d_stats_blk, (size_t)STATS_BLOCKS * 6))) return rc;
     if ((rc = alloc(&d_ctl, 1))) return rc;
     Ctl c0{};
     c0.ff_manual = 1.0;
@@ -817,7 +819,7 @@ struct Engine {
   }
 
   int stats_launch() {
-    FE_DISPATCH(*this, (k_stats_finalize<Sh><<<1, CTA, 0, stream>>>(d_desc, 0)));
+    FE_DISPATCH(*this, (k_stats_finalize<Sh><<<STATS_BLOCKS, CTA, 0, stream>>>(d_desc, 0, d_stats_blk)));
     ++launches;
     FE_CUDA(cudaGetLastError());
     FE_CUDA(cudaMemcpyAsync(h_stats, reinterpret_cast<char*>(d_ctl) + offsetof(Ctl, stats), 6 * sizeof(double),

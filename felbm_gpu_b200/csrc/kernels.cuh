@@ -1146,15 +1146,30 @@ __global__ void __launch_bounds__(CTA) k_mass(const LatDesc* __restrict__ descs,
   }
 }
 
-// Sum the flow-statistics partials of the last collision pass into ctl->stats.
+// Sum the flow-statistics partials of the last collision pass (one record
+// per collide warp) into ctl->stats. Each of the STATS_BLOCKS blocks sums a
+// fixed contiguous range of records into blk[block]; the last block to finish
+// sums those in block order, so every call adds in the same order.
+constexpr int STATS_BLOCKS = 148;
 template <class Sh>
-__global__ void __launch_bounds__(CTA) k_stats_finalize(const LatDesc* __restrict__ descs, int lat) {
+__global__ void __launch_bounds__(CTA) k_stats_finalize(const LatDesc* __restrict__ descs, int lat,
+                                                         double* __restrict__ blk) {
   __shared__ Red s;
   const LatDesc& D = descs[lat];
+  const int count = D.nbricks * P4W;
+  const int per = (count + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int r0 = min(count, (int)blockIdx.x * per), r1 = min(count, r0 + per);
   double tot[6];
-  sum_partials<6>(D.part4, D.nbricks * P4W, 6, tot, s, true);  // one record per collide warp
+  sum_partials<6>(D.part4 + (int64_t)r0 * 6, r1 - r0, 6, tot, s, true);
   if (threadIdx.x == 0)
-    for (int q = 0; q < 6; ++q) D.ctl->stats[q] = tot[q];
+    for (int q = 0; q < 6; ++q) blk[blockIdx.x * 6 + q] = tot[q];
+  if (last_block(&D.ctl->counts, gridDim.x, s)) {
+    sum_partials<6>(blk, gridDim.x, 6, tot, s, true);
+    if (threadIdx.x == 0) {
+      for (int q = 0; q < 6; ++q) D.ctl->stats[q] = tot[q];
+      D.ctl->counts = 0;
+    }
+  }
 }
 
 }  // namespace fe
