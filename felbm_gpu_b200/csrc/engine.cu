@@ -722,14 +722,36 @@ struct Engine {
       if ((rc = mass_pass())) return rc;
       apply = 1;
     }
-    FE_DISPATCH(*this, (k_download_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
-                                                                                  d_tmp + Vn, apply)));
-    ++launches;
-    FE_CUDA(cudaGetLastError());
-    FE_CUDA(copy_to_host(h, d_tmp, Vn * sizeof(double)));
-    FE_CUDA(copy_to_host(g, d_tmp + Vn, Vn * sizeof(double)));
+    Staging* sg = narrow_transfers(Vn);
+    if (sg) {  // FP32 values on the link, widened on the host (exact)
+      float* t = reinterpret_cast<float*>(d_tmp);
+      FE_DISPATCH(*this, (k_download_state<S, float><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, t,
+                                                                                         t + Vn, apply)));
+      ++launches;
+      FE_CUDA(cudaGetLastError());
+      FE_CUDA(sg->to_host_widen(h, t, (size_t)Vn, stream));
+      FE_CUDA(sg->to_host_widen(g, t + Vn, (size_t)Vn, stream));
+    } else {
+      FE_DISPATCH(*this, (k_download_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
+                                                                                    d_tmp + Vn, apply)));
+      ++launches;
+      FE_CUDA(cudaGetLastError());
+      FE_CUDA(copy_to_host(h, d_tmp, Vn * sizeof(double)));
+      FE_CUDA(copy_to_host(g, d_tmp + Vn, Vn * sizeof(double)));
+    }
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
+  }
+  // The staging area for state transfers of Vn values per lattice in FP32
+  // (storages whose arithmetic is FP32: their values are FP32 numbers, so
+  // narrowing on the host is what the device's conversion does and widening
+  // is exact), or nullptr for the FP64 path (also taken under
+  // FELBM_FP64_TRANSFERS=1, for tests).
+  Staging* narrow_transfers(int64_t Vn) const {
+    if (storage == FE_F64 || (size_t)Vn * sizeof(float) < (size_t(4) << 20)) return nullptr;
+    const char* w = std::getenv("FELBM_FP64_TRANSFERS");
+    if (w && w[0] == '1') return nullptr;
+    return Staging::get();
   }
   // Large transfers through the pinned staging buffers (plain copies if
   // those cannot be allocated).
@@ -766,10 +788,19 @@ struct Engine {
     if ((rc = tracer_hook(-1, state_id, false))) return rc;  // deferred tracer advances see the old state
     ++state_id;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
-    FE_CUDA(copy_to_device(d_tmp, h, Vn * sizeof(double)));
-    FE_CUDA(copy_to_device(d_tmp + Vn, g, Vn * sizeof(double)));
-    FE_DISPATCH(*this, (k_upload_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
-                                                                                d_tmp + Vn)));
+    Staging* sg = narrow_transfers(Vn);
+    if (sg) {  // narrowed on the host, as the device's conversion would
+      float* t = reinterpret_cast<float*>(d_tmp);
+      FE_CUDA(sg->to_device_narrow(t, h, (size_t)Vn, stream));
+      FE_CUDA(sg->to_device_narrow(t + Vn, g, (size_t)Vn, stream));
+      FE_DISPATCH(*this, (k_upload_state<S, float><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, t,
+                                                                                       t + Vn)));
+    } else {
+      FE_CUDA(copy_to_device(d_tmp, h, Vn * sizeof(double)));
+      FE_CUDA(copy_to_device(d_tmp + Vn, g, Vn * sizeof(double)));
+      FE_DISPATCH(*this, (k_upload_state<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
+                                                                                  d_tmp + Vn)));
+    }
     ++launches;
     FE_CUDA(cudaGetLastError());
     int32_t zero = 0;

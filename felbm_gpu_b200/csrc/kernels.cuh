@@ -1004,10 +1004,12 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
 // ---------------------------------------------------------------------------
 // Post-stream state in the reference layout f[k*n + ref(i)] (double), with a
 // queued mass correction injected as the reference's k_inject_mass does.
-template <class S>
+// Out = float for the storages with FP32 arithmetic: the values are the same
+// (each is an FP32 number), widened to double on the host.
+template <class S, class Out = double>
 __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                         int parity, double* __restrict__ h_out,
-                                                         double* __restrict__ g_out, int apply_lambda) {
+                                                         int parity, Out* __restrict__ h_out,
+                                                         Out* __restrict__ g_out, int apply_lambda) {
   using R = typename S::real;
   using PH = typename S::hpop;
   using PG = typename S::gpop;
@@ -1028,7 +1030,7 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
     for (int k = 0; k < Q; ++k) {
       hv[k] = ld_pop<HV<S>>(hin, a + k * AOSOA, k, shh);
       cd += (double)hv[k];
-      g_out[k * n + q] = (double)ld_pop<GV<S>>(gin, a + k * AOSOA, k, shg);
+      g_out[k * n + q] = (Out)ld_pop<GV<S>>(gin, a + k * AOSOA, k, shg);
     }
     const double phi = cd * (1.0 - cd);
     const bool inj = lambda != 0.0 && phi > 0.0;
@@ -1036,7 +1038,7 @@ __global__ void __launch_bounds__(CTA) k_download_state(const LatDesc* __restric
     for (int k = 0; k < Q; ++k) {
       R v = hv[k];
       if (inj) v += (R)(weight<double>(k) * (-lambda * phi));
-      h_out[k * n + q] = (double)v;
+      h_out[k * n + q] = (Out)v;
     }
   }
 }
@@ -1081,10 +1083,12 @@ __global__ void __launch_bounds__(CTA) k_inject(const LatDesc* __restrict__ desc
 
 // Post-stream state from the reference layout (reference upload_state,
 // multiphase_gpu.cuh:354-359).
-template <class S>
+// In = float for the storages with FP32 arithmetic: the host narrowed each
+// value as the conversion below would.
+template <class S, class In = double>
 __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                       int parity, const double* __restrict__ h_in,
-                                                       const double* __restrict__ g_in) {
+                                                       int parity, const In* __restrict__ h_in,
+                                                       const In* __restrict__ g_in) {
   using PH = typename S::hpop;
   using PG = typename S::gpop;
   const int2 wk = work[blockIdx.x];

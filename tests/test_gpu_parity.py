@@ -114,3 +114,47 @@ def test_download_into_caller_buffers(require_gpu):
                 e.download_state(bad, gb)
     finally:
         e.free()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16g", "bf16s"])
+def test_fp32_transfers_equal_fp64_transfers(require_gpu, storage, monkeypatch):
+    """Large state transfers of the FP32-arithmetic storages move FP32 values
+    (narrowed on the host before the copy up, widened after the copy down);
+    FELBM_FP64_TRANSFERS=1 moves FP64 and converts on the device. Both give
+    the same state and the same download, bit for bit, with and without a
+    queued mass correction (64^3, above the size where the FP32 path starts)."""
+    from felbm_gpu_b200 import MultiPhaseGPU, default_params, geometry
+    solid, _ = geometry.grf((64, 64, 64), 4.0, 0.45, 5, flow_axis=0)
+    p = default_params(use_mrt=1, use_halfway_bb=1, correct_op_mass=1, surface_tension=5e-3,
+                       interface_width=4.0, gx=1e-5, storage=storage)
+    rng = np.random.default_rng(3)
+
+    def job(fp64):
+        if fp64:
+            monkeypatch.setenv("FELBM_FP64_TRANSFERS", "1")
+        else:
+            monkeypatch.delenv("FELBM_FP64_TRANSFERS", raising=False)
+        e = MultiPhaseGPU(p, solid)
+        try:
+            assert e.Vn * 4 >= 4 << 20
+            w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+            h = (w[:, None] * c_fixed[None, :]).ravel()
+            g = (w[:, None] * (1.0 + 0.01 * c_fixed[None, :])).ravel()
+            e.upload_state(h, g)
+            e.record_target_mass()
+            e.run(3)
+            out = [np.concatenate(e.download_state())]
+            e.apply_mass_correction(want_drift=False)
+            out.append(np.concatenate(e.download_state()))
+            return out
+        finally:
+            e.free()
+
+    e0 = MultiPhaseGPU(p, solid)
+    n = e0.n
+    e0.free()
+    c_fixed = 0.5 + 0.5 * np.tanh(rng.standard_normal(n))
+    a = job(False)
+    b = job(True)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
