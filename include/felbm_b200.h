@@ -171,10 +171,15 @@ int fe_set_params(fe_engine* e, const fe_params* p);
 void* fe_engine_stream(fe_engine* e);
 
 /* ---- state ------------------------------------------------------------- */
-/* Replaces upload_state (multiphase_gpu.cuh:354-359): h, g are Vn doubles. */
+/* Replaces upload_state (multiphase_gpu.cuh:354-359): h, g are Vn doubles.
+ * Large states of the storages other than FE_F64 cross the link as FP32
+ * (narrowed on the host, the conversion the device would apply); the
+ * stored state is the same either way. */
 int fe_upload_state(fe_engine* e, const double* h, const double* g, int64_t vn);
 /* Replaces download_state (multiphase_gpu.cuh:449-455); includes a pending
- * order-parameter mass correction, as the reference's state would. */
+ * order-parameter mass correction, as the reference's state would. Storages
+ * other than FE_F64 hold FP32 values, which large downloads move as FP32 and
+ * widen on the host (exact). */
 int fe_download_state(fe_engine* e, double* h, double* g, int64_t vn);
 
 /* ---- open boundaries --------------------------------------------------- */
