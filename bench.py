@@ -15,7 +15,10 @@ Arms:
   --impl reference the reference's CPU path on this box's host cores: the CPU
                    oracle (C++/OpenMP restatement of the reference step; the
                    reference's own CPU engine lives in the absent felbm_local
-                   tree), on a bounded sample of the same workload per step.
+                   tree), on the same 300^3 lattice, same seed and parameters.
+                   Its process never loads the engine library: the lattice
+                   and the order parameter are built by a child process and
+                   handed over as arrays.
 
 Multi-GPU (torchrun, N ranks): independent replicas, one lattice per GPU, no
 collective on the data path ("scaling": "weak"); the timed region is
@@ -65,6 +68,14 @@ def parse():
     ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per solve of the 64-solve sweep")
     ap.add_argument("--stream-seconds", type=float, default=15.0, help="arrival window of the request stream")
     ap.add_argument("--stream-rate", type=float, default=4.0, help="Poisson arrival rate (requests / s)")
+    ap.add_argument("--e2e-steps", type=int, default=500,
+                    help="steps of the end-to-end job (one state upload and download per job)")
+    ap.add_argument("--no-ref-kernels", action="store_true",
+                    help="skip timing the reference's own kernels on this GPU")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="also run every storage type against FP64 on the precision configuration")
+    ap.add_argument("--seed", type=int, default=2024, help="seed of the random-field lattice (rank r adds r)")
+    ap.add_argument("--emit-workload", default=None, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -75,22 +86,107 @@ def dist_env():
     return ws, rank, lrank
 
 
-def workload(size: int, seed: int = 2024):
+def workload(size: int, seed: int = 2024, **over):
     """The production dispersion configuration: fluid physics of the
     reference's cfg/3d_image/params.cfg (rho0 = rho1 = 1, tau = 0.9, W = 5,
     sigma = 0.0083, mobility_coeff 0.02) with a 45 degree contact angle
-    (phi = 6 sigma cos 45) and body force 1e-6 along x."""
+    (phi = 6 sigma cos 45) and body force 1e-6 along x, on a random field
+    (correlation length 6) at porosity 0.37, largest x-spanning cluster,
+    periodic, mass correction, slab start. Keyword overrides go to the
+    physics parameters."""
     from felbm_gpu_b200 import default_params, geometry
     shape = (size, size, size)
     solid, por = geometry.grf(shape, 6.0, 0.37, seed, flow_axis=0)
     sigma, W = 0.0083, 5.0
-    p = default_params(rho0=1.0, rho1=1.0, tau0=0.9, tau1=0.9, surface_tension=sigma, interface_width=W,
-                       mobility_coeff=0.02, phi=6 * sigma * np.cos(np.radians(45.0)), gx=1e-6,
-                       use_mrt=1, use_halfway_bb=1, correct_op_mass=1,
-                       stream_matrix_free=1, grad_matrix_free=1, fused=1, fuse_collision=1,
-                       mrt_fast_transform=1, stream_inplace=1)
+    kw = dict(rho0=1.0, rho1=1.0, tau0=0.9, tau1=0.9, surface_tension=sigma, interface_width=W,
+              mobility_coeff=0.02, phi=6 * sigma * np.cos(np.radians(45.0)), gx=1e-6,
+              use_mrt=1, use_halfway_bb=1, correct_op_mass=1,
+              stream_matrix_free=1, grad_matrix_free=1, fused=1, fuse_collision=1,
+              mrt_fast_transform=1, stream_inplace=1)
+    kw.update(over)
+    p = default_params(**kw)
     c = geometry.order_parameter(solid, "slab", W, origin=(0, 0, 0), axis=0, thickness=size // 2)
     h, g = geometry.equilibrium(c, 1.0, p.rho0, p.rho1)
+    return solid, por, p, h, g
+
+
+def plain_workload(size: int = 200, seed: int = 12345, **over):
+    """The plain-method configuration: quasi-2-D size x size x 1, fully
+    periodic, random non-overlapping cylinder pack (radii uniform 6-12,
+    porosity 0.65), density ratio 1, tau 1 in both phases, W = 4,
+    sigma = 1e-3, mobility coefficient 0.02, MRT with s_e = s_eps = 1.19 and
+    s_q = 1.2 (nu rates from tau), slab c = 1 for x < size / 2, body force
+    1e-6 along x, contact angle 90 degrees (phi = 0), halfway bounce-back."""
+    from felbm_gpu_b200 import default_params, geometry
+    solid, _ = geometry.cylinders((1, size, size), 6.0, 12.0, 0.65, seed)
+    kw = dict(rho0=1.0, rho1=1.0, tau0=1.0, tau1=1.0, surface_tension=1e-3, interface_width=4.0,
+              mobility_coeff=0.02, use_mrt=1, use_halfway_bb=1, gx=1e-6, phi=0.0)
+    kw.update(over)
+    p = default_params(**kw)
+    for k, v in ((1, 1.19), (2, 1.19), (3, 1.2)):  # FE_MRT_E, FE_MRT_EPS, FE_MRT_Q fixed
+        p.mrt_rate_mode[k] = 2
+        p.mrt_rate_value[k] = v
+    c = geometry.order_parameter(solid, "slab", 4.0, origin=(0, 0, 0), axis=0, thickness=size // 2)
+    h, g = geometry.equilibrium(c, 1.0, p.rho0, p.rho1)
+    return solid, p, h, g
+
+
+def precision_workload(size: int = 150, mrt: bool = True, seed: int = 7, **over):
+    """The precision configuration: random-field medium (correlation length
+    6, porosity 0.35, largest x-spanning cluster) between open inlet and
+    outlet along x (2 empty + 2 buffer layers, copy_to_buffers), pressure
+    difference 1e-3 in density units, periodic in y and z, contact angle 60
+    degrees, slab start, BGK or MRT. Returns (solid, params, open boundary,
+    h, g, porosity)."""
+    from felbm_gpu_b200 import OpenBoundary, default_params, geometry
+    medium, por = geometry.grf((size, size, size), 6.0, 0.35, seed, flow_axis=0)
+    solid = geometry.pad_open(medium, 0, 2, 2)
+    inl, outl, bv, br, coord = geometry.open_lists(solid, 0, 2, split_axis=1)
+    sigma, W = 1e-3, 4.0
+    kw = dict(rho0=1.0, rho1=1.0, tau0=1.0, tau1=1.0, surface_tension=sigma, interface_width=W,
+              mobility_coeff=0.02, phi=6 * sigma * np.cos(np.radians(60.0)), use_mrt=int(mrt), use_halfway_bb=1)
+    kw.update(over)
+    p = default_params(**kw)
+    ob = OpenBoundary(inlet=inl, outlet=outl, inlet_coord=coord, buf_verts=bv, buf_refs=br, copy_to_buffers=True,
+                      use_in_prs=True, p_in=1.0 + 1e-3 / 3.0, use_out_prs=True, p_out=1.0, use_in_fluid=True,
+                      use_out_fluid=True, c_out_fixed=0.0, inlet_c_a=1.0, rho_out_fixed=p.rho1)
+    nx = solid.shape[2]
+    c = geometry.order_parameter(solid, "slab", W, origin=(0, 0, 0), axis=0, thickness=nx // 2)
+    h, g = geometry.equilibrium(c, 1.0, p.rho0, p.rho1)
+    return solid, p, ob, h, g, por
+
+
+def emit_workload(path: str, size: int, seed: int):
+    """Child process of the reference arm: the workload's mask, order
+    parameter and parameter block into `path` (.npz)."""
+    solid, por, p, h, _ = workload(size, seed)
+    c = h.reshape(Q, -1).sum(axis=0)  # at rest h_k = w_k c
+    np.savez(path, solid=np.packbits(solid.ravel()), shape=np.array(solid.shape), c=c,
+             params=np.frombuffer(bytes(p), np.uint8), porosity=np.array(por))
+
+
+# D3Q19 weights in the velocity order of the C-ABI (rest, 6 axes, 12 edges)
+W19 = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+
+
+def workload_without_engine(size: int, seed: int):
+    """The workload of workload(size, seed) in a process that must not load
+    the engine library: a child process builds it, this one rebuilds the
+    rest-state populations h_k = w_k c, g_k = w_k p0 (p0 = 1) in numpy."""
+    import tempfile
+    from oracle.oracle_py import capi
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "workload.npz")
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--emit-workload", path, "--size", str(size),
+                        "--seed", str(seed)], check=True)
+        z = np.load(path)
+        shape = tuple(int(v) for v in z["shape"])
+        solid = np.unpackbits(z["solid"], count=int(np.prod(shape))).reshape(shape)
+        c = z["c"]
+        p = capi.FeParams.from_buffer_copy(z["params"].tobytes())
+        por = float(z["porosity"])
+    h = (W19[:, None] * c[None, :]).ravel()
+    g = np.repeat(W19, c.size)
     return solid, por, p, h, g
 
 
@@ -175,24 +271,50 @@ def profiled_traffic(storage: str, size: int, brick: str = "8x8x8"):
     return None
 
 
-def cpu_sample_mlups(storage_label: str, seconds: float = 12.0):
-    """The CPU oracle on a bounded sample of the workload: a 100^3 lattice of
-    the same random-field construction, all host threads, steps until ~seconds."""
+def host_threads() -> int:
+    """Host threads this process may run on (the CPU affinity mask, which a
+    container's CPU set narrows), the oracle's OpenMP thread count."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_timing(size: int, seed: int, warmup: int, steps: int):
+    """The CPU oracle (the reference step restated in C++/OpenMP, FP64) on
+    the benched lattice, in this process: `warmup` steps of the reference
+    driver loop (forcing factor, step, mass correction), then `steps` timed
+    ones, host wall clock, all host threads. This process must not have
+    loaded the engine library (the lattice comes from a child process)."""
+    from oracle import oracle_py
     from oracle.oracle_py import Oracle
-    solid, por, p, h, g = workload(100, seed=99)
+    solid, por, p, h, g = workload_without_engine(size, seed)
+    cores = host_threads()
+    oracle_py.set_threads(cores)
     o = Oracle(p, solid)
     o.upload_state(h, g)
+    del h, g
     o.record_target_mass()
-    o.run(1, 0)
-    steps, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
-        o.run(1, steps + 1)
-        steps += 1
+    o.run(warmup, 0)
+    t0 = time.perf_counter()
+    o.run(steps, warmup)
     dt = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": o.n * steps / dt / 1e6, "unit": "MLUPS", "cores": cores, "kind": "port",
-            "sample": f"CPU oracle (FP64, OpenMP) on a 100^3 GRF sample of the same construction "
-                      f"({o.n} sites), {steps} steps in {dt:.1f} s"}
+    return {"mlups": o.n * steps / dt / 1e6, "seconds": dt, "sites": int(o.n), "cores": oracle_py.threads(),
+            "porosity": por, "warmup": warmup, "steps": steps}
+
+
+def cpu_sample_mlups(size: int, seed: int, warmup: int = 2, steps: int = 8):
+    """The reference arm, run as a child process on a bounded sample of the
+    same job (a few steps of the same lattice), so that this leg and
+    `--impl reference` time the same code in the same kind of process."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--size", str(size), "--seed",
+           str(seed), "--steps", str(steps), "--warmup", str(warmup)]
+    r = subprocess.run(cmd, check=True, capture_output=True, text=True)
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    cb = dict(line["cpu_baseline"])
+    cb["sample"] = (f"the reference arm (--impl reference) as a child process: {steps} timed steps after "
+                    f"{warmup} warm-up steps of the benched lattice; " + cb["sample"])
+    return cb
 
 
 def sweep_specs(count: int, steps: int, seed: int = 7):
@@ -357,32 +479,173 @@ def serve_legs(args):
 
 
 def run_reference_arm(args, ws, rank):
+    """The reference's CPU path on this box's host cores, on the benched
+    lattice itself (same size, seed, parameters and initial state). Under
+    torchrun only rank 0 runs it."""
     if rank != 0:
         return 0
-    from oracle.oracle_py import Oracle
-    solid, por, p, h, g = workload(100, seed=99)
-    o = Oracle(p, solid)
-    o.upload_state(h, g)
-    o.record_target_mass()
-    o.run(max(args.warmup, 1), 0)
-    t0 = time.perf_counter()
-    o.run(args.steps, args.warmup)
-    dt = time.perf_counter() - t0
-    v = o.n * args.steps / dt / 1e6
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    r = oracle_timing(args.size, args.seed, max(args.warmup, 1), args.steps)
+    v = r["mlups"]
     line = {"metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "GRF porous sample 100^3 (same construction as the 300^3 workload), "
-                                   "fused MRT, correct_op_mass", "sites": int(o.n)},
-            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": cores, "kind": "port",
-                             "sample": f"CPU oracle (C++/OpenMP restatement of the reference step) on a 100^3 "
-                                       f"sample ({o.n} sites) per step; the reference's own CPU engine "
-                                       f"(felbm_local) is not in the reference snapshot"},
+            "config": {"workload": f"{args.size}^3 GRF porous (corr 6, porosity 0.37, largest cluster), periodic, "
+                                   f"body force 1e-6, fused MRT, theta 45, correct_op_mass, slab IC "
+                                   f"(the same lattice, seed and parameters as the engine arm)",
+                       "sites": r["sites"], "porosity": r["porosity"], "seed": args.seed},
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": r["cores"], "kind": "port",
+                             "sample": f"CPU oracle (C++/OpenMP restatement of the reference step, FP64; the "
+                                       f"reference's own CPU engine, felbm_local, is not in the reference "
+                                       f"snapshot) on the whole {args.size}^3 lattice ({r['sites']} sites): "
+                                       f"{r['warmup']} warm-up + {r['steps']} timed steps of the driver loop "
+                                       f"(step + mass correction), {r['seconds']:.1f} s, {r['cores']} threads"},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_kernels_leg(solid, p, h0, g0, warmup: int, steps: int, precision: str = "f32"):
+    """The reference's own device kernels (include/felbm_gpu/device_engine.cuh,
+    compiled unmodified for sm_100a into oracle/_ref/) on this GPU, driven in
+    the MultiPhaseGPU::step order on the CPU oracle's neighbour and case
+    tables, on the benched lattice: the same-box GPU baseline. Times the
+    reference driver loop (step + mass correction, whose host read-back of
+    the mass sums blocks every step) and the steps alone, host wall clock
+    around queued work with the device synchronised on both sides."""
+    from oracle.oracle_py import Oracle
+    from oracle.ref_py import RefKernels, available
+    if not available(precision):
+        return {"unavailable": "oracle/_ref not built (the reference sources were absent at build time)"}
+    o = Oracle(p, solid)
+    r = RefKernels(p, o, precision=precision)
+    n = r.n
+    del o
+    try:
+        r.upload_state(h0, g0)
+        r.record_target_mass()
+        lib, hd = r.lib, r._h
+        for _ in range(warmup):
+            lib.ref_step(hd)
+            r.apply_mass_correction()
+        assert lib.ref_sync() == 0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            lib.ref_step(hd)
+            r.apply_mass_correction()
+        assert lib.ref_sync() == 0
+        dt_loop = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            lib.ref_step(hd)
+        assert lib.ref_sync() == 0
+        dt_step = time.perf_counter() - t0
+    finally:
+        r.close()
+    return {"impl": "reference device_engine.cuh kernels, unmodified, sm_100a, all six fast switches on",
+            "precision": precision, "sites": int(n), "steps": steps, "warmup": warmup,
+            "mlups_step_plus_correction": n * steps / dt_loop / 1e6,
+            "ms_per_step_plus_correction": dt_loop * 1e3 / steps,
+            "mlups_step": n * steps / dt_step / 1e6, "ms_per_step": dt_step * 1e3 / steps,
+            "clock": "host wall clock around queued steps, device synchronised on both sides"}
+
+
+def interface_area(solid: np.ndarray, c_sites: np.ndarray) -> int:
+    """Fluid node pairs along x, y, z (periodic) whose c straddles 1/2."""
+    grid = np.full(solid.shape, np.nan)
+    grid[solid == 0] = c_sites
+    s = grid - 0.5
+    n = 0
+    for ax in range(3):
+        if solid.shape[ax] == 1:
+            continue
+        t = np.roll(s, -1, axis=ax)
+        n += int(np.count_nonzero((s * t) < 0))  # NaN pairs compare False
+    return n
+
+
+def precision_run(solid, p, ob, h, g, storage: str, steps: int, tracers: int = 0, dm: float = 1e-2):
+    """One solve in `storage`: fields after `steps`, the mass before and
+    after, and (tracers > 0) the longitudinal dispersion coefficient of
+    `tracers` tracers of diffusivity dm seeded in the fluid, from the growth
+    of the variance of their unwrapped x displacement over the run."""
+    import ctypes as C
+    from felbm_gpu_b200 import MultiPhaseGPU, _capi
+    from felbm_gpu_b200.tracers import Tracers, seed
+    q = _capi.FeParams()
+    C.pointer(q)[0] = p
+    q.storage = _capi.STORAGE[storage]
+    e = MultiPhaseGPU(q, solid)
+    try:
+        if ob is not None:
+            e.set_open_bnd(ob)
+        e.upload_state(h, g)
+        if p.correct_op_mass:
+            e.record_target_mass()
+        m0 = e.get_target_mass() if p.correct_op_mass else None
+        disp = None
+        if tracers:
+            pos, _ = seed(solid, tracers, rng_seed=5)
+            tr = Tracers(e, pos, dm, rng_seed=9)
+            nx = solid.shape[2]
+            x_prev = tr.download()[0][0].copy()
+            dx = np.zeros_like(x_prev)
+            done = 0
+            while done < steps:
+                k = min(10, steps - done)
+                for _ in range(k):
+                    e.run(1)
+                    tr.step()
+                done += k
+                x = tr.download()[0][0]
+                d = x - x_prev
+                d -= nx * np.round(d / nx)  # minimal image: a tracer moves < 1 node a step
+                dx += d
+                x_prev = x.copy()
+            disp = float(np.var(dx) / (2.0 * steps))
+            tr.free()
+        else:
+            e.run(steps)
+        f = e.download()
+        m = e.current_mass() if p.correct_op_mass else None
+        return f, m0, m, disp
+    finally:
+        e.free()
+
+
+def precision_study(size: int = 150, steps: int = 5000, mass_steps: int = 2000):
+    """Every storage type beside FP64 on the precision configuration (open,
+    BGK and MRT, `steps`) and on the production configuration at `size`
+    (periodic, mass correction, tracers, `mass_steps`): max|dc|, max|du|, the
+    relative difference of the interface area, the order-parameter mass
+    drift per 1e4 steps and the tracer dispersion coefficient."""
+    cases = []
+    for mrt in (False, True):
+        solid, p, ob, h, g, por = precision_workload(size, mrt)
+        cases.append((f"open {size}^3 {'MRT' if mrt else 'BGK'}", solid, p, ob, h, g, por, steps, 0))
+    solid, por, p, h, g = workload(size)
+    cases.append((f"periodic {size}^3 MRT, mass correction, 4000 tracers", solid, p, None, h, g, por, mass_steps,
+                  4000))
+    out = []
+    for name, solid, p, ob, h, g, por, nsteps, ntr in cases:
+        ref, m0, m_ref, d_ref = precision_run(solid, p, ob, h, g, "f64", nsteps, ntr)
+        a_ref = interface_area(solid, ref["c"])
+        for st in ("f64", "f32", "f16g", "bf16g", "f16s", "bf16s"):
+            f, m0s, m, disp = (ref, m0, m_ref, d_ref) if st == "f64" else precision_run(solid, p, ob, h, g, st,
+                                                                                         nsteps, ntr)
+            du = np.sqrt((f["ux"] - ref["ux"]) ** 2 + (f["uy"] - ref["uy"]) ** 2 + (f["uz"] - ref["uz"]) ** 2)
+            area = interface_area(solid, f["c"])
+            rec = {"case": name, "storage": st, "steps": nsteps, "sites": int(len(ref["c"])), "porosity": por,
+                   "max_abs_dc": float(np.max(np.abs(f["c"] - ref["c"]))), "max_abs_du": float(np.max(du)),
+                   "max_abs_u_fp64": float(np.max(np.sqrt(ref["ux"] ** 2 + ref["uy"] ** 2 + ref["uz"] ** 2))),
+                   "interface_area": area, "interface_area_rel_diff": (area - a_ref) / a_ref if a_ref else 0.0}
+            if m0s is not None:
+                rec["mass_drift_rel_per_1e4_steps"] = abs(m - m0s) / abs(m0s) * 1e4 / nsteps
+            if disp is not None:
+                rec["dispersion_coeff"] = disp
+                rec["dispersion_rel_diff"] = (disp - d_ref) / d_ref
+            out.append(rec)
+    return out
 
 
 def reduce_ranks(dist, ms: float, n: int, device: str):
@@ -400,6 +663,9 @@ def reduce_ranks(dist, ms: float, n: int, device: str):
 
 def main():
     args = parse()
+    if args.emit_workload:
+        emit_workload(args.emit_workload, args.size, args.seed)
+        return 0
     ws, rank, lrank = dist_env()
     if args.impl == "reference":
         return run_reference_arm(args, ws, rank)
@@ -412,7 +678,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from felbm_gpu_b200 import MultiPhaseGPU
     from felbm_gpu_b200 import _capi
-    solid, por, p, h0, g0 = workload(args.size, seed=2024 + rank)
+    solid, por, p, h0, g0 = workload(args.size, seed=args.seed + rank)
     p.storage = _capi.STORAGE[args.storage]
     tuned = None
     if args.brick != "auto":
@@ -470,8 +736,9 @@ def main():
         # asynchronous form, flow_stats_launch / _collect: step t's are
         # collected once step t+1 is queued, so the device does not idle
         # while the host reads them), and the final state comes back
-        # (fe_download_state). Host wall clock around all of it.
-        ke = args.steps
+        # (fe_download_state). Host wall clock around all of it. The job is
+        # --e2e-steps long (the production runs are 20,000 steps), at least K.
+        ke = max(args.steps, args.e2e_steps)
         # the caller's host buffers for the result, as a driver holds them
         hd = np.empty_like(h0)
         gd = np.empty_like(g0)
@@ -535,7 +802,17 @@ def main():
                       "tracer_ms_per_step": dtp * 1e3 / kp - ms / args.steps}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample_mlups(args.storage)
+        cpu = cpu_sample_mlups(args.size, args.seed)
+    ref_kernels = None
+    if rank == 0 and ws == 1 and not args.no_ref_kernels:
+        # the reference's kernels need the lattice's FP32 device memory
+        # beside ours (about 1.5 KB a site): run them with our engine freed
+        eng.free()
+        ref_kernels = reference_kernels_leg(solid, p, h0, g0, warmup=max(args.warmup, 3), steps=max(args.steps, 20))
+    precision = None
+    if rank == 0 and ws == 1 and args.precision_study:
+        eng.free()
+        precision = precision_study(150)
     serving = None
     if ws == 1 and not args.no_serve:
         eng.free()
@@ -552,7 +829,8 @@ def main():
                            "layout": {"brick": brick, "graph_steps": graph_steps,
                                       "autotune": tuned["candidates"] if tuned else None}},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "production": production, "serving": serving}
+                "clocks": clk.summary(), "production": production, "serving": serving,
+                "reference_kernels": ref_kernels, "precision_study": precision}
         print(json.dumps(line), flush=True)
     eng.free()
     if dist:

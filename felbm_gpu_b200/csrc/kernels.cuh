@@ -213,7 +213,7 @@ struct Pro {
   int32_t nbase[64][Sh::W];
   uint16_t slot_of[Sh::C];
   double lambda;
-  float ff;
+  double ff;
 };
 
 // forcing_factor_at (reference felbm_gpu_main.cu:587-594)
@@ -234,7 +234,7 @@ template <class SMem>
 __device__ __forceinline__ void load_step_scalars(const LatDesc& D, SMem& s) {
   {
     const Ctl& C = *D.ctl;
-    s.ff = (float)forcing_factor_dev(D.prm, C);
+    s.ff = forcing_factor_dev(D.prm, C);
     s.lambda = C.lambda;
   }
 }
@@ -330,7 +330,7 @@ template <class Sh>
 struct alignas(16) Head {
   uint16_t slot_of[Sh::C];
   double lambda;
-  float ff;
+  double ff;  // forcing factor in double: narrowed to the arithmetic type where used
   int first, cnt;
 };
 

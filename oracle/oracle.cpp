@@ -11,6 +11,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <omp.h>
 
 namespace {
 
@@ -914,6 +915,11 @@ void or_run(or_engine* e, int nsteps, int64_t t0) {
     or_step(e);
     or_apply_mass_correction(e);
   }
+}
+
+int or_threads(void) { return omp_get_max_threads(); }
+void or_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
 }
 
 void or_mrt_matrices(double* M, double* Minv) {

@@ -61,6 +61,9 @@ int64_t or_inplace_program(const or_engine* e, int32_t* a, int32_t* b, uint8_t* 
 /* fe_run equivalent: nsteps x (forcing factor of step t, step, mass correction) */
 void or_run(or_engine* e, int nsteps, int64_t t0);
 void or_mrt_matrices(double* M, double* Minv);
+/* OpenMP threads the oracle's loops use (omp_get_max_threads / omp_set_num_threads) */
+int or_threads(void);
+void or_set_threads(int n);
 
 #ifdef __cplusplus
 }

@@ -2,19 +2,38 @@
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg to
 compare against; the product never imports it. The struct layouts are the C-ABI's
-(include/felbm_b200.h), taken from felbm_gpu_b200._capi.
+(include/felbm_b200.h), taken from felbm_gpu_b200/_abi.py, which loads no
+library: a process that only runs the oracle never loads the engine.
 """
 from __future__ import annotations
 
 import ctypes as C
+import importlib.util
 import os
 import subprocess
+import sys
 
 import numpy as np
 
-from felbm_gpu_b200 import _capi as capi
-
 _HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _abi():
+    """felbm_gpu_b200._abi without importing the package (whose import loads
+    the engine library); registered under its package name, so a later
+    import of the package shares the same structure types."""
+    name = "felbm_gpu_b200._abi"
+    if name not in sys.modules:
+        path = os.path.join(os.path.dirname(_HERE), "felbm_gpu_b200", "_abi.py")
+        spec = importlib.util.spec_from_file_location(name, path)
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+capi = _abi()
+
 LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
 
@@ -49,6 +68,8 @@ _sig = {
     "or_table": (None, [_vp, C.c_int, C.POINTER(C.c_int32)]),
     "or_run": (None, [_vp, C.c_int, C.c_int64]),
     "or_mrt_matrices": (None, [_dp, _dp]),
+    "or_threads": (C.c_int, []),
+    "or_set_threads": (None, [C.c_int]),
     "or_inplace_program": (C.c_int64, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
 }
 for _n, (_r, _a) in _sig.items():
@@ -162,6 +183,14 @@ class Oracle:
         out = np.empty(self.n, np.int64)
         _lib.or_site_nodes(self._h, out.ctypes.data_as(_i64p))
         return out
+
+
+def threads() -> int:
+    return _lib.or_threads()
+
+
+def set_threads(n: int):
+    _lib.or_set_threads(int(n))
 
 
 def mrt_matrices():

@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-from felbm_gpu_b200 import _capi as capi
+from .oracle_py import capi  # the C-ABI's layouts, without the engine library
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(_HERE, "_ref")

@@ -77,6 +77,19 @@ def make_case(name: str, **over) -> Case:
         p = default_params(**kw)
         h, g = _ic(solid, p, "slab", 4.0, origin=(0, 0, 0), axis=0, thickness=10)
         return Case(name, solid, p, h, g, correct_mass=True)
+    if name == "fluid_mrt":           # all-fluid MRT: the droplet of fluid_bgk, MRT with the reference rates
+        solid = np.zeros((12, 12, 12), np.uint8)
+        kw = dict(rho0=5.0, rho1=1.0, surface_tension=0.01, interface_width=4.0, use_halfway_bb=0, use_mrt=1)
+        kw.update(over)
+        p = default_params(**kw)
+        h, g = _ic(solid, p, "droplet", 4.0, centre=(6, 6, 6), radius=3.0)
+        return Case(name, solid, p, h, g)
+    if name == "c1_cyl2d":            # the plain-method configuration, 200 x 200 x 1
+        return c1_case(**over)
+    if name in ("c2_open_bgk", "c2_open_mrt"):  # the precision configuration, 150^3 open
+        return c2_case(mrt=name.endswith("mrt"), **over)
+    if name == "c3_grf300":           # the production configuration, 300^3 periodic
+        return c3_case(**over)
     if name.startswith("openbnd"):    # compare_cpu_gpu geom=openbnd: duct, pressure inlet/outlet
         mode = int(over.pop("inlet_mode", 0))
         copybuf = bool(over.pop("copy_to_buffers", name.endswith("_buf")))
@@ -102,5 +115,31 @@ def make_case(name: str, **over) -> Case:
     raise KeyError(name)
 
 
-CASES = ["fluid_bgk", "spheres_bgk", "spheres_mrt", "spheres_mrt_wet", "cyl2d_mrt", "grf_mrt_mass",
+CASES = ["fluid_bgk", "fluid_mrt", "spheres_bgk", "spheres_mrt", "spheres_mrt_wet", "cyl2d_mrt", "grf_mrt_mass",
          "grf_bgk_mass", "openbnd_bgk", "openbnd_mrt_buf"]
+
+# inlet injection schedules of the open-boundary cases (the `inlet_mode`
+# override): 1 alternate, 2 split, 4 stripes (reference d_inlet_gate,
+# include/felbm_gpu/device_engine.cuh:699-728, modes 1, 2, 3)
+INLET_MODES = {"alternate": 1, "split": 2, "stripes": 4}
+
+
+def c1_case(size: int = 200, seed: int = 12345, **over) -> Case:
+    """The plain-method configuration (bench.plain_workload), 200 x 200 x 1."""
+    import bench
+    solid, p, h, g = bench.plain_workload(size, seed, **over)
+    return Case("c1_cyl2d", solid, p, h, g)
+
+
+def c2_case(mrt: bool, size: int = 150, seed: int = 7, **over) -> Case:
+    """The precision configuration (bench.precision_workload), 150^3 open."""
+    import bench
+    solid, p, ob, h, g, _ = bench.precision_workload(size, mrt, seed, **over)
+    return Case("c2_open_mrt" if mrt else "c2_open_bgk", solid, p, h, g, open_bnd=ob)
+
+
+def c3_case(size: int = 300, seed: int = 2024, **over) -> Case:
+    """The production configuration, the benched lattice itself (bench.workload)."""
+    import bench
+    solid, _, p, h, g = bench.workload(size, seed, **over)
+    return Case("c3_grf300", solid, p, h, g, correct_mass=True)

@@ -199,3 +199,30 @@ def test_two_rate_form_equals_general_transform(require_gpu, storage, monkeypatc
         b.free()
         for e in engines.values():
             e.free()
+
+
+def test_batch_members_match_oracle(require_gpu):
+    """Members of a mixed batch (porous MRT with mass correction, the 2-D
+    cylinder pack on the general MRT transform, the open duct, wetting walls)
+    against the FP64 oracle directly, 100 steps, at the FP64 parity bound."""
+    from parity import maxdiff, run_oracle
+    names = ["grf_mrt_mass", "cyl2d_mrt", "openbnd_bgk", "spheres_mrt_wet"]
+    b = Batch()
+    engines = {n: make_engine(n, "f64") for n in names}
+    try:
+        for e in engines.values():
+            b.add(e)
+        b.run(60)
+        b.run(40)
+        for n, e in engines.items():
+            h, g = e.download_state()
+            f = e.download()
+            ho, go, fo, _ = run_oracle(make_case(n), 100)
+            assert maxdiff(h, ho) <= 1e-12, (n, maxdiff(h, ho))
+            assert maxdiff(g, go) <= 1e-12, (n, maxdiff(g, go))
+            for k in ("c", "rho", "ux", "uy", "uz", "p", "mu"):
+                assert maxdiff(f[k], fo[k]) <= 1e-12, (n, k, maxdiff(f[k], fo[k]))
+    finally:
+        b.free()
+        for e in engines.values():
+            e.free()

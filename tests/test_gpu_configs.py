@@ -1,0 +1,138 @@
+"""B200 engine against the FP64 oracle on the measured configurations and on
+the driver paths the small parity cases do not reach: the time-dependent
+forcing factor (reference src/felbm_gpu_main.cu:587-594,743), the inlet
+injection schedules (include/felbm_gpu/device_engine.cuh:699-728), the
+plain-method, precision and production configurations themselves.
+
+Tolerances (stated contract): FP64 storage max|dh|, max|dg| and the fields
+c, rho, u, p, mu <= 1e-12 after 100 steps; FP32 storage max|d| / max|ref|
+<= 1e-6 on h and g and max|dc| <= 1e-5 after 20 steps.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from cases import INLET_MODES, make_case
+from felbm_gpu_b200 import MultiPhaseGPU
+from oracle.oracle_py import Oracle
+from parity import maxdiff, reldiff, run_engine, run_oracle, with_storage
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+FIELDS = ("c", "rho", "ux", "uy", "uz", "p", "mu")
+TIMEDEP = {"sinusoidal": 1, "square": 2}
+
+
+def assert_fp64(h, g, f, ho, go, fo, tag=""):
+    assert maxdiff(h, ho) <= TOL64, (tag, "h", maxdiff(h, ho))
+    assert maxdiff(g, go) <= TOL64, (tag, "g", maxdiff(g, go))
+    for k in FIELDS:
+        assert maxdiff(f[k], fo[k]) <= TOL64, (tag, k, maxdiff(f[k], fo[k]))
+
+
+def forcing_factor_at(timedep: int, period: float, t: int) -> float:
+    """The reference driver's forcing_factor_at (felbm_gpu_main.cu:589-593)."""
+    if timedep == 1:
+        return math.sin(2.0 * math.pi * t / period)
+    if timedep == 2:
+        x = math.sin(2.0 * math.pi * t / period)
+        return -1.0 if x < 0 else (1.0 if x > 0 else 0.0)
+    return 1.0
+
+
+# -- (i) forcing vector and its time dependence ----------------------------
+@pytest.mark.parametrize("timedep", sorted(TIMEDEP))
+@pytest.mark.parametrize("name", ["spheres_mrt_wet", "grf_bgk_mass"])
+def test_forcing_timedep_run(require_gpu, name, timedep):
+    """fe_run takes the forcing factor of step t from the step counter
+    (sin(2 pi t / period), or its sign), times the forcing vector f, in
+    double; the oracle runs the reference driver's loop. The force is large
+    enough (|f| = 2e-4) that a factor rounded to FP32 would show above 1e-12."""
+    case = make_case(name, fx=2e-4, fy=-1e-4, fz=5e-5, forcing_timedep=TIMEDEP[timedep], forcing_period=30.0)
+    h, g, f, _, _ = run_engine(case, 100, "f64")
+    ho, go, fo, _ = run_oracle(case, 100)
+    assert_fp64(h, g, f, ho, go, fo, (name, timedep))
+    # the force changed the flow: a run without it differs by far more than the tolerance
+    case0 = make_case(name)
+    h0, _, _, _, _ = run_engine(case0, 100, "f64")
+    assert maxdiff(h0, h) > 1e-8
+
+
+@pytest.mark.parametrize("name", ["grf_mrt_mass", "cyl2d_mrt"])
+def test_forcing_factor_step_loop(require_gpu, name):
+    """The reference driver loop (felbm_gpu_main.cu:741-745) through the
+    public calls: fe_set_forcing_factor, fe_step, fe_apply_mass_correction
+    per step; factor 0.3 for 50 steps, then the sinusoidal factor of t."""
+    case = make_case(name, fx=2e-4, fy=1e-4, forcing_period=40.0)
+    factors = [0.3 if t < 50 else forcing_factor_at(1, 40.0, t) for t in range(100)]
+    e = MultiPhaseGPU(with_storage(case.params, "f64"), case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        if case.correct_mass:
+            e.record_target_mass()
+        for ff in factors:
+            e.set_forcing_factor(ff)
+            e.step(1)
+            e.apply_mass_correction(want_drift=False)
+        h, g = e.download_state()
+        f = e.download()
+    finally:
+        e.free()
+    o = Oracle(case.params, case.solid)
+    o.upload_state(case.h0, case.g0)
+    if case.correct_mass:
+        o.record_target_mass()
+    for ff in factors:
+        o.set_forcing_factor(ff)
+        o.step(1)
+        o.apply_mass_correction()
+    ho, go = o.download_state()
+    fo = o.download()
+    assert_fp64(h, g, f, ho, go, fo, name)
+
+
+# -- (ii) inlet injection schedules through the engine ----------------------
+@pytest.mark.parametrize("mode", sorted(INLET_MODES))
+@pytest.mark.parametrize("name", ["openbnd_bgk", "openbnd_mrt_buf"])
+def test_inlet_modes_fp64_100_steps(require_gpu, name, mode):
+    """Alternate (time-periodic gate with a tanh ramp), split (tanh across
+    the split axis) and stripes (periodic in the inlet coordinate) injection
+    of the inlet fluid, engine against the oracle."""
+    case = make_case(name, inlet_mode=INLET_MODES[mode])
+    h, g, f, _, _ = run_engine(case, 100, "f64")
+    ho, go, fo, _ = run_oracle(case, 100)
+    assert_fp64(h, g, f, ho, go, fo, (name, mode))
+
+
+# -- (iv) plain-method configuration, 200 x 200 x 1 --------------------------
+def test_c1_fp64_100_steps(require_gpu):
+    case = make_case("c1_cyl2d")
+    assert 25000 < case.h0.size // 19 < 27000
+    h, g, f, _, _ = run_engine(case, 100, "f64")
+    ho, go, fo, _ = run_oracle(case, 100)
+    assert_fp64(h, g, f, ho, go, fo, "c1")
+
+
+# -- (v) precision configuration, 150^3 open inlet/outlet --------------------
+@pytest.mark.parametrize("name", ["c2_open_bgk", "c2_open_mrt"])
+def test_c2_fp64_100_steps(require_gpu, name):
+    case = make_case(name)
+    assert case.h0.size // 19 > 1_000_000
+    h, g, f, _, _ = run_engine(case, 100, "f64")
+    ho, go, fo, _ = run_oracle(case, 100)
+    assert_fp64(h, g, f, ho, go, fo, name)
+
+
+# -- (vi) production configuration, 300^3, FP32 ------------------------------
+def test_c3_fp32_20_steps(require_gpu):
+    """The benched lattice itself (9,984,164 sites) in the benched storage."""
+    case = make_case("c3_grf300")
+    h, g, f, _, _ = run_engine(case, 20, "f32")
+    ho, go, fo, _ = run_oracle(case, 20)
+    assert case.h0.size // 19 == 9_984_164
+    assert reldiff(h, ho) <= 1e-6, reldiff(h, ho)
+    assert reldiff(g, go) <= 1e-6, reldiff(g, go)
+    assert maxdiff(f["c"], fo["c"]) <= 1e-5, maxdiff(f["c"], fo["c"])
+    assert maxdiff(f["rho"], fo["rho"]) <= 1e-5

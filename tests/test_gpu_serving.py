@@ -139,3 +139,34 @@ def test_stats_and_idle(require_gpu):
     assert st["site_steps"] >= sites
     assert st["mlups_busy"] > 0 and st["ttr_p99"] >= st["ttr_p50"] > 0
     assert len(res) == 2
+
+
+def test_served_solves_match_oracle(require_gpu):
+    """Served FP64 solves, admitted while others run, against the FP64 oracle
+    directly (the state the server builds from the slab description, then
+    the reference driver loop with mass correction): fields within 1e-12."""
+    from oracle.oracle_py import Oracle
+    specs = [solve_spec(k) for k in (0, 1, 5)]
+    srv = Server(storage="f64", max_active=2, chunk_steps=16)
+    try:
+        for k, (p, solid, init, W, steps) in enumerate(specs):
+            srv.submit(k, p, solid, steps, init=init, init_width=W)
+        res = collect(srv, len(specs))
+    finally:
+        srv.close()
+    assert len(res) == len(specs)
+    for r in res:
+        assert r.status == 0, r.message
+        p, solid, init, W, steps = specs[r.id]
+        kind, a = init
+        c = geometry.order_parameter(solid, "slab", W, origin=a[:3], axis=int(a[3]), thickness=a[4])
+        h0, g0 = geometry.equilibrium(c, 1.0, p.rho0, p.rho1)
+        o = Oracle(p, solid)
+        o.upload_state(h0, g0)
+        o.record_target_mass()
+        o.run(steps, 0)
+        fo = o.download()
+        for k in ("c", "rho", "ux", "uy", "uz", "p"):
+            d = float(np.max(np.abs(r.fields[k] - fo[k])))
+            assert d <= 1e-12, (r.id, k, d)
+        assert abs(r.mass_final - o.current_mass()) <= 1e-12 * abs(r.mass_final)
