@@ -65,6 +65,30 @@ class FeTuneReport(C.Structure):
                 ("cand_graph_steps", C.c_int * 8), ("cand_mlups", C.c_double * 8)]
 
 
+class FeDriverCfg(C.Structure):
+    _fields_ = [("model", C.c_char * 32),
+                ("output_dir", C.c_char * 256), ("output_name", C.c_char * 128),
+                ("timeseries_file", C.c_char * 128), ("log_file", C.c_char * 128),
+                ("param_file", C.c_char * 256), ("velocity_set", C.c_char * 16),
+                ("domain_geometry", C.c_char * 64), ("domain_cfg_file", C.c_char * 256),
+                ("fluid_initializer", C.c_char * 64), ("fluid_init_filename", C.c_char * 256),
+                ("restart_file", C.c_char * 256),
+                ("size_x", C.c_int), ("size_y", C.c_int), ("size_z", C.c_int),
+                ("max_iterations", C.c_int64),
+                ("log_skip", C.c_int), ("file_skip", C.c_int),
+                ("checkpoint_skip", C.c_uint32), ("output_deflate", C.c_int), ("output_float32", C.c_int),
+                ("gpu_device", C.c_int), ("logging", C.c_int), ("console", C.c_int),
+                ("use_open_bnd", C.c_int), ("in_out_dir", C.c_int), ("buffer_layers", C.c_int),
+                ("empty_layers", C.c_int), ("extrude_buffers", C.c_int),
+                ("image_periodic", C.c_int), ("transverse_periodic", C.c_int),
+                ("particles_enable", C.c_int), ("particles_number", C.c_int64),
+                ("particles_init_mode", C.c_char * 32), ("particles_plane_offsets", C.c_char * 256),
+                ("particles_dm_groups", C.c_char * 512),
+                ("particles_int_order", C.c_int), ("particles_substeps", C.c_int), ("particles_file_skip", C.c_int),
+                ("particles_dt", C.c_double),
+                ("unknown_keys", C.c_int)]
+
+
 BRICK = {"auto": 0, "8x8x8": 1, "16x16x1": 2, "8x8x4": 3, "16x8x8": 4}
 
 

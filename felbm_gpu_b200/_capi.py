@@ -1,8 +1,9 @@
 """ctypes binding of the C-ABI in include/felbm_b200.h.
 
 Loads felbm_gpu_b200/_lib/libfelbm_b200.so (built in-tree by
-``make -C felbm_gpu_b200`` or ``__graft_entry__.build()``). There is no
-fallback: if the library is missing, importing this module raises.
+``make -C felbm_gpu_b200`` or ``__graft_entry__.build()``), or the build named
+by the environment variable FELBM_B200_LIB. There is no fallback: if the
+library is missing, importing this module raises.
 """
 from __future__ import annotations
 
@@ -12,7 +13,7 @@ import os
 from ._abi import *  # noqa: F401,F403  (structure layouts and constants)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libfelbm_b200.so")
+LIB_PATH = os.environ.get("FELBM_B200_LIB") or os.path.join(_HERE, "_lib", "libfelbm_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
@@ -31,6 +32,9 @@ _fp = C.POINTER(C.c_float)
 SIGNATURES = {
     "fe_params_default": (C.c_int, [C.POINTER(FeParams)]),
     "fe_params_derive": (C.c_int, [C.POINTER(FeParams)]),
+    "fe_driver_cfg_default": (C.c_int, [C.POINTER(FeDriverCfg)]),
+    "fe_cfg_read": (C.c_int, [C.c_char_p, C.POINTER(FeParams), C.POINTER(FeOpenBnd), C.POINTER(FeDriverCfg)]),
+    "fe_cfg_switch_log": (C.c_int, [C.POINTER(FeParams), C.c_char_p, C.c_int]),
     "fe_engine_create": (C.c_int, [C.POINTER(FeParams), C.c_int, C.c_int, C.c_int, _u8p, C.c_int, C.POINTER(_vp)]),
     "fe_engine_destroy": (C.c_int, [_vp]),
     "fe_engine_size": (C.c_int, [_vp, _i64p, _i64p]),

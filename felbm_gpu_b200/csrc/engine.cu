@@ -295,6 +295,7 @@ struct Engine {
   size_t smem_p4 = 0;
   bool open_bnd = false;
   double ff_manual = 1.0;
+  int step_mode = 0;          // control mode of the last stepping call (0 fe_step, 1 fe_run)
   int ctl_mode = 0;           // run mode and forcing factor last written to
   double ctl_ff = 1.0;        // the control block (its initial values)
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
@@ -498,6 +499,7 @@ struct Engine {
     if ((rc = alloc(&d_ctl, 1))) return rc;
     Ctl c0{};
     c0.ff_manual = 1.0;
+    c0.ff_last = 1.0;
     FE_CUDA(cudaMemcpy(d_ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice));
     D.ctl = d_ctl;
     fill_prm();
@@ -541,7 +543,7 @@ struct Engine {
   // Dynamic shared memory of the collide pass (CollideSmem).
   template <class S, class Sh>
   int set_attrs() {
-    smem_p4 = CollideSmem<Sh, typename S::real>::BYTES;
+    smem_p4 = CollideSmem<S, Sh>::BYTES;
     FE_CUDA((collide_smem_attr<S, Sh>((int)smem_p4)));
     return FE_OK;
   }
@@ -585,11 +587,14 @@ struct Engine {
     return k;
   }
 
+  // run_mode 1: fe_run (corrections queued after each step, forcing factor
+  // from the step counter); 0: fe_step (factor ff); 2: a field refresh
+  // without a step (no correction queued, the last step's factor)
   int set_ctl_mode(int run_mode, double ff) {
-    run_mode = run_mode ? 1 : 0;
+    if (run_mode != 2) step_mode = run_mode;
     if (run_mode == ctl_mode && ff == ctl_ff) return FE_OK;  // already on the device
     // auto_correct, ff_auto, ff_manual are contiguous in Ctl
-    struct { int32_t auto_correct, ff_auto; double ff_manual; } m{run_mode, run_mode, ff};
+    struct { int32_t auto_correct, ff_auto; double ff_manual; } m{run_mode == 1 ? 1 : 0, run_mode, ff};
     static_assert(offsetof(Ctl, ff_auto) == offsetof(Ctl, auto_correct) + 4, "Ctl layout");
     static_assert(offsetof(Ctl, ff_manual) == offsetof(Ctl, auto_correct) + 8, "Ctl layout");
     FE_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(d_ctl) + offsetof(Ctl, auto_correct), &m, sizeof(m),
@@ -821,9 +826,11 @@ struct Engine {
   }
   // Corrected velocity of the current state into node-indexed device grids
   // (solid nodes are left as they are), on the engine stream.
+  // The forcing factor is the one the next step takes (the mode of the last
+  // stepping call), as in the velocity the next step's field pass forms.
   int velocity_grid(double* ux, double* uy, double* uz, double* c = nullptr) {
     int rc;
-    if ((rc = set_ctl_mode(0, ff_manual))) return rc;
+    if ((rc = set_ctl_mode(step_mode, ff_manual))) return rc;
     FieldOut o{nullptr, c, ux, uy, uz, nullptr, nullptr};
     FE_DISPATCH(*this, (fields_launch<S FE_COMMA Sh FE_COMMA 2>(o)));
     FE_CUDA(cudaGetLastError());
@@ -835,8 +842,9 @@ struct Engine {
     int rc;
     if ((rc = ensure_tmp(7 * n))) return rc;
     // the moment pass forms the lambda of a queued correction (the pending flag
-    // stays set: no collision runs, so the correction is still owed)
-    if ((rc = set_ctl_mode(0, ff_manual))) return rc;
+    // stays set: no collision runs, so the correction is still owed); the
+    // forcing factor is the last step's
+    if ((rc = set_ctl_mode(2, ff_manual))) return rc;
     FieldOut o{d_tmp + 0 * n, d_tmp + 1 * n, d_tmp + 2 * n, d_tmp + 3 * n, d_tmp + 4 * n, d_tmp + 5 * n,
                d_tmp + 6 * n};
     FE_DISPATCH(*this, (fields_launch<S FE_COMMA Sh FE_COMMA 1>(o)));
@@ -1068,7 +1076,7 @@ struct Batch {
   }
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {
-    const size_t sm = CollideSmem<Sh, typename S::real>::BYTES;
+    const size_t sm = CollideSmem<S, Sh>::BYTES;
     launch_collide<S, Sh>(g.mrt, g.hbb != 0, g.wide != 0, g.nwork, sm, st, d_desc, g.d_work, par);
   }
   template <class S>

@@ -216,8 +216,11 @@ struct Pro {
   double ff;
 };
 
-// forcing_factor_at (reference felbm_gpu_main.cu:587-594)
+// forcing_factor_at (reference felbm_gpu_main.cu:587-594); a field refresh
+// without a step (ff_auto == 2) takes the factor of the last step, as the
+// reference's download_raw reads the DevParams value the driver set last.
 __device__ __forceinline__ double forcing_factor_dev(const DevPrm& P, const Ctl& C) {
+  if (C.ff_auto == 2) return C.ff_last;
   if (!C.ff_auto) return C.ff_manual;
   const double PI = 3.14159265358979323846;
   if (P.forcing_timedep == 1) return sin(2.0 * PI * double(C.t) / P.forcing_period);

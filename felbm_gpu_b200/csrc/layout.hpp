@@ -46,7 +46,7 @@ struct Ctl {
   int32_t open_step;     // number of open-boundary applications so far
   int32_t pending;       // 1: a mass correction is queued for the next pass
   int32_t auto_correct;  // 1: queue a correction after each step (fe_run)
-  int32_t ff_auto;       // 1: forcing factor from t; 0: ff_manual
+  int32_t ff_auto;       // 1: forcing factor from t; 0: ff_manual; 2: ff_last
   double ff_manual;
   double target_mass;    // M0
   double M, W;           // sums of the last moment pass
@@ -59,6 +59,7 @@ struct Ctl {
   double stats[6];       // flow statistics of the last finalize
   int32_t status;        // nonzero: a kernel detected a problem
   int32_t pad_;
+  double ff_last;        // forcing factor of the last collision pass (field refreshes use it)
 };
 
 // Physics parameters of one lattice, in double (each kernel converts to its

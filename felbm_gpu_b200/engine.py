@@ -50,6 +50,36 @@ def default_params(**kw) -> capi.FeParams:
     return p
 
 
+def read_cfg(settings_path: str, params: capi.FeParams | None = None):
+    """Read the reference driver's settings.cfg and the params.cfg it names
+    (fe_cfg_read). Returns (params, open-boundary flags and values as an
+    OpenBoundary without node lists, driver-level keys as a dict, the
+    fast-path switch mapping as text)."""
+    p = capi.FeParams()
+    if params is None:
+        check(lib.fe_params_default(C.byref(p)))
+    else:
+        C.pointer(p)[0] = params
+    b = capi.FeOpenBnd()
+    d = capi.FeDriverCfg()
+    check(lib.fe_cfg_read(str(settings_path).encode(), C.byref(p), C.byref(b), C.byref(d)))
+    drv = {}
+    for k, _ in capi.FeDriverCfg._fields_:
+        v = getattr(d, k)
+        drv[k] = v.decode() if isinstance(v, bytes) else v
+    ob = OpenBoundary(inlet=np.zeros(0, np.int32), outlet=np.zeros(0, np.int32),
+                      copy_to_buffers=bool(b.copy_to_buffers), use_in_vel=bool(b.use_in_vel),
+                      use_in_prs=bool(b.use_in_prs), use_in_fluid=bool(b.use_in_fluid),
+                      use_out_prs=bool(b.use_out_prs), use_out_fluid=bool(b.use_out_fluid),
+                      u_in=(b.u_in_x, b.u_in_y, b.u_in_z), p_in=b.p_in, p_out=b.p_out, c_out_fixed=b.c_out_fixed,
+                      rho_out_fixed=b.rho_out_fixed, inlet_c_a=b.inlet_c_a, inlet_mode=b.inlet_mode,
+                      split_axis=b.split_axis, inlet_period=b.inlet_period, inlet_duty=b.inlet_duty,
+                      inlet_ramp=b.inlet_ramp, split_pos=b.split_pos)
+    buf = C.create_string_buffer(4096)
+    check(lib.fe_cfg_switch_log(C.byref(p), buf, len(buf)))
+    return p, ob, drv, buf.value.decode()
+
+
 def autotune(params, solid: np.ndarray, steps: int = 20, device: int = 0) -> dict:
     """Time the brick shapes and graph lengths this lattice can use and record
     the fastest for its size class (fe_autotune); engines created afterwards

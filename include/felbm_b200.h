@@ -136,6 +136,54 @@ typedef struct fe_open_bnd {
   double inlet_period, inlet_duty, inlet_ramp, split_pos;
 } fe_open_bnd;
 
+/* ---- configuration files ------------------------------------------------
+ * The reference driver's settings.cfg (and the params.cfg its `param_file`
+ * names, relative to the settings file), read as felbm_gpu reads them
+ * (src/felbm_gpu_main.cu:190-235 and the Settings keys it uses through
+ * felbm_local's util::ConfigFile): `key = value`, `#` comments, quoted
+ * strings, booleans true/false. The driver-level keys land here; the
+ * physics and solver keys in fe_params (its fields carry the key names:
+ * acceleration_* -> gx..gz, forcing_* -> fx..fz, the six fast-path switches,
+ * use_mrt, mrt_lambda, use_halfway_bb, correct_op_mass; rho0 .. phi from
+ * params.cfg); the open-boundary flags and values in fe_open_bnd (its node
+ * lists come from the geometry, fe_geom_open_lists). */
+typedef struct fe_driver_cfg {
+  char model[32];
+  char output_dir[256], output_name[128], timeseries_file[128], log_file[128];
+  char param_file[256], velocity_set[16];
+  char domain_geometry[64], domain_cfg_file[256];
+  char fluid_initializer[64], fluid_init_filename[256];
+  char restart_file[256];        /* [gpu] resume from this checkpoint ("" none) */
+  int size_x, size_y, size_z;
+  int64_t max_iterations;
+  int log_skip, file_skip;
+  uint32_t checkpoint_skip;      /* [gpu] checkpoint every N steps (0 never)   */
+  int output_deflate;            /* [gpu] gzip level 0-9 of field files        */
+  int output_float32;            /* [gpu] float32 instead of float64 fields    */
+  int gpu_device;                /* [gpu] -1: leave the device as it is        */
+  int logging, console;
+  int use_open_bnd, in_out_dir, buffer_layers, empty_layers, extrude_buffers;
+  int image_periodic, transverse_periodic;
+  int particles_enable;
+  int64_t particles_number;
+  char particles_init_mode[32], particles_plane_offsets[256], particles_dm_groups[512];
+  int particles_int_order, particles_substeps, particles_file_skip;
+  double particles_dt;
+  int unknown_keys;              /* keys of either file this reader ignored    */
+} fe_driver_cfg;
+
+/* Defaults of the driver-level keys. */
+int fe_driver_cfg_default(fe_driver_cfg* d);
+/* Read settings.cfg (+ params.cfg) over the given parameter block (keys
+ * absent from the files keep p's values), then derive kappa, beta, mobility,
+ * bnd_coeff. ob may be NULL. Refuses what the reference driver refuses
+ * (model single_phase; correct_op_mass with open boundaries,
+ * felbm_gpu_main.cu:242-254). */
+int fe_cfg_read(const char* settings_path, fe_params* p, fe_open_bnd* ob, fe_driver_cfg* d);
+/* How each of the six fast-path switches of p maps onto this engine, one
+ * line per key, into buf (NUL-terminated; FE_ERR_ARG if len is too small). */
+int fe_cfg_switch_log(const fe_params* p, char* buf, int len);
+
 /* Macroscopic fields, each n doubles in the reference site order
  * (reference RawFields, multiphase_gpu.cuh:730). Any pointer may be NULL. */
 typedef struct fe_fields {
@@ -218,7 +266,10 @@ int fe_current_mass(fe_engine* e, double* m);
 /* ---- readout ----------------------------------------------------------- */
 /* Replaces download()/download_raw() (multiphase_gpu.cuh:704-757): refresh the
  * macroscopic fields from the current state (moments, open-boundary field
- * enforcement, mu, velocity/pressure correction) and copy them out. */
+ * enforcement, mu, velocity/pressure correction) and copy them out. The
+ * velocity correction takes the forcing factor of the last step (1 before
+ * any step), as the reference's refresh reads the DevParams forcing_factor
+ * the driver set for the last step. */
 int fe_download_fields(fe_engine* e, const fe_fields* f);
 /* Replaces flow_stats (multiphase_gpu.cuh:645-651): out = {sum ux, sum uy,
  * sum uz, sum u^2, sum c, max u^2} of the fields of the last step. */

@@ -8,8 +8,12 @@
 //   flow_stats(), flow_stats_launch/pending/ready/collect(), state_size(), free(),
 // plus set_open_bnd() with the reference's argument meaning. Construction takes
 // the solid mask and parameter block instead of felbm_local's SubDomain /
-// Settings / ParametersMultiPhase objects; errors throw fe::Error instead of
-// exiting the process.
+// Settings / ParametersMultiPhase objects (read_cfg() fills the parameter
+// block from the reference's settings.cfg / params.cfg); errors throw
+// fe::Error instead of exiting the process. The reference driver copies the
+// device velocity (d_ux, d_uy, d_uz, d_c) to the host for its tracer worker
+// (felbm_gpu_main.cu:760-763); here the tracers run on the device beside the
+// engine (fe_tracers_*), and download() returns the fields.
 #pragma once
 #include <stdexcept>
 #include <string>
@@ -26,6 +30,18 @@ struct Error : std::runtime_error {
 
 inline void check(int status) {
   if (status != FE_OK) throw Error(status, fe_last_error());
+}
+
+// settings.cfg (+ the params.cfg it names) over p; the six fast-path switches
+// are logged by switch_log()
+inline void read_cfg(const std::string& settings, fe_params& p, fe_open_bnd& ob, fe_driver_cfg& d) {
+  check(fe_cfg_read(settings.c_str(), &p, &ob, &d));
+}
+inline std::string switch_log(const fe_params& p) {
+  std::string buf(4096, '\0');
+  check(fe_cfg_switch_log(&p, &buf[0], (int)buf.size()));
+  buf.resize(std::char_traits<char>::length(buf.c_str()));
+  return buf;
 }
 
 class MultiPhaseGPU {
@@ -93,6 +109,13 @@ class MultiPhaseGPU {
                 std::vector<double>& uy, std::vector<double>& uz, std::vector<double>& p) {
     for (auto* v : {&c, &rho, &ux, &uy, &uz, &p}) v->resize(n_);
     fe_fields f{rho.data(), c.data(), ux.data(), uy.data(), uz.data(), p.data(), nullptr};
+    check(fe_download_fields(e_, &f));
+  }
+  // the same with the chemical potential mu (download_raw's field set + mu)
+  void download(std::vector<double>& c, std::vector<double>& rho, std::vector<double>& ux,
+                std::vector<double>& uy, std::vector<double>& uz, std::vector<double>& p, std::vector<double>& mu) {
+    for (auto* v : {&c, &rho, &ux, &uy, &uz, &p, &mu}) v->resize(n_);
+    fe_fields f{rho.data(), c.data(), ux.data(), uy.data(), uz.data(), p.data(), mu.data()};
     check(fe_download_fields(e_, &f));
   }
   // :645-683
