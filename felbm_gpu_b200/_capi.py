@@ -83,7 +83,7 @@ SIGNATURES = {
     "fe_tracers_set_velocity": (C.c_int, [_vp, _dp, _dp]),
     "fe_tracers_seed": (C.c_int, [_u8p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int64,
                                   C.c_uint64, _dp, _i32p]),
-    "fe_write_fields_h5": (C.c_int, [_vp, C.c_char_p, C.c_int]),
+    "fe_write_fields_h5": (C.c_int, [_vp, C.c_char_p, C.c_int, C.c_int]),
     "fe_write_geometry_h5": (C.c_int, [C.c_char_p, _u8p, C.c_int, C.c_int, C.c_int]),
     "fe_checkpoint_write": (C.c_int, [_vp, C.c_char_p, C.c_uint32]),
     "fe_settle_mass_correction": (C.c_int, [_vp]),
@@ -99,6 +99,7 @@ SIGNATURES = {
     "fe_tune_clear": (C.c_int, []),
     "fe_write_series": (C.c_int, [C.c_char_p, C.c_int, C.c_uint32, _dp, C.c_int64]),
     "fe_write_stretching": (C.c_int, [C.c_char_p, C.c_int, _dp, C.c_int64]),
+    "fe_h5_write_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, _i64p, C.c_void_p, C.c_int]),
     "fe_h5_read_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), _i64p, C.POINTER(C.c_int),
                                      C.c_void_p, C.c_int64]),
     "fe_server_create": (C.c_int, [C.POINTER(FeServerConfig), C.POINTER(C.c_void_p)]),

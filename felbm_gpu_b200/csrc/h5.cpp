@@ -2,6 +2,8 @@
 // version 0, version-1 object headers, symbol-table group). See h5.hpp.
 #include "h5.hpp"
 
+#include <zlib.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -17,6 +19,8 @@ constexpr uint64_t UNDEF = ~0ull;     // undefined address
 constexpr int LEAF_K = 8;             // symbol-table node: 2K = 16 entries
 constexpr int INTERNAL_K = 16;        // group B-tree node: 2K = 32 children
 constexpr uint64_t HEAP_FREE_NONE = 1;  // "no free block" in a local heap (offsets are 8-aligned)
+constexpr int ISTORE_K = 32;          // chunk B-tree node: 2K = 64 children (superblock 0 default)
+constexpr unsigned FILTER_DEFLATE = 1;
 
 uint64_t pad8(uint64_t x) { return (x + 7) & ~7ull; }
 size_t elem_size(Type t) { return t == F64 ? 8 : 4; }
@@ -116,15 +120,28 @@ int write(const std::string& path, const std::vector<Dataset>& sets_in) {
   const uint64_t btree_size = 24 + (2 * INTERNAL_K + 1) * 8 + 2 * INTERNAL_K * 8;
   const uint64_t snod = btree + btree_size;
   const uint64_t snod_size = 8 + 2 * LEAF_K * 40;
-  // dataset object headers, then the data
+  // dataset object headers, then the data (chunked datasets: the chunk
+  // B-tree node, then the compressed chunk)
   std::vector<std::vector<Msg>> hdrs(sets.size());
-  std::vector<uint64_t> hdr_at(sets.size()), data_at(sets.size()), data_len(sets.size());
+  std::vector<uint64_t> hdr_at(sets.size()), data_at(sets.size()), data_len(sets.size()), bt_at(sets.size(), 0);
+  std::vector<std::vector<unsigned char>> packed(sets.size());
   uint64_t p = snod + snod_size;
   for (size_t q = 0; q < sets.size(); ++q) {
     const Dataset& d = sets[q];
     uint64_t count = 1;
     for (uint64_t x : d.dims) count *= x;
     data_len[q] = count * elem_size(d.type);
+    if (d.deflate < 0 || d.deflate > 9) return fe_fail(FE_ERR_ARG, "hdf5 writer: deflate level 0-9");
+    const bool chunked = d.deflate > 0 && count > 0;
+    if (chunked) {
+      if (data_len[q] >= (1ull << 32)) return fe_fail(FE_ERR_ARG, "hdf5 writer: a chunk is limited to 4 GB");
+      uLongf clen = compressBound((uLong)data_len[q]);
+      packed[q].resize(clen);
+      if (compress2(packed[q].data(), &clen, static_cast<const Bytef*>(d.data), (uLong)data_len[q], d.deflate) != Z_OK)
+        return fe_fail(FE_ERR_IO, "hdf5 writer: deflate failed");
+      packed[q].resize(clen);
+      data_len[q] = clen;
+    }
     Buf ds;                              // dataspace, version 1
     ds.u8(0, 1);
     ds.u8(1, (unsigned)d.dims.size());
@@ -136,23 +153,60 @@ int write(const std::string& path, const std::vector<Dataset>& sets_in) {
     fv.u8(1, 1);                         // space allocated early
     fv.u8(2, 2);                         // fill value never written
     fv.u8(3, 0);
-    Buf ly;                              // layout, version 3, contiguous (address set below)
+    Buf ly;                              // layout, version 3 (addresses set below)
     ly.u8(0, 3);
-    ly.u8(1, 1);
-    ly.at(18);
-    hdrs[q] = {{0x0001, 0, ds.b}, {0x0003, 1, datatype(d.type)}, {0x0005, 1, fv.b}, {0x0008, 0, ly.b}};
+    if (chunked) {
+      ly.u8(1, 2);                       // chunked
+      ly.u8(2, (unsigned)d.dims.size() + 1);
+      ly.at(11 + 4 * (d.dims.size() + 1));
+    } else {
+      ly.u8(1, 1);                       // contiguous
+      ly.at(18);
+    }
+    hdrs[q] = {{0x0001, 0, ds.b}, {0x0003, 1, datatype(d.type)}, {0x0005, 1, fv.b}};
+    if (chunked) {
+      Buf fp;                            // filter pipeline, version 1: deflate(level)
+      fp.u8(0, 1);
+      fp.u8(1, 1);
+      fp.at(8);
+      fp.u16(8, FILTER_DEFLATE);
+      fp.u16(10, 0);                     // no name
+      fp.u16(12, 0);                     // flags: mandatory
+      fp.u16(14, 1);                     // one client value
+      fp.u32(16, (unsigned)d.deflate);
+      fp.at(24);                         // padded to an even number of values
+      hdrs[q].push_back({0x000B, 1, fp.b});
+    }
+    hdrs[q].push_back({0x0008, 0, ly.b});
     hdr_at[q] = p;
     p = pad8(p + header_size(hdrs[q]));
   }
+  auto bt_size = [&](size_t rank) {
+    const uint64_t key = 8 + 8 * (rank + 1);
+    return 24 + (2 * ISTORE_K + 1) * key + 2 * ISTORE_K * 8;
+  };
   for (size_t q = 0; q < sets.size(); ++q) {
+    if (!packed[q].empty()) {
+      bt_at[q] = p;
+      p = pad8(p + bt_size(sets[q].dims.size()));
+    }
     data_at[q] = p;
     p = pad8(p + data_len[q]);
     Buf ly;
     ly.u8(0, 3);
-    ly.u8(1, 1);
-    ly.u64(2, data_len[q] ? data_at[q] : UNDEF);
-    ly.u64(10, data_len[q]);
-    hdrs[q][3].body = ly.b;
+    if (!packed[q].empty()) {
+      const size_t rank = sets[q].dims.size();
+      ly.u8(1, 2);
+      ly.u8(2, (unsigned)rank + 1);
+      ly.u64(3, bt_at[q]);
+      for (size_t a = 0; a < rank; ++a) ly.u32(11 + 4 * a, (uint32_t)sets[q].dims[a]);  // one chunk
+      ly.u32(11 + 4 * rank, (uint32_t)elem_size(sets[q].type));
+    } else {
+      ly.u8(1, 1);
+      ly.u64(2, data_len[q] ? data_at[q] : UNDEF);
+      ly.u64(10, data_len[q]);
+    }
+    hdrs[q].back().body = ly.b;
   }
   const uint64_t eof = p;
 
@@ -217,7 +271,31 @@ int write(const std::string& path, const std::vector<Dataset>& sets_in) {
   f.at(snod + snod_size);
   for (size_t q = 0; q < sets.size(); ++q) {
     put_header(f, hdr_at[q], hdrs[q]);
-    f.bytes(data_at[q], sets[q].data, data_len[q]);
+    if (packed[q].empty()) {
+      f.bytes(data_at[q], sets[q].data, data_len[q]);
+      continue;
+    }
+    // chunk B-tree (node type 1, leaf): key 0 = the chunk (stored size,
+    // filter mask, offset 0 per axis), its address, then the bounding key
+    const size_t rank = sets[q].dims.size();
+    const uint64_t b = bt_at[q], key = 8 + 8 * (rank + 1);
+    f.bytes(b, "TREE", 4);
+    f.u8(b + 4, 1);
+    f.u8(b + 5, 0);
+    f.u16(b + 6, 1);
+    f.u64(b + 8, UNDEF);
+    f.u64(b + 16, UNDEF);
+    f.u32(b + 24, (uint32_t)data_len[q]);
+    f.u32(b + 28, 0);
+    for (size_t a = 0; a <= rank; ++a) f.u64(b + 32 + 8 * a, 0);
+    f.u64(b + 24 + key, data_at[q]);
+    const uint64_t k1 = b + 24 + key + 8;
+    f.u32(k1, 0);
+    f.u32(k1 + 4, 0);
+    for (size_t a = 0; a < rank; ++a) f.u64(k1 + 8 + 8 * a, sets[q].dims[a]);
+    f.u64(k1 + 8 + 8 * rank, 0);
+    f.at(b + bt_size(rank));
+    f.bytes(data_at[q], packed[q].data(), packed[q].size());
   }
   f.at(eof);
   FILE* fp = std::fopen(path.c_str(), "wb");
@@ -279,8 +357,9 @@ int read(const std::string& path, std::vector<Read>& out) {
       r.name = reinterpret_cast<const char*>(&f.b[heap_data + noff]);
       // version-1 object header: dataspace, datatype, layout
       const unsigned nmsg = (unsigned)f.get(oh + 2, 2);
-      uint64_t p = oh + 16, addr = UNDEF, len = 0;
-      bool have_type = false;
+      uint64_t p = oh + 16, addr = UNDEF, len = 0, btree_at = UNDEF;
+      bool have_type = false, chunked = false, deflate = false;
+      std::vector<uint64_t> cdims;
       for (unsigned m = 0; m < nmsg && f.ok; ++m) {
         const unsigned type = (unsigned)f.get(p, 2), msz = (unsigned)f.get(p + 2, 2);
         const uint64_t d = p + 8;
@@ -294,16 +373,54 @@ int read(const std::string& path, std::vector<Read>& out) {
           else if (cls == 0 && size == 4) r.type = (f.b[d + 1] & 0x08) ? I32 : U32;
           else return fe_fail(FE_ERR_IO, path + ": unsupported datatype of " + r.name);
           have_type = true;
+        } else if (type == 0x000B) {
+          // filter pipeline: deflate alone
+          const unsigned ver = f.b[d], nf = f.b[d + 1];
+          uint64_t q = d + (ver == 1 ? 8 : 2);
+          for (unsigned k = 0; k < nf && f.ok; ++k) {
+            const unsigned id = (unsigned)f.get(q, 2);
+            const unsigned nlen = (ver == 1 || id >= 256) ? (unsigned)f.get(q + 2, 2) : 0;
+            const unsigned ncd = (unsigned)f.get(q + (ver == 1 || id >= 256 ? 6 : 4), 2);
+            if (id != FILTER_DEFLATE)
+              return fe_fail(FE_ERR_IO, path + ": filter " + std::to_string(id) + " not supported (" + r.name + ")");
+            deflate = true;
+            q += (ver == 1 || id >= 256 ? 8 : 6) + (ver == 1 ? pad8(nlen) : nlen) + 4 * ncd;
+            if (ver == 1 && (ncd & 1)) q += 4;
+          }
         } else if (type == 0x0008) {
-          if (f.b[d] != 3 || f.b[d + 1] != 1)
-            return fe_fail(FE_ERR_IO, path + ": only contiguous datasets are supported (" + r.name + ")");
-          addr = f.get(d + 2, 8);
-          len = f.get(d + 10, 8);
+          if (f.b[d] != 3 || (f.b[d + 1] != 1 && f.b[d + 1] != 2))
+            return fe_fail(FE_ERR_IO, path + ": only contiguous or chunked datasets are supported (" + r.name + ")");
+          if (f.b[d + 1] == 1) {
+            addr = f.get(d + 2, 8);
+            len = f.get(d + 10, 8);
+          } else {
+            chunked = true;
+            const unsigned nd = f.b[d + 2];
+            btree_at = f.get(d + 3, 8);
+            for (unsigned a = 0; a < nd; ++a) cdims.push_back(f.get(d + 11 + 4 * a, 4));
+          }
         }
         p = d + msz;
       }
       uint64_t count = r.dims.empty() ? 0 : 1;
       for (uint64_t x : r.dims) count *= x;
+      if (chunked) {
+        // one chunk covering the dataset (what write() makes), deflated
+        bool one = have_type && cdims.size() == r.dims.size() + 1 && btree_at + 24 <= f.b.size();
+        for (size_t a = 0; one && a < r.dims.size(); ++a) one = cdims[a] == r.dims[a];
+        if (!one || !deflate || std::memcmp(&f.b[btree_at], "TREE", 4) != 0 || f.b[btree_at + 4] != 1 ||
+            f.b[btree_at + 5] != 0 || f.get(btree_at + 6, 2) != 1)
+          return fe_fail(FE_ERR_IO, path + ": chunked dataset " + r.name + " is not one deflated chunk");
+        const uint64_t key = 8 + 8 * cdims.size();
+        const uint64_t clen = f.get(btree_at + 24, 4), caddr = f.get(btree_at + 24 + key, 8);
+        if (!f.ok || caddr + clen > f.b.size()) return fe_fail(FE_ERR_IO, path + ": bad chunk of " + r.name);
+        r.bytes.resize(count * elem_size(r.type));
+        uLongf got_len = (uLongf)r.bytes.size();
+        if (uncompress(r.bytes.data(), &got_len, &f.b[caddr], (uLong)clen) != Z_OK || got_len != r.bytes.size())
+          return fe_fail(FE_ERR_IO, path + ": inflate failed for " + r.name);
+        out.push_back(std::move(r));
+        continue;
+      }
       if (!f.ok || !have_type || count * elem_size(r.type) != len || (len && addr + len > f.b.size()))
         return fe_fail(FE_ERR_IO, path + ": bad dataset " + r.name);
       if (len) r.bytes.assign(f.b.begin() + addr, f.b.begin() + addr + len);

@@ -1,7 +1,8 @@
 // On-disk formats of the reference driver (felbm_gpu_main.cu:86-189), over
 // the public C-ABI: field dumps <output_name>_<iter>.h5, geometry.h5, the
 // checkpoint, and particles_<step>.h5. Same dataset names, shapes and types;
-// no gzip (contiguous datasets: the reference's fast default is gzip off).
+// field files optionally gzip-compressed as the reference's output_deflate
+// (one chunk per dataset); the rest contiguous.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -17,8 +18,8 @@ using fe::h5::Dataset;
 
 extern "C" {
 
-int fe_write_fields_h5(fe_engine* e, const char* path, int float32) {
-  if (!e || !path) return fe_fail(FE_ERR_ARG, "fe_write_fields_h5: bad arguments");
+int fe_write_fields_h5(fe_engine* e, const char* path, int float32, int deflate) {
+  if (!e || !path || deflate < 0 || deflate > 9) return fe_fail(FE_ERR_ARG, "fe_write_fields_h5: bad arguments");
   int64_t n = 0;
   int rc = fe_engine_size(e, &n, nullptr);
   if (rc) return rc;
@@ -36,6 +37,7 @@ int fe_write_fields_h5(fe_engine* e, const char* path, int float32) {
     d.dims = {(uint64_t)n};
     d.type = float32 ? fe::h5::F32 : fe::h5::F64;
     d.data = float32 ? (const void*)(vf.data() + q * n) : (const void*)(v.data() + q * n);
+    d.deflate = deflate;
     sets.push_back(d);
   }
   return fe::h5::write(path, sets);
@@ -180,6 +182,22 @@ int fe_write_stretching(const char* path, int header, const double* rows, int64_
 
 // Generic read of one dataset of a file written here (tests, tools): the
 // element type (FE_H5_*), the dimensions and the raw little-endian bytes.
+int fe_h5_write_dataset(const char* path, const char* name, int type, int rank, const int64_t* dims,
+                        const void* data, int deflate) {
+  if (!path || !name || !dims || !data || type < 0 || type > 3 || rank < 1 || rank > 2)
+    return fe_fail(FE_ERR_ARG, "fe_h5_write_dataset: bad arguments");
+  Dataset d;
+  d.name = name;
+  d.type = (fe::h5::Type)type;
+  for (int a = 0; a < rank; ++a) {
+    if (dims[a] < 0) return fe_fail(FE_ERR_ARG, "fe_h5_write_dataset: negative extent");
+    d.dims.push_back((uint64_t)dims[a]);
+  }
+  d.data = data;
+  d.deflate = deflate;
+  return fe::h5::write(path, {d});
+}
+
 int fe_h5_read_dataset(const char* path, const char* name, int* type, int64_t* dims, int* rank, void* data,
                        int64_t capacity_bytes) {
   if (!path || !name || !type || !dims || !rank) return fe_fail(FE_ERR_ARG, "fe_h5_read_dataset: bad arguments");

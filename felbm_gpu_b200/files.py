@@ -14,8 +14,22 @@ _i64 = C.POINTER(C.c_int64)
 _DT = {0: np.float64, 1: np.float32, 2: np.int32, 3: np.uint32}
 
 
-def write_fields(engine, path: str, float32: bool = False):
-    check(lib.fe_write_fields_h5(engine._h, path.encode(), int(float32)))
+def write_fields(engine, path: str, float32: bool = False, deflate: int = 0):
+    """Field file <output_name>_<iter>.h5: output_float32 and output_deflate
+    (gzip level 0-9, one chunk per dataset) as the reference's cfg keys."""
+    check(lib.fe_write_fields_h5(engine._h, path.encode(), int(float32), int(deflate)))
+
+
+def write_dataset(path: str, name: str, arr: np.ndarray, deflate: int = 0):
+    """A new file holding one 1-D or 2-D array (float64, float32, int32 or
+    uint32), contiguous or (deflate 1-9) one gzip-filtered chunk."""
+    arr = np.ascontiguousarray(arr)
+    code = {np.dtype(np.float64): 0, np.dtype(np.float32): 1, np.dtype(np.int32): 2, np.dtype(np.uint32): 3}
+    if arr.dtype not in code or arr.ndim not in (1, 2):
+        raise ValueError("write_dataset: 1-D or 2-D float64, float32, int32 or uint32")
+    dims = np.array(arr.shape, np.int64)
+    check(lib.fe_h5_write_dataset(path.encode(), name.encode(), code[arr.dtype], arr.ndim,
+                                  dims.ctypes.data_as(_i64), arr.ctypes.data_as(C.c_void_p), int(deflate)))
 
 
 def write_geometry(path: str, solid: np.ndarray):

@@ -512,10 +512,12 @@ int fe_tracers_seed(const uint8_t* solid, int nx, int ny, int nz, int mode, int 
 /* ---- files ----------------------------------------------------------------
  * The reference driver's on-disk formats (felbm_gpu_main.cu:86-189), HDF5
  * with the same dataset names, shapes and types, written without libhdf5
- * (contiguous datasets, no gzip). Fields of the current state (refreshed as
+ * (contiguous datasets). Fields of the current state (refreshed as
  * fe_download_fields): density, concentration, u_x, u_y, u_z, pressure, n
- * values each in the reference order, float32 or float64. */
-int fe_write_fields_h5(fe_engine* e, const char* path, int float32);
+ * values each in the reference order, float32 or float64 (output_float32);
+ * deflate 1-9 (output_deflate) stores each as one chunk through the gzip
+ * filter at that level, as write_fields_h5 does (felbm_gpu_main.cu:94-98). */
+int fe_write_fields_h5(fe_engine* e, const char* path, int float32, int deflate);
 /* geometry.h5: coords [n][3] int (x, y, z of each site) and size [3] int. */
 int fe_write_geometry_h5(const char* path, const uint8_t* solid, int nx, int ny, int nz);
 /* Checkpoint (write_checkpoint / read_checkpoint, :151-189): h, g (Vn
@@ -542,6 +544,10 @@ int fe_write_particles_h5(const char* path, int64_t n, const double* pos, const 
  * lambda_w lambda_nw n_w n_nw). */
 int fe_write_series(const char* path, int header, uint32_t iter, const double stats[6], int64_t n);
 int fe_write_stretching(const char* path, int header, const double* rows, int64_t nrows);
+/* A new file holding one dataset (type as below, rank 1 or 2), contiguous,
+ * or with deflate 1-9 one chunk through the gzip filter at that level. */
+int fe_h5_write_dataset(const char* path, const char* name, int type, int rank, const int64_t* dims,
+                        const void* data, int deflate);
 /* One dataset of a file written here: type 0 double, 1 float, 2 int32,
  * 3 uint32; dims[rank]; raw bytes into data (NULL: shape only). */
 int fe_h5_read_dataset(const char* path, const char* name, int* type, int64_t* dims, int* rank, void* data,

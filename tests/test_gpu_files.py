@@ -55,15 +55,16 @@ def test_checkpoint_of_other_geometry_is_refused(require_gpu, tmp_path):
         ec.free()
 
 
-@pytest.mark.parametrize("f32", [False, True])
-def test_field_file_matches_download(require_gpu, tmp_path, f32):
+@pytest.mark.parametrize("f32,deflate", [(False, 0), (True, 0), (False, 4), (True, 9)])
+def test_field_file_matches_download(require_gpu, tmp_path, f32, deflate):
+    """output_float32 / output_deflate (gzip level, one chunk per dataset)."""
     case = make_case("spheres_mrt_wet")
     p = str(tmp_path / "fields_20.h5")
     e = MultiPhaseGPU(case.params, case.solid)
     try:
         e.upload_state(case.h0, case.g0)
         e.run(20)
-        files.write_fields(e, p, float32=f32)
+        files.write_fields(e, p, float32=f32, deflate=deflate)
         f = e.download()
     finally:
         e.free()
