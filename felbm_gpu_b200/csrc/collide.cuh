@@ -33,60 +33,32 @@
 #pragma once
 #include <type_traits>
 
-#include "bulk.cuh"
 #include "kernels.cuh"
 
 namespace fe {
 
-// How the main pass gets each opposite pair's stencil values (cd_c, bd_c,
-// bd_p of both directions): from a per-thread shared-memory stash the
-// pre-pass fills (FE_COLLIDE_STASH 1), or recomputed from the (c, p) tile
-// (0: a third of the shared memory, so more CTAs fit an SM).
-#ifndef FE_COLLIDE_STASH
-#define FE_COLLIDE_STASH 1
-#endif
-// Resident CTAs per SM of the FP32-arithmetic variants (2: 128 registers a
-// thread; 3: 80).
-#ifndef FE_COLLIDE_MINB
-#define FE_COLLIDE_MINB 2
-#endif
-
-// Resident CTAs per SM: FP64 arithmetic needs the full budget of 255
-// registers a thread.
+// Resident CTAs per SM: FP32 arithmetic fits 128 registers a thread, FP64
+// needs the full budget of 255.
 template <class S>
 struct CollideMinBlocks {
-  static constexpr int value = sizeof(typename S::real) == 8 ? 1 : FE_COLLIDE_MINB;
+  static constexpr int value = 65536 / ((sizeof(typename S::real) == 8 ? 256 : 128) * P4T);
 };
 
 constexpr int NPAIR = (Q - 1) / 2;  // 9 opposite pairs
 
-// The g populations of a brick's first FE_COLLIDE_GBULK chunks of P4T sites
-// are brought into shared memory by bulk copies issued before the tile
-// staging (one contiguous AoSoA range per chunk), so the site loop reads
-// them from shared memory; 0 reads them from global memory per site.
-#ifndef FE_COLLIDE_GBULK
-#define FE_COLLIDE_GBULK 0
-#endif
-
 // Dynamic shared memory of the collide pass: site indices, the interleaved
-// (c, p) tile and the lap(mu) tile (halo 2), the per-thread stash (two
-// pairs and one scalar per opposite pair), and the g chunks.
+// (c, p) tile and the lap(mu) tile (halo 2), and the per-thread stash (two
+// pairs and one scalar per opposite pair).
 template <class S, class Sh>
 struct CollideSmem {
   using R = typename S::real;
   using T = Tile<Sh, 2>;
-  static constexpr bool STASH = FE_COLLIDE_STASH != 0;
   static constexpr int NT16 = (T::N * 4 + 15) & ~15;
   static constexpr int NTR = (T::N * (int)sizeof(R) + 15) & ~15;
   static constexpr int NTV = (T::N * (int)sizeof(V2<R>) + 15) & ~15;
-  static constexpr int STV = STASH ? 2 * NPAIR * P4T * (int)sizeof(V2<R>) : 0;
-  static constexpr int STS = STASH ? NPAIR * P4T * (int)sizeof(R) : 0;
-  static constexpr int GCH = FE_COLLIDE_GBULK;                        // chunks staged
-  static constexpr int GBLK = P4T / AOSOA + 1;                        // AoSoA blocks a chunk can touch
-  static constexpr int GCHE = GBLK * Q * AOSOA;                       // g entries a chunk buffer holds
-  static constexpr int GB = GCH * GCHE * (int)sizeof(typename S::gpop);
-  static constexpr int OFF_G = NT16 + NTV + NTR + STV + STS;
-  static constexpr int BYTES = OFF_G + GB;
+  static constexpr int STV = 2 * NPAIR * P4T * (int)sizeof(V2<R>);
+  static constexpr int STS = NPAIR * P4T * (int)sizeof(R);
+  static constexpr int BYTES = NT16 + NTV + NTR + STV + STS;
 };
 
 // Per-site scalars shared by every direction of the collision.
@@ -119,37 +91,10 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   R* s_l = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTV);
   V* s_sv = reinterpret_cast<V*>(dsm + SM::NT16 + SM::NTV + SM::NTR) + threadIdx.x;            // [(2 pr + j) P4T]
   R* s_sc = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTV + SM::NTR + SM::STV) + threadIdx.x;  // [pr P4T]
-  PG* s_g = reinterpret_cast<PG*>(dsm + SM::OFF_G);  // [GCH][GCHE]
-  __shared__ uint64_t s_gbar;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
-  const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
-  if (SM::GCH && threadIdx.x == 0) mbar_init(&s_gbar);
   load_brick<Sh, 2, P4T>(D, brick, s, s_idx);
-  if (SM::GCH && threadIdx.x == 0) {
-    // the g of the first chunks of sites: AoSoA blocks b0..b1 of each chunk
-    // are one contiguous range; the copies run while the tiles are staged
-    uint32_t total = 0;
-#pragma unroll
-    for (int ch = 0; ch < SM::GCH; ++ch) {
-      const int r0 = ch * P4T;
-      if (r0 >= s.cnt) break;
-      const int m = min(P4T, s.cnt - r0);
-      const int b0 = (s.first + r0) >> 5, b1 = (s.first + r0 + m - 1) >> 5;
-      total += (uint32_t)((b1 - b0 + 1) * Q * AOSOA * (int)sizeof(PG));
-    }
-    mbar_arrive_expect_tx(&s_gbar, total);
-#pragma unroll
-    for (int ch = 0; ch < SM::GCH; ++ch) {
-      const int r0 = ch * P4T;
-      if (r0 >= s.cnt) break;
-      const int m = min(P4T, s.cnt - r0);
-      const int b0 = (s.first + r0) >> 5, b1 = (s.first + r0 + m - 1) >> 5;
-      bulk_g2s(s_g + ch * SM::GCHE, gin + (int64_t)b0 * (Q * AOSOA), (uint32_t)((b1 - b0 + 1) * Q * AOSOA * sizeof(PG)),
-               &s_gbar);
-    }
-  }
   {
     const F* const src[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
                              static_cast<const F*>(D.lapmu)};
@@ -174,6 +119,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   const R itau0 = (R)(1.0 / Pm.tau0), itau1 = (R)(1.0 / Pm.tau1), ffac = (R)s.ff;
   const R gxa = (R)Pm.gx, gya = (R)Pm.gy, gza = (R)Pm.gz;
   const R fxa = (R)Pm.fx * ffac, fya = (R)Pm.fy * ffac, fza = (R)Pm.fz * ffac;
+  const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
   PH* __restrict__ hout = static_cast<PH*>(D.pop[parity ^ 1][0]);
   PG* __restrict__ gout = static_cast<PG*>(D.pop[parity ^ 1][1]);
   const F* __restrict__ fmu = static_cast<const F*>(D.mu);
@@ -182,7 +128,6 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   double st[6] = {0, 0, 0, 0, 0, 0};
   int bad = 0;
   const int first = s.first, cnt = s.cnt;
-  bool gwaited = false, gok = false;
 
   for (int r = threadIdx.x; r < cnt; r += P4T) {
     const int64_t i = first + r;
@@ -193,28 +138,13 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     SiteScal<R> q;
     q.mu = (R)fmu[i];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
-    // post-stream g of the site (what P1 read), the pairs (k, k+1) together;
-    // from the staged chunk when the site's chunk was copied in
+    // post-stream g of the site (what P1 read), the pairs (k, k+1) together
     const IX a0 = (IX)pbase(i);
-    const PG* gsrc = gin;
-    IX ga = a0;
-    if (SM::GCH && r < SM::GCH * P4T) {
-      if (!gwaited) {
-        gok = mbar_wait(&s_gbar, 0, 1 << 20);
-        gwaited = true;
-        if (!gok) atomicOr(&D.ctl->status, 4);
-      }
-      if (gok) {
-        const int ch = r / P4T;
-        gsrc = s_g + ch * SM::GCHE;
-        ga = (IX)(((int)(i >> 5) - ((first + ch * P4T) >> 5)) * (Q * AOSOA) + (int)(i & (AOSOA - 1)));
-      }
-    }
-    R g0 = ld_pop<GV<S>>(gsrc, ga, 0, shg);
+    R g0 = ld_pop<GV<S>>(gin, a0, 0, shg);
     V gp[NPAIR];
 #pragma unroll
     for (int k = 1; k < Q; k += 2)
-      gp[k >> 1] = V(ld_pop<GV<S>>(gsrc, ga + k * AOSOA, k, shg), ld_pop<GV<S>>(gsrc, ga + (k + 1) * AOSOA, k + 1, shg));
+      gp[k >> 1] = V(ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg), ld_pop<GV<S>>(gin, a0 + (k + 1) * AOSOA, k + 1, shg));
     // push target of direction k: slot k of x + e_k, or slot opp(k) of x
     // (halfway bounce-back) when x + e_k is solid
     auto dst = [&](int k) -> IX {
@@ -236,11 +166,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const V fm = s_cp[pos - o], fp = s_cp[pos + o], fm2 = s_cp[pos - 2 * o], fp2 = s_cp[pos + 2 * o];
       V cd, ba, bb;
       pair_derivs2<HBB>(cp0, fm, fp, fm2, fp2, cd, ba, bb);
-      if constexpr (SM::STASH) {
-        s_sc[pr * P4T] = cd.x();
-        s_sv[(2 * pr) * P4T] = V(ba.x(), bb.x());
-        s_sv[(2 * pr + 1) * P4T] = V(ba.y(), bb.y());
-      }
+      s_sc[pr * P4T] = cd.x();
+      s_sv[(2 * pr) * P4T] = V(ba.x(), bb.x());
+      s_sv[(2 * pr + 1) * P4T] = V(ba.y(), bb.y());
       // pairs: central terms count twice, biased ones as a difference
       const R aw = alpha * weight<R>(k);
       const V db = ba - bb;
@@ -375,19 +303,8 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
       const int o = T::off(k), pr = k >> 1;
-      R cdc;
-      V BC, BP;
-      if constexpr (SM::STASH) {
-        cdc = s_sc[pr * P4T];
-        BC = s_sv[(2 * pr) * P4T];
-        BP = s_sv[(2 * pr + 1) * P4T];
-      } else {
-        V cd, ba, bb;
-        pair_derivs2<HBB>(cp0, s_cp[pos - o], s_cp[pos + o], s_cp[pos - 2 * o], s_cp[pos + 2 * o], cd, ba, bb);
-        cdc = cd.x();
-        BC = V(ba.x(), bb.x());
-        BP = V(ba.y(), bb.y());
-      }
+      const R cdc = s_sc[pr * P4T];
+      const V BC = s_sv[(2 * pr) * P4T], BP = s_sv[(2 * pr + 1) * P4T];
       const R lm = s_l[pos - o], lp = s_l[pos + o];
       // avg of +e takes the +e neighbour, of -e the -e one
       const V la = fma2(V(R(0.5)), V(lp, lm), V(hl));
@@ -497,9 +414,6 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       }
     }
   }
-  // the copies must have landed before the CTA's shared memory is released:
-  // the issuing thread waits for them (bounded) unless it already has
-  if (SM::GCH && threadIdx.x == 0 && !gwaited && !mbar_wait(&s_gbar, 0, 1 << 20)) atomicOr(&D.ctl->status, 4);
   // flow-statistics partials per warp (reference k_flow_stats :660-683, summed
   // on demand), no block barrier
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

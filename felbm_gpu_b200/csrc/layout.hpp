@@ -55,7 +55,7 @@ struct Ctl {
   unsigned int count1;   // last-block counters (reset by the last block)
   unsigned int count4;
   unsigned int countm;
-  unsigned int counts;
+  unsigned int counts;   // owned by k_stats_finalize, launched on the engine's stream only
   double stats[6];       // flow statistics of the last finalize
   int32_t status;        // nonzero: a kernel detected a problem
   int32_t pad_;

@@ -23,7 +23,9 @@
 //    results: order them on one stream or with events;
 //  - the first call on each device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture is started.
+//    before any stream capture is started. The address is kept for the life
+//    of the process, so a cudaDeviceReset (which reloads the module and may
+//    move the array) must not be followed by further calls on that device.
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -241,7 +241,12 @@ int fe_step(fe_engine* e, int nsteps);
 /* Replaces apply_mass_correction() (multiphase_gpu.cuh:689-700). When drift
  * is non-NULL the drift M - M0 is computed now and returned (a blocking
  * reduction, as in the reference); when NULL the correction is queued and
- * fused into the next step's moment pass. No-op unless correct_op_mass. */
+ * fused into the next step's moment pass. No-op unless correct_op_mass.
+ * Unlike the reference, the stored populations take the correction later:
+ * fe_current_mass (and a reduction of a state taken by other means) sees the
+ * corrected total only after fe_settle_mass_correction, the next step, or a
+ * download (fe_download_state, fe_download_fields, checkpoints), which all
+ * apply the queued correction first. */
 int fe_apply_mass_correction(fe_engine* e, double* drift);
 /* The driver's hot loop (felbm_gpu_main.cu:741-745): nsteps x (step + mass
  * correction), with forcing_factor_at(t) evaluated per step from the
@@ -336,7 +341,9 @@ int fe_init_equilibrium(int64_t n, const double* c, const double* p, const doubl
  * FE_ERR_ARG. All calls on a device share that array: calls whose work
  * overlaps on the GPU race and give wrong results. The first call on each
  * device sets up the array's address (with that device current); make it
- * before starting any stream capture. */
+ * before starting any stream capture. The address is kept for the life of
+ * the process: after a cudaDeviceReset the library must not be called on
+ * that device again. */
 #define FE_NOALLOC_MAX_SITES 33554432LL
 int fe_mass_weight_noalloc(const double* d_h, int64_t n, double* d_out, void* stream);
 

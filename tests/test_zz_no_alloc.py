@@ -54,3 +54,26 @@ def test_noalloc_rejects_sizes_beyond_scratch(require_gpu):
                                           None)
     assert rc == _capi.FE_ERR_ARG
     assert b"exceeds the fixed scratch capacity" in _capi.lib.fe_last_error()
+
+
+@pytest.mark.parametrize("n", [1, 2047, 2048, 2049, 3 * 2048 + 5])
+def test_noalloc_block_edges(require_gpu, n):
+    """Sizes around the 2048-site block split (one partial block, exactly one
+    block, one site over, several blocks and a ragged tail): M and W against
+    a numpy sum on two calls in a row, so a stale counter would show."""
+    import torch
+    gen = torch.Generator(device="cuda").manual_seed(n)
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for call in range(2):
+        h = torch.rand(19 * n, dtype=torch.float64, device="cuda", generator=gen) * (2.0 / 19.0)
+        torch.cuda.synchronize()
+        _capi.check(_capi.lib.fe_mass_weight_noalloc(C.c_void_p(h.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                                     stream))
+        torch.cuda.synchronize()
+        m, w = out.cpu().numpy()
+        c = h.cpu().numpy().reshape(19, n).sum(0)
+        m_ref = float(c.sum())
+        w_ref = float(np.maximum(c * (1.0 - c), 0.0).sum())
+        assert abs(m - m_ref) <= TOL * abs(m_ref), (n, call, m, m_ref)
+        assert abs(w - w_ref) <= TOL * max(abs(w_ref), 1e-300), (n, call, w, w_ref)
