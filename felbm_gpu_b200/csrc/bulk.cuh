@@ -1,6 +1,7 @@
-// Asynchronous bulk copies global -> shared memory of this CTA (the sm_90+
-// TMA engine's untiled form, cp.async.bulk) completed on an mbarrier, with
-// bounded waits. Sources are this GPU's own memory; no multicast.
+// Asynchronous copies global -> shared memory of this CTA by the TMA engine:
+// contiguous bulk copies (cp.async.bulk) and 3-D box copies described by a
+// tensor map (cp.async.bulk.tensor), completed on an mbarrier, with bounded
+// waits. Sources are this GPU's own memory; no multicast.
 #pragma once
 #include <cstdint>
 
@@ -28,6 +29,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// The box at element coordinates (x, y, z) of the 3-D tensor `tmap` (a
+// CUtensorMap in global memory) to shared dst (128-byte aligned), counted on
+// bar. x times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_box3(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
 

@@ -46,19 +46,28 @@ struct CollideMinBlocks {
 
 constexpr int NPAIR = (Q - 1) / 2;  // 9 opposite pairs
 
-// Dynamic shared memory of the collide pass: site indices, the interleaved
-// (c, p) tile and the lap(mu) tile (halo 2), and the per-thread stash (two
-// pairs and one scalar per opposite pair).
+// Dynamic shared memory of the collide pass (each region 128-byte aligned,
+// the alignment of a TMA destination): the halo-1 site-index tile (push
+// targets), the interleaved (c, p) tile and the lap(mu) tile (halo 2), and
+// the per-thread stash (two pairs and one scalar per opposite pair). The raw
+// c and p tiles land in the stash region and are interleaved from there
+// before the stash is used.
 template <class S, class Sh>
 struct CollideSmem {
   using R = typename S::real;
+  using F = typename S::fld;
   using T = Tile<Sh, 2>;
-  static constexpr int NT16 = (T::N * 4 + 15) & ~15;
-  static constexpr int NTR = (T::N * (int)sizeof(R) + 15) & ~15;
-  static constexpr int NTV = (T::N * (int)sizeof(V2<R>) + 15) & ~15;
+  using T1 = Tile<Sh, 1>;
+  static constexpr int al(int b) { return (b + 127) & ~127; }
+  static constexpr int IDX = al(T1::N * 4);
+  static constexpr int CP = al(T::N * (int)sizeof(V2<R>));
+  static constexpr int LT = al(T::N * (int)sizeof(F));
+  static constexpr int RAW = al(T::N * (int)sizeof(F));  // one raw field tile
   static constexpr int STV = 2 * NPAIR * P4T * (int)sizeof(V2<R>);
   static constexpr int STS = NPAIR * P4T * (int)sizeof(R);
-  static constexpr int BYTES = NT16 + NTV + NTR + STV + STS;
+  static constexpr int OFF_CP = IDX, OFF_L = OFF_CP + CP, OFF_ST = OFF_L + LT;
+  static constexpr int BYTES = OFF_ST + al(STV + STS);
+  static_assert(2 * RAW <= al(STV + STS), "the raw c and p tiles fit the stash region");
 };
 
 // Per-site scalars shared by every direction of the collision.
@@ -80,32 +89,55 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   using PG = typename S::gpop;
   using F = typename S::fld;
   using T = Tile<Sh, 2>;
+  using T1 = Tile<Sh, 1>;
   using SM = CollideSmem<S, Sh>;
   // population offsets: 32-bit while the lattice's arrays stay below 2^32
   // entries (the host picks WIDE otherwise)
   using IX = typename std::conditional<WIDE, int64_t, uint32_t>::type;
   __shared__ Head<Sh> s;
-  extern __shared__ __align__(16) unsigned char dsm[];
-  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);
-  V* s_cp = reinterpret_cast<V*>(dsm + SM::NT16);
-  R* s_l = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTV);
-  V* s_sv = reinterpret_cast<V*>(dsm + SM::NT16 + SM::NTV + SM::NTR) + threadIdx.x;            // [(2 pr + j) P4T]
-  R* s_sc = reinterpret_cast<R*>(dsm + SM::NT16 + SM::NTV + SM::NTR + SM::STV) + threadIdx.x;  // [pr P4T]
+  __shared__ uint64_t s_bar;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);  // halo-1 tile
+  V* s_cp = reinterpret_cast<V*>(dsm + SM::OFF_CP);
+  F* s_l = reinterpret_cast<F*>(dsm + SM::OFF_L);
+  F* raw_c = reinterpret_cast<F*>(dsm + SM::OFF_ST);
+  F* raw_p = reinterpret_cast<F*>(dsm + SM::OFF_ST + SM::RAW);
+  V* s_sv = reinterpret_cast<V*>(dsm + SM::OFF_ST) + threadIdx.x;                  // [(2 pr + j) P4T]
+  R* s_sc = reinterpret_cast<R*>(dsm + SM::OFF_ST + SM::STV) + threadIdx.x;         // [pr P4T]
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
-  load_brick<Sh, 2, P4T>(D, brick, s, s_idx);
+  // the copy engine writes 128-byte aligned boxes
+  if (smem_u32(dsm) & 127u) {
+    if (threadIdx.x == 0) atomicOr(&D.ctl->status, 8);
+    return;
+  }
+  // prologue: the brick's slot list, its halo-1 site-index tile and the c, p,
+  // lap(mu) tiles (halo 2) by copy engine, on one barrier
+  head_init(&s_bar);
+  if (threadIdx.x == 0) {
+    head_begin<Sh>(D, brick, s, &s_bar, (uint32_t)(3 * T::N * sizeof(F) + T1::N * 4));
+    tile_copy<Sh, 2>(raw_c, D, TM_C2, s.bx, s.by, s.bz, &s_bar);
+    tile_copy<Sh, 2>(raw_p, D, TM_P2, s.bx, s.by, s.bz, &s_bar);
+    tile_copy<Sh, 2>(s_l, D, TM_L2, s.bx, s.by, s.bz, &s_bar);
+    bulk_g2s(s_idx, D.tile1 + (int64_t)brick * T1::N, (uint32_t)(T1::N * 4), &s_bar);
+  }
+  if (threadIdx.x == P4T - 1) load_step_scalars(D, s);
+  if (!head_wait(D, &s_bar)) return;
+  // (c, p) pairs, with a queued mass correction applied to c
   {
-    const F* const src[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
-                             static_cast<const F*>(D.lapmu)};
-    R* const dst[3] = {reinterpret_cast<R*>(s_cp), reinterpret_cast<R*>(s_cp) + 1, s_l};
-    stage<Sh, 2, 3, P4T, true>(src, dst, true, s.lambda, s_idx);
+    const double lam = s.lambda;
+    for (int t = threadIdx.x; t < T::N; t += P4T) {
+      R c = (R)raw_c[t];
+      if (lam != 0.0 && is_site(c)) c = corr_c<R>(c, lam);
+      s_cp[t] = V(c, (R)raw_p[t]);
+    }
   }
   if (!WIDE) {
     // from here on the index tile holds each site's AoSoA population base
     // (below 2^32 - 1 for narrow offsets; 0xffffffff marks no site), so a
-    // push target is one add; every thread rewrites the positions it staged
-    for (int t = threadIdx.x; t < T::N; t += P4T) {
+    // push target is one add
+    for (int t = threadIdx.x; t < T1::N; t += P4T) {
       const int32_t v = s_idx[t];
       if (v >= 0) s_idx[t] = (int32_t)((uint32_t)(v >> 5) * (uint32_t)(Q * AOSOA) + (uint32_t)(v & (AOSOA - 1)));
     }
@@ -131,12 +163,13 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
 
   for (int r = threadIdx.x; r < cnt; r += P4T) {
     const int64_t i = first + r;
-    const int pos = T::pos(s.slot_of[r]);
+    const int slot = s.slot_of[r];
+    const int pos = T::pos(slot), pos1 = T1::pos(slot);
     const V cp0 = s_cp[pos];
     const R c = cp0.x(), p = cp0.y();
-    const R lmu = s_l[pos];
+    const R lmu = (R)s_l[pos];
     SiteScal<R> q;
-    q.mu = (R)fmu[i];
+    q.mu = (R)fmu[grid_entry<Sh>(D, s.bx, s.by, s.bz, slot)];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
     // post-stream g of the site (what P1 read), the pairs (k, k+1) together
     const IX a0 = (IX)pbase(i);
@@ -149,11 +182,11 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     // (halfway bounce-back) when x + e_k is solid
     auto dst = [&](int k) -> IX {
       if constexpr (WIDE) {
-        const int dn = s_idx[pos + T::off(k)];
+        const int dn = s_idx[pos1 + T1::off(k)];
         return dn >= 0 ? (IX)(dn >> 5) * (IX)(Q * AOSOA) + (IX)(k * AOSOA + (dn & (AOSOA - 1)))
                        : a0 + (IX)(lat_opp(k) * AOSOA);
       } else {
-        const uint32_t b = (uint32_t)s_idx[pos + T::off(k)];
+        const uint32_t b = (uint32_t)s_idx[pos1 + T1::off(k)];
         return b != 0xffffffffu ? b + (uint32_t)(k * AOSOA) : a0 + (uint32_t)(lat_opp(k) * AOSOA);
       }
     };
@@ -223,11 +256,11 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     }
     // open-boundary overwrite of g by the plain equilibrium (apply_open_bnd)
     if (flag & BC_G_OVER) {
-      const int64_t sb = D.bcsrc[i];
+      const int64_t sb = D.bcsrc[i], dsb = D.dense_of[sb];
       const F* ubc = static_cast<const F*>(D.u_bc);
       const R bux = (R)ubc[sb], buy = (R)ubc[D.n + sb], buz = (R)ubc[2 * D.n + sb];
-      const R bp = (R) static_cast<const F*>(D.p)[sb];
-      const R brho = rho1 + drho * (R) static_cast<const F*>(D.c)[sb];
+      const R bp = (R) static_cast<const F*>(D.p)[dsb];
+      const R brho = rho1 + drho * (R) static_cast<const F*>(D.c)[dsb];
       const R bu_sq = bux * bux + buy * buy + buz * buz;
       g0 = weight<R>(0) * (bp - brho * cs2 * R(GAMMA) * bu_sq);
 #pragma unroll
@@ -305,7 +338,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const int o = T::off(k), pr = k >> 1;
       const R cdc = s_sc[pr * P4T];
       const V BC = s_sv[(2 * pr) * P4T], BP = s_sv[(2 * pr + 1) * P4T];
-      const R lm = s_l[pos - o], lp = s_l[pos + o];
+      const R lm = (R)s_l[pos - o], lp = (R)s_l[pos + o];
       // avg of +e takes the +e neighbour, of -e the -e one
       const V la = fma2(V(R(0.5)), V(lp, lm), V(hl));
       const V AVG(is_site(lp) ? la.x() : lmu, is_site(lm) ? la.y() : lmu);

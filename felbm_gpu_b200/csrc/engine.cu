@@ -19,6 +19,9 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda.h>
+#include <mutex>
+#include <cudaTypedefs.h>
 #include "../../include/felbm_b200.h"
 #include "collide.cuh"
 #include "fe_internal.hpp"
@@ -266,6 +269,23 @@ static cudaError_t collide_smem_attr(int bytes) {
   set((const void*)k_collide<S, Sh, 2, true, false>);
   return e;
 }
+// cuTensorMapEncodeTiled from the driver (no link against libcuda), looked
+// up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
 // True when the lattice's population arrays reach 2^32 entries.
 static bool pops_wide(int64_t n) { return (uint64_t)((n + AOSOA - 1) / AOSOA) * AOSOA * Q >= (1ull << 32); }
 
@@ -282,6 +302,7 @@ struct Engine {
   LatDesc* d_desc = nullptr;
   int2* d_work = nullptr;   // (lattice, brick) of the stencil passes
   int2* d_cwork = nullptr;  // (lattice, chunk) of the flat passes
+  int2* d_ghwork = nullptr; // (lattice, row block) of the grid-image refresh
   Ctl* d_ctl = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
@@ -484,13 +505,15 @@ struct Engine {
         FE_CUDA(cudaMemset(q, 0, popn * pop_size(f)));
         D.pop[b][f] = q;
       }
-    void** flds[] = {&D.c, &D.p, &D.jx, &D.jy, &D.jz, &D.mu, &D.lapmu};
-    for (void** f : flds) {
+    // momentum per site; the stencil fields on the dense node grid, NaN
+    // everywhere until the passes write the fluid nodes and their images
+    for (void** f : {&D.jx, &D.jy, &D.jz}) {
       unsigned char* q;
       if ((rc = alloc(&q, (size_t)D.n * fld_size()))) return rc;
       FE_CUDA(cudaMemset(q, 0, (size_t)D.n * fld_size()));
       *f = q;
     }
+    if ((rc = setup_grid())) return rc;
     if ((rc = alloc(&D.part1, (size_t)D.nchunks * 2))) return rc;
     if ((rc = alloc(&D.part4, (size_t)nbk * P4W * 6))) return rc;
     FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * P4W * 6 * 8));
@@ -523,20 +546,91 @@ struct Engine {
     return FE_OK;
   }
 
-  // Site-index tiles (halo 2 and 1) and slot lists of every brick, built
-  // once on the device by k_build_tiles and read by the stencil passes.
+  // Halo-1 site-index tiles (push targets) and slot lists of every brick,
+  // built once on the device by k_build_tiles and read by the stencil passes.
   template <class Sh>
   int alloc_tiles() {
-    int32_t *t2, *t1;
+    int32_t* t1;
     uint16_t* sl;
     const size_t nbk = (size_t)hd.nbricks;
     int rc;
-    if ((rc = alloc(&t2, nbk * Tile<Sh, 2>::N)) || (rc = alloc(&t1, nbk * Tile<Sh, 1>::N)) ||
-        (rc = alloc(&sl, nbk * Sh::C)))
-      return rc;
-    hd.tile2 = t2;
+    if ((rc = alloc(&t1, nbk * Tile<Sh, 1>::N)) || (rc = alloc(&sl, nbk * Sh::C))) return rc;
     hd.tile1 = t1;
     hd.slots = sl;
+    return FE_OK;
+  }
+
+  // The dense node grids of c, p, mu, lap(mu) (node coordinates [-2, nb B + 2)
+  // per axis; z only for 3-D bricks), the site -> grid entry table, the
+  // tensor maps of their halo boxes and the row blocks of k_ghost.
+  int setup_grid() {
+    LatDesc& D = hd;
+    const int B[3] = {1 << L.lb[0], 1 << L.lb[1], 1 << L.lb[2]};
+    D.hz = L.shape2d ? 0 : 1;
+    D.gdx = L.nb[0] * B[0] + 4;
+    D.gdy = L.nb[1] * B[1] + 4;
+    D.gdz = D.hz ? L.nb[2] * B[2] + 4 : 1;
+    D.gsy = D.gdx;
+    D.gsz = (int64_t)D.gdx * D.gdy;
+    const int64_t cells = D.gsz * D.gdz;
+    if (cells >= ((int64_t)1 << 31)) return fe_fail(FE_ERR_ARG, "lattice too large for the 32-bit field grid");
+    const size_t es = fld_size();
+    for (void** f : {&D.c, &D.p, &D.mu, &D.lapmu}) {
+      unsigned char* q;
+      int rc;
+      if ((rc = alloc(&q, (size_t)cells * es))) return rc;
+      FE_CUDA(cudaMemset(q, 0xff, (size_t)cells * es));  // all-ones: a NaN in FP32 and FP64
+      *f = q;
+    }
+    std::vector<int32_t> dense((size_t)D.n);
+    for (int64_t i = 0; i < D.n; ++i) {
+      const int64_t node = L.node_of[i];
+      const int64_t x = node % D.nx, y = (node / D.nx) % D.ny, z = node / ((int64_t)D.nx * D.ny);
+      dense[i] = (int32_t)((x + 2) + D.gsy * (y + 2) + D.gsz * (z + 2 * D.hz));
+    }
+    int32_t* dd;
+    int rc;
+    if ((rc = upload_vec(&dd, dense))) return rc;
+    D.dense_of = dd;
+    const int rows = D.gdy * D.gdz;
+    D.ghost_blocks = (rows + GHOST_ROWS - 1) / GHOST_ROWS;
+    std::vector<int2> gw(D.ghost_blocks);
+    for (int b = 0; b < D.ghost_blocks; ++b) gw[b] = make_int2(0, b);
+    if ((rc = upload_vec(&d_ghwork, gw))) return rc;
+    FE_DISPATCH(*this, rc = build_tmaps<S FE_COMMA Sh>());
+    return rc;
+  }
+
+  // Tensor maps of the halo boxes: c with halo 1 (P2) and 2 (P4), p and
+  // lap(mu) with halo 2 (P4), mu with halo 1 (P3); x halo 2 in every box.
+  template <class S, class Sh>
+  int build_tmaps() {
+    using F = typename S::fld;
+    auto enc = tmap_encoder();
+    if (!enc) return fe_fail(FE_ERR_CUDA, "cuTensorMapEncodeTiled not available from the driver");
+    const LatDesc& D = hd;
+    alignas(64) CUtensorMap maps[TM_N];
+    auto make = [&](int id, void* base, int H) -> int {
+      const cuuint64_t dims[3] = {(cuuint64_t)D.gdx, (cuuint64_t)D.gdy, (cuuint64_t)D.gdz};
+      const cuuint64_t strides[2] = {(cuuint64_t)D.gdx * sizeof(F), (cuuint64_t)D.gsz * sizeof(F)};
+      const cuuint32_t box[3] = {(cuuint32_t)(Sh::BX + 4), (cuuint32_t)(Sh::BY + 2 * H),
+                                 (cuuint32_t)(D.hz ? Sh::BZ + 2 * H : 1)};
+      const cuuint32_t estr[3] = {1, 1, 1};
+      const CUresult r = enc(&maps[id], sizeof(F) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                             3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fe_fail(FE_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+      return FE_OK;
+    };
+    int rc;
+    if ((rc = make(TM_C1, D.c, 1)) || (rc = make(TM_C2, D.c, 2)) || (rc = make(TM_P2, D.p, 2)) ||
+        (rc = make(TM_MU1, D.mu, 1)) || (rc = make(TM_L2, D.lapmu, 2)))
+      return rc;
+    unsigned char* q;
+    if ((rc = alloc(&q, sizeof(maps)))) return rc;
+    FE_CUDA(cudaMemcpy(q, maps, sizeof(maps), cudaMemcpyHostToDevice));
+    hd.tmap = q;
     return FE_OK;
   }
 
@@ -560,26 +654,30 @@ struct Engine {
   void launch_step_t(int par, cudaStream_t st, cudaEvent_t* ev) {
     const int nb = hd.nbricks;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
+    using F = typename S::fld;
     rec(0);
     k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
+    k_ghost<F><<<hd.ghost_blocks, CTA, 0, st>>>(d_desc, d_ghwork, GF_C | GF_P);
     rec(2);
     if (hd.prm.hbb) k_cfield<S, Sh, 0, true><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
     else k_cfield<S, Sh, 0, false><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
+    k_ghost<F><<<hd.ghost_blocks, CTA, 0, st>>>(d_desc, d_ghwork, GF_MU | GF_P);
     rec(3);
     if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
     else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
+    k_ghost<F><<<hd.ghost_blocks, CTA, 0, st>>>(d_desc, d_ghwork, GF_LAPMU);
     rec(4);
     launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
-    launches += 4;
+    launches += 7;
   }
   void launch_step(int par, cudaStream_t st, cudaEvent_t* ev = nullptr) {
     FE_DISPATCH(*this, launch_step_t<S FE_COMMA Sh>(par, st, ev));
   }
   int kernels_per_step() const {
-    int k = 4;
+    int k = 7;  // four passes and three grid-image refreshes
     if (open_bnd) {
       const int nio = hd.n_inlet + hd.n_outlet;
       k += (nio ? 1 : 0) + (hd.n_buf ? 1 : 0) + (nio + hd.n_buf ? 1 : 0);
@@ -705,9 +803,15 @@ struct Engine {
     return FE_OK;
   }
 
+  // The control block, and the problems the kernels recorded in it: tile
+  // copies of a stencil pass that did not land (bits 4, 8) or a non-finite
+  // velocity in the collision pass (bit 1).
   int read_ctl(Ctl* c) {
     FE_CUDA(cudaMemcpyAsync(c, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
     FE_CUDA(cudaStreamSynchronize(stream));
+    if (c->status & 12)
+      return fe_fail(FE_ERR_CUDA, "a stencil pass's tile copies did not complete (status " + std::to_string(c->status) + ")");
+    if (c->status & 1) return fe_fail(FE_ERR_DIVERGED, "non-finite velocity in the collision pass");
     return FE_OK;
   }
   int write_ctl_field(size_t off, const void* v, size_t sz) {
@@ -820,9 +924,10 @@ struct Engine {
   void fields_launch(FieldOut o) {
     k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
+    k_ghost<typename S::fld><<<hd.ghost_blocks, CTA, 0, stream>>>(d_desc, d_ghwork, GF_C | GF_P);
     if (hd.prm.hbb) k_cfield<S, Sh, OUT, true><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     else k_cfield<S, Sh, OUT, false><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
-    launches += 2;
+    launches += 3;
   }
   // Corrected velocity of the current state into node-indexed device grids
   // (solid nodes are left as they are), on the engine stream.
@@ -901,8 +1006,9 @@ struct Batch {
   LatDesc* d_desc = nullptr;
   int2* d_cwork = nullptr;
   int2* d_gwork = nullptr;          // the groups' work lists, one after another
-  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0;  // bytes (grow-only)
-  int ncwork = 0;
+  int2* d_hwork = nullptr;          // the members' grid-image row blocks
+  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0, cap_hwork = 0;  // bytes (grow-only)
+  int ncwork = 0, nhwork = 0;
   int64_t since_build = 0;          // steps since the last rebuild
   bool dirty = true;
   int64_t same_members = 0;  // launches since the last membership change
@@ -922,13 +1028,13 @@ struct Batch {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_arrays() {
-    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork})
+    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork, (void*)d_hwork})
       if (a) cudaFree(a);
     groups.clear();
     d_desc = nullptr;
-    d_cwork = d_gwork = nullptr;
-    cap_desc = cap_cwork = cap_gwork = 0;
-    ncwork = 0;
+    d_cwork = d_gwork = d_hwork = nullptr;
+    cap_desc = cap_cwork = cap_gwork = cap_hwork = 0;
+    ncwork = nhwork = 0;
   }
   void drop_graphs() {
     for (int p = 0; p < 2; ++p) {
@@ -1017,7 +1123,7 @@ struct Batch {
     since_build = 0;
     join_parity.assign(mem.size(), 0);
     std::vector<LatDesc> descs(mem.size());
-    std::vector<int2> cw;
+    std::vector<int2> cw, hw;
     int rc;
     for (size_t q = 0; q < mem.size(); ++q) {
       Engine* e = mem[q];
@@ -1030,6 +1136,7 @@ struct Batch {
       }
       descs[q] = d;
       for (int c = 0; c < d.nchunks; ++c) cw.push_back(make_int2((int)q, c));
+      for (int b = 0; b < d.ghost_blocks; ++b) hw.push_back(make_int2((int)q, b));
       if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;  // queued correction, forcing from t
     }
     std::vector<int2> gw;
@@ -1059,7 +1166,9 @@ struct Batch {
     for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
     if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
     if ((rc = upload_vec(&d_cwork, &cap_cwork, cw))) return rc;
+    if ((rc = upload_vec(&d_hwork, &cap_hwork, hw))) return rc;
     ncwork = (int)cw.size();
+    nhwork = (int)hw.size();
     dirty = false;
     return FE_OK;
   }
@@ -1090,10 +1199,14 @@ struct Batch {
       if (nb) k_bc_buffers<S><<<(nb + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
       if (nall) k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
     }
+    using F = typename S::fld;
+    k_ghost<F><<<nhwork, CTA, 0, st>>>(d_desc, d_hwork, GF_C | GF_P);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p2<S, typename decltype(t)::type>(g, st); });
+    k_ghost<F><<<nhwork, CTA, 0, st>>>(d_desc, d_hwork, GF_MU | GF_P);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p3<S, typename decltype(t)::type>(g, st); });
+    k_ghost<F><<<nhwork, CTA, 0, st>>>(d_desc, d_hwork, GF_LAPMU);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p4<S, typename decltype(t)::type>(g, par, st); });
   }
@@ -1109,7 +1222,7 @@ struct Batch {
   }
   // kernels of one step, the count launch_step_t makes
   int64_t launches_per_step() const {
-    int64_t k = 1 + 3 * (int64_t)groups.size();
+    int64_t k = 4 + 3 * (int64_t)groups.size();
     for (const Engine* e : mem)
       if (e->open_bnd) {
         const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf;

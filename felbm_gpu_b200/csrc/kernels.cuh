@@ -10,17 +10,18 @@
 //   P3 k_lapmu    mu stencil -> Laplacian of mu
 //   P4 k_collide  c, p stencils to distance 2, lap(mu) to distance 1, own g:
 //                 equilibria + Guo force + BGK/MRT relaxation, push h, g
-// The stencil passes (P2, P3, P4) run one CTA per brick. Its prologue reads
-// the brick's precomputed record (neighbour-brick ids and per-axis tile
-// tables, built on the host) and the occupancy words of the neighbour bricks
-// into shared memory; from those it resolves the site index of every tile
-// position (brick + halo) without further global traffic, stages the stencil
-// fields into shared-memory tiles (solid positions hold NaN, so one load gives
-// value and occupancy), then runs one thread per fluid site of the brick. All
-// stencil case logic (central / one-sided / biased, halfway bounce-back,
-// wetting) is derived from tile occupancy with selects, so no per-site tables
-// are read from HBM. P1 and the state transfers touch only a site's own
-// populations and run over flat chunks of CHUNK sites.
+// The stencil passes (P2, P3, P4) run one CTA per brick. The stencil fields
+// live on a dense node grid (solid nodes NaN, periodic images around it), so
+// a brick's field tile (brick + halo) is one box of the grid: one thread
+// issues the box copies (TMA, cp.async.bulk.tensor) and a bulk copy of the
+// brick's slot list, all completing on one mbarrier, and the CTA waits for
+// them once; solid positions arrive as NaN, so one load gives value and
+// occupancy. Then one thread per fluid site of the brick. All stencil case
+// logic (central / one-sided / biased, halfway bounce-back, wetting) is
+// derived from tile occupancy with selects, so no per-site tables are read
+// from HBM. P1 and the state transfers touch only a site's own populations
+// and run over flat chunks of CHUNK sites; between the passes, k_ghost
+// refreshes the periodic images of the fields a pass wrote.
 //
 // Streaming is push, fused into P4: the post-collision value f*_k of site x
 // is written to slot k of x + e_k, or to slot opp(k) of x itself when x + e_k
@@ -32,6 +33,7 @@
 
 #include <cstdint>
 
+#include "bulk.cuh"
 #include "d3q19.hpp"
 #include "layout.hpp"
 #include "mrt.hpp"
@@ -205,6 +207,21 @@ struct Tile {
   }
 };
 
+// A field tile staged from the dense grid: halo H along y and z (z only for
+// 3-D bricks) and always 2 along x, so every box starts on a 16-byte
+// boundary of the grid. Same indexing as Tile (Tile<Sh, 2> is TileX<Sh, 2>).
+template <class Sh, int H>
+struct TileX {
+  static constexpr int TX = Sh::BX + 4, TY = Sh::BY + 2 * H, TZ = Sh::BZ + 2 * H * Sh::HZ;
+  static constexpr int N = TX * TY * TZ;
+  static constexpr int SY = TX, SZ = TX * TY;
+  __device__ static constexpr int off(int k) { return lat_cx(k) + SY * lat_cy(k) + SZ * lat_cz(k) * Sh::HZ; }
+  __device__ static __forceinline__ int pos(int s) {
+    const int lx = s & (Sh::BX - 1), ly = (s >> Sh::LBX) & (Sh::BY - 1), lz = s >> (Sh::LBX + Sh::LBY);
+    return (lx + 2) + SY * (ly + H) + SZ * (lz + H * Sh::HZ);
+  }
+};
+
 // Prologue state in shared memory (static part).
 template <class Sh>
 struct Pro {
@@ -328,56 +345,85 @@ struct IdxTile {
 };
 
 // Per-CTA head of the stencil passes: the brick's fluid slots in site order,
-// its site range and the step scalars.
+// its site range, brick coordinates and the step scalars.
 template <class Sh>
 struct alignas(16) Head {
   uint16_t slot_of[Sh::C];
   double lambda;
   double ff;  // forcing factor in double: narrowed to the arithmetic type where used
   int first, cnt;
+  int bx, by, bz;
 };
 
-// The brick's head and its halo-H site-index tile, precomputed once by
-// k_build_tiles (the geometry is static), in one phase of independent
-// coalesced loads; ends with a barrier. s_idx must be 16-byte aligned.
-template <class Sh, int H, int NT = CTA, bool SCALARS = true>
-__device__ __forceinline__ void load_brick(const LatDesc& D, int brick, Head<Sh>& s, int32_t* __restrict__ s_idx) {
-  using T = Tile<Sh, H>;
-  static_assert(T::N % 4 == 0 && Sh::C % 8 == 0, "16-byte rows");
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    s.first = __ldg(&D.rec[brick].first);
-    s.cnt = __ldg(&D.rec[brick].cnt);
-  }
-  if (SCALARS && tid == NT - 1) load_step_scalars(D, s);
-  const int4* src = reinterpret_cast<const int4*>(H == 2 ? D.tile2 : D.tile1) + (int64_t)brick * (T::N / 4);
-  int4* dst = reinterpret_cast<int4*>(s_idx);
-  for (int q = tid; q < T::N / 4; q += NT) dst[q] = __ldg(src + q);
-  const uint4* ss = reinterpret_cast<const uint4*>(D.slots) + (int64_t)brick * (Sh::C / 8);
-  uint4* sd = reinterpret_cast<uint4*>(s.slot_of);
-  for (int q = tid; q < Sh::C / 8; q += NT) sd[q] = __ldg(ss + q);
-  __syncthreads();
+// Grid entry of slot `slot` of the brick at brick coordinates (bx, by, bz).
+template <class Sh>
+__device__ __forceinline__ int64_t grid_entry(const LatDesc& D, int bx, int by, int bz, int slot) {
+  const int x = bx * Sh::BX + (slot & (Sh::BX - 1)) + 2;
+  const int y = by * Sh::BY + ((slot >> Sh::LBX) & (Sh::BY - 1)) + 2;
+  const int z = bz * Sh::BZ + (slot >> (Sh::LBX + Sh::LBY)) + 2 * D.hz;
+  return x + D.gsy * y + D.gsz * z;
 }
 
-// Setup: the site-index tiles (halo 2 and halo 1) and the slot list of every
-// brick, from the occupancy words; one CTA per brick, run once per lattice.
+// The tensor map `id` of the lattice (a CUtensorMap in device memory).
+__device__ __forceinline__ const void* tmap_of(const LatDesc& D, int id) {
+  return static_cast<const char*>(D.tmap) + 128 * id;
+}
+
+// Box copy of the halo-H tile of brick (bx, by, bz) from a stencil-field
+// grid into shared memory (x0 = bx * BX: 16-byte aligned for the 4- and
+// 8-byte fields).
+template <class Sh, int H>
+__device__ __forceinline__ void tile_copy(void* dst, const LatDesc& D, int id, int bx, int by, int bz,
+                                          uint64_t* bar) {
+  tma_box3(dst, tmap_of(D, id), bx * Sh::BX, by * Sh::BY + 2 - H, D.hz ? bz * Sh::BZ + 2 - H : 0, bar);
+}
+
+// A stencil pass's prologue: thread 0 sets up the transaction barrier and
+// the whole CTA passes a block barrier (no thread polls it before), then
+// thread 0 reads the brick's head and issues the slot-list copy and the
+// caller's tile copies (their bytes in `tile_bytes`) on that barrier.
+__device__ __forceinline__ void head_init(uint64_t* bar) {
+  if (threadIdx.x == 0) mbar_init(bar);
+  __syncthreads();
+}
+template <class Sh>
+__device__ __forceinline__ void head_begin(const LatDesc& D, int brick, Head<Sh>& s, uint64_t* bar, uint32_t tile_bytes) {
+  s.first = __ldg(&D.rec[brick].first);
+  s.cnt = __ldg(&D.rec[brick].cnt);
+  s.bx = __ldg(&D.brick_xyz[3 * brick + 0]);
+  s.by = __ldg(&D.brick_xyz[3 * brick + 1]);
+  s.bz = __ldg(&D.brick_xyz[3 * brick + 2]);
+  mbar_arrive_expect_tx(bar, tile_bytes + (uint32_t)(Sh::C * sizeof(uint16_t)));
+  bulk_g2s(s.slot_of, D.slots + (int64_t)brick * Sh::C, (uint32_t)(Sh::C * sizeof(uint16_t)), bar);
+}
+
+// Every thread waits for the prologue's copies (bounded). False in every
+// thread of the CTA when any thread's wait ran out: the CTA then computes
+// nothing and the control block's status records it.
+__device__ __forceinline__ bool head_wait(const LatDesc& D, uint64_t* bar) {
+  const bool ok = mbar_wait(bar, 0, 1 << 22);
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) atomicOr(&D.ctl->status, 4);
+    return false;
+  }
+  return true;
+}
+
+// Setup: the halo-1 site-index tile (the collide pass's push targets) and
+// the slot list of every brick, from the occupancy words; one CTA per brick,
+// run once per lattice.
 template <class Sh>
 __global__ void __launch_bounds__(CTA) k_build_tiles(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
-  using T2 = Tile<Sh, 2>;
   using T1 = Tile<Sh, 1>;
   __shared__ Pro<Sh> s;
-  __shared__ IdxTile<Sh, 2> t2;
   __shared__ IdxTile<Sh, 1> t1;
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
   const int brick = wk.y;
   prologue<Sh, CTA, false>(D, brick, s);
-  build_idx_tile<Sh, 2>(s, t2.idx, t2.rbits, t2.rbase);
   build_idx_tile<Sh, 1>(s, t1.idx, t1.rbits, t1.rbase);
-  int32_t* g2 = const_cast<int32_t*>(D.tile2) + (int64_t)brick * T2::N;
   int32_t* g1 = const_cast<int32_t*>(D.tile1) + (int64_t)brick * T1::N;
   uint16_t* gs = const_cast<uint16_t*>(D.slots) + (int64_t)brick * Sh::C;
-  for (int t = threadIdx.x; t < T2::N; t += CTA) g2[t] = t2.idx[t];
   for (int t = threadIdx.x; t < T1::N; t += CTA) g1[t] = t1.idx[t];
   for (int r = threadIdx.x; r < Sh::C; r += CTA) gs[r] = r < s.rec.cnt ? s.slot_of[r] : (uint16_t)0;
 }
@@ -510,8 +556,9 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
       if (lat_cy(k)) jy += R(lat_cy(k)) * gv[k];
       if (lat_cz(k)) jz += R(lat_cz(k)) * gv[k];
     }
-    fc[i] = (F)c;
-    fp[i] = (F)p;
+    const int64_t di = __ldg(&D.dense_of[i]);
+    fc[di] = (F)c;
+    fp[di] = (F)p;
     if (write_j) {  // read only by P2's pressure correction (drho != 0), the
       fjx[i] = (F)jx;  // open-boundary kernels and field downloads (need_j | forced)
       fjy[i] = (F)jy;
@@ -549,43 +596,14 @@ __device__ __forceinline__ R corr_c(R c, double lambda) {
   return phi > 0.0 ? (R)(cd - lambda * phi) : c;
 }
 
-// Stage NF fields into halo-H tiles (NaN at solid positions); field 0 is the
-// order parameter when `correct` (corrected on the fly). Every thread first
-// reads the site indices of all its positions, then issues all its gathers
-// before the first use, so a CTA waits for one round of L2/HBM latency instead
-// of one per position. The fields are read-only for the kernel (__ldg).
-// With IL, fields 0 and 1 go to one interleaved tile (dst[1] = dst[0] + 1,
-// stride 2), read back as two-lane pairs.
-template <class Sh, int H, int NF, int NT = CTA, bool IL = false, class R, class F>
-__device__ __forceinline__ void stage(const F* const (&src)[NF], R* const (&dst)[NF], bool correct, double lambda,
-                                      const int32_t* __restrict__ s_idx) {
-  using T = Tile<Sh, H>;
-  constexpr int PER = (T::N + NT - 1) / NT;
-  int j[PER];
-#pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int t = threadIdx.x + u * NT;
-    j[u] = (t < T::N) ? s_idx[t] : -1;
-  }
-  F v[PER][NF];
-#pragma unroll
-  for (int u = 0; u < PER; ++u)
-#pragma unroll
-    for (int f = 0; f < NF; ++f) v[u][f] = j[u] >= 0 ? __ldg(src[f] + j[u]) : F(0);
-#pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int t = threadIdx.x + u * NT;
-    if (t < T::N) {
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        R x = nan_v<R>();
-        if (j[u] >= 0) {
-          x = (R)v[u][f];
-          if (f == 0 && correct) x = corr_c<R>(x, lambda);
-        }
-        dst[f][(IL && f < 2) ? 2 * t : t] = x;
-      }
-    }
+// Apply a queued mass correction to a staged order-parameter tile (solid
+// positions stay NaN); every thread its strided positions.
+template <int N, int NT, class R>
+__device__ __forceinline__ void correct_tile(R* __restrict__ t, double lambda) {
+  if (lambda == 0.0) return;
+  for (int q = threadIdx.x; q < N; q += NT) {
+    const R x = t[q];
+    if (is_site(x)) t[q] = corr_c<R>(x, lambda);
   }
 }
 
@@ -725,18 +743,20 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
                                                  FieldOut out) {
   using R = typename S::real;
   using F = typename S::fld;
-  using T = Tile<Sh, 1>;
+  using T = TileX<Sh, 1>;
   __shared__ Head<Sh> s;
-  __shared__ __align__(16) int32_t s_idx[T::N];
-  __shared__ R s_c[T::N];
+  __shared__ uint64_t s_bar;
+  __shared__ __align__(128) F s_c[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  load_brick<Sh, 1>(D, wk.y, s, s_idx);
-  {
-    const F* const src[1] = {static_cast<const F*>(D.c)};
-    R* const dst[1] = {s_c};
-    stage<Sh, 1, 1>(src, dst, true, s.lambda, s_idx);
+  head_init(&s_bar);
+  if (threadIdx.x == 0) {
+    head_begin<Sh>(D, wk.y, s, &s_bar, (uint32_t)sizeof(s_c));
+    tile_copy<Sh, 1>(s_c, D, TM_C1, s.bx, s.by, s.bz, &s_bar);
   }
+  if (threadIdx.x == CTA - 1) load_step_scalars(D, s);
+  if (!head_wait(D, &s_bar)) return;
+  correct_tile<T::N, CTA>(s_c, s.lambda);
   __syncthreads();
   const DevPrm& Pm = D.prm;
   const R alpha = R(ALPHA), cs2 = R(CS2);
@@ -750,17 +770,19 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   const int first = s.first, cnt = s.cnt;
   for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int64_t i = first + r;
-    const int pos = T::pos(s.slot_of[r]);
-    const R c0 = s_c[pos];
+    const int slot = s.slot_of[r];
+    const int pos = T::pos(slot);
+    const int64_t di = grid_entry<Sh>(D, s.bx, s.by, s.bz, slot);
+    const R c0 = (R)s_c[pos];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
     if (flag & BC_SITE) {
       if (OUT) {
-        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, s.slot_of[r]) : (int64_t)D.ref_of[i];
+        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, slot) : (int64_t)D.ref_of[i];
         const F* ub = static_cast<const F*>(D.u_bc);
         out.put(q, (double)c0, (double)(rho1 + drho * c0), (double)ub[i], (double)ub[D.n + i],
-                (double)ub[2 * D.n + i], (double)fp[i], (double) static_cast<const F*>(D.mu)[i]);
+                (double)ub[2 * D.n + i], (double)fp[di], (double)fmu[di]);
       } else if (D.snap_u[0]) {
-        const int64_t q = node_of<Sh>(D, wk.y, s.slot_of[r]);
+        const int64_t q = node_of<Sh>(D, wk.y, slot);
         const F* ub = static_cast<const F*>(D.u_bc);
         D.snap_u[0][q] = (double)ub[i];
         D.snap_u[1][q] = (double)ub[D.n + i];
@@ -775,7 +797,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     R gx = 0, gy = 0, gz = 0, lap = 0;
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
-      const R cm = s_c[pos - T::off(k)], cp = s_c[pos + T::off(k)];
+      const R cm = (R)s_c[pos - T::off(k)], cp = (R)s_c[pos + T::off(k)];
       const R aw2 = R(2) * alpha * weight<R>(k);
       const bool sm = is_site(cm), sp = is_site(cp);
       const R cdv = cd_sel<HBB>(c0, cm, cp, sm, sp);
@@ -786,7 +808,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     }
     const R rho = rho1 + drho * c0;
     const R mu = four_beta * (c0 * (R(1) - c0)) * (R(0.5) - c0) + (-kappa * lap);
-    fmu[i] = (F)mu;
+    fmu[di] = (F)mu;
     // the correction changes p only through drho (k_vel_press_corr :194-195);
     // u is needed here only for that, for output, or for the tracers' snapshot
     if (Pm.drho != 0.0 || OUT || D.snap_u[0]) {
@@ -796,13 +818,13 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
       const R ux = (R)fjx[i] * inv + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff * irho + mor * gx);
       const R uy = (R)fjy[i] * inv + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff * irho + mor * gy);
       const R uz = (R)fjz[i] * inv + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff * irho + mor * gz);
-      const R p = (R)fp[i] + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
-      if (Pm.drho != 0.0) fp[i] = (F)p;
+      const R p = (R)fp[di] + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
+      if (Pm.drho != 0.0) fp[di] = (F)p;
       if (OUT) {
-        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, s.slot_of[r]) : (int64_t)D.ref_of[i];
+        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, slot) : (int64_t)D.ref_of[i];
         out.put(q, (double)c0, (double)rho, (double)ux, (double)uy, (double)uz, (double)p, (double)mu);
       } else if (D.snap_u[0]) {
-        const int64_t q = node_of<Sh>(D, wk.y, s.slot_of[r]);
+        const int64_t q = node_of<Sh>(D, wk.y, slot);
         D.snap_u[0][q] = (double)ux;
         D.snap_u[1][q] = (double)uy;
         D.snap_u[2][q] = (double)uz;
@@ -820,32 +842,32 @@ template <class S, class Sh, bool HBB>
 __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
   using R = typename S::real;
   using F = typename S::fld;
-  using T = Tile<Sh, 1>;
+  using T = TileX<Sh, 1>;
   __shared__ Head<Sh> s;
-  __shared__ __align__(16) int32_t s_idx[T::N];
-  __shared__ R s_m[T::N];
+  __shared__ uint64_t s_bar;
+  __shared__ __align__(128) F s_m[T::N];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  load_brick<Sh, 1, CTA, false>(D, wk.y, s, s_idx);
-  {
-    const F* const src[1] = {static_cast<const F*>(D.mu)};
-    R* const dst[1] = {s_m};
-    stage<Sh, 1, 1>(src, dst, false, 0.0, s_idx);
+  head_init(&s_bar);
+  if (threadIdx.x == 0) {
+    head_begin<Sh>(D, wk.y, s, &s_bar, (uint32_t)sizeof(s_m));
+    tile_copy<Sh, 1>(s_m, D, TM_MU1, s.bx, s.by, s.bz, &s_bar);
   }
-  __syncthreads();
+  if (!head_wait(D, &s_bar)) return;
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
-  const int first = s.first, cnt = s.cnt;
+  const int cnt = s.cnt;
   for (int r = threadIdx.x; r < cnt; r += CTA) {
-    const int pos = T::pos(s.slot_of[r]);
-    const R m0 = s_m[pos];
+    const int slot = s.slot_of[r];
+    const int pos = T::pos(slot);
+    const R m0 = (R)s_m[pos];
     R lap = 0;
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
-      const R mm = s_m[pos - T::off(k)], mp = s_m[pos + T::off(k)];
+      const R mm = (R)s_m[pos - T::off(k)], mp = (R)s_m[pos + T::off(k)];
       lap += R(2) * alpha * weight<R>(k) * lap_sel<HBB>(m0, mm, mp, R(0), is_site(mm), is_site(mp));
     }
-    flm[first + r] = (F)lap;
+    flm[grid_entry<Sh>(D, s.bx, s.by, s.bz, slot)] = (F)lap;
   }
 }
 
@@ -900,10 +922,11 @@ __global__ void k_bc_fields(const LatDesc* __restrict__ descs, int lat) {
   if (j >= D.n_inlet + D.n_outlet) return;
   const bool inlet = j < D.n_inlet;
   const int64_t i = D.bc_list[j];
+  const int64_t di = D.dense_of[i];
   F* fc = static_cast<F*>(D.c);
   F* fp = static_cast<F*>(D.p);
   F* ubc = static_cast<F*>(D.u_bc);
-  const R c_raw = (R)fc[i];
+  const R c_raw = (R)fc[di];
   static_cast<F*>(D.c_raw_bc)[i] = (F)c_raw;
   const R rho_raw = (R)Pm.rho1 + (R)Pm.drho * c_raw;
   const R inv = R(1) / (R(CS2) * rho_raw);
@@ -912,15 +935,15 @@ __global__ void k_bc_fields(const LatDesc* __restrict__ descs, int lat) {
   R uz = (R) static_cast<const F*>(D.jz)[i] * inv;
   if (inlet) {
     if (Pm.use_in_vel) { ux = (R)Pm.u_in[0]; uy = (R)Pm.u_in[1]; uz = (R)Pm.u_in[2]; }
-    if (Pm.use_in_prs) fp[i] = (F)Pm.p_in;
+    if (Pm.use_in_prs) fp[di] = (F)Pm.p_in;
     if (Pm.use_in_fluid) {
       const double gate = inlet_gate(Pm, (unsigned)D.ctl->open_step, D.bc_coord ? D.bc_coord[j] : 0.0);
       const R cc = (R(1) - (R)Pm.inlet_c_a) + (R(2) * (R)Pm.inlet_c_a - R(1)) * (R)gate;
-      fc[i] = (F)cc;
+      fc[di] = (F)cc;
     }
   } else {
-    if (Pm.use_out_prs) fp[i] = (F)Pm.p_out;
-    if (Pm.use_out_fluid) fc[i] = (F)Pm.c_out_fixed;
+    if (Pm.use_out_prs) fp[di] = (F)Pm.p_out;
+    if (Pm.use_out_fluid) fc[di] = (F)Pm.c_out_fixed;
   }
   ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz;
 }
@@ -932,29 +955,22 @@ __global__ void k_bc_buffers(const LatDesc* __restrict__ descs, int lat) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= D.n_buf) return;
   const int64_t b = D.buf_verts[j], r = D.buf_refs[j];
+  const int64_t db = D.dense_of[b], dr = D.dense_of[r];
   F* fc = static_cast<F*>(D.c);
   F* fp = static_cast<F*>(D.p);
   F* ubc = static_cast<F*>(D.u_bc);
-  static_cast<F*>(D.c_raw_bc)[b] = fc[b];
-  fc[b] = fc[r];
-  fp[b] = fp[r];
+  static_cast<F*>(D.c_raw_bc)[b] = fc[db];
+  fc[db] = fc[dr];
+  fp[db] = fp[dr];
   ubc[b] = ubc[r]; ubc[D.n + b] = ubc[D.n + r]; ubc[2 * D.n + b] = ubc[2 * D.n + r];
 }
 
-// Site index of node (x, y, z) (periodic), -1 if solid: brick grid + occupancy.
-__device__ __forceinline__ int64_t site_at(const LatDesc& D, int x, int y, int z) {
+// Grid entry of node (x, y, z), periodic in each axis (solid nodes hold NaN).
+__device__ __forceinline__ int64_t grid_entry_node(const LatDesc& D, int x, int y, int z) {
   x = (x % D.nx + D.nx) % D.nx;
   y = (y % D.ny + D.ny) % D.ny;
   z = (z % D.nz + D.nz) % D.nz;
-  const int bx = x >> D.lbx, by = y >> D.lby, bz = z >> D.lbz;
-  const int id = D.brick_grid[((int64_t)bz * D.nby + by) * D.nbx + bx];
-  if (id < 0) return -1;
-  const int slot = (x & ((1 << D.lbx) - 1)) | ((y & ((1 << D.lby) - 1)) << D.lbx) |
-                   ((z & ((1 << D.lbz) - 1)) << (D.lbx + D.lby));
-  const int w = slot >> 6, b = slot & 63;
-  const uint64_t m = D.mask[(int64_t)id * D.words + w];
-  if (!((m >> b) & 1ull)) return -1;
-  return D.base[(int64_t)id * D.words + w] + __popcll(m & ((1ull << b) - 1ull));
+  return (x + 2) + D.gsy * (y + 2) + D.gsz * (z + 2 * D.hz);
 }
 
 // mu and the velocity/pressure correction of every boundary node, exactly as
@@ -969,18 +985,19 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= D.n_inlet + D.n_outlet + D.n_buf) return;
   const int64_t i = j < D.n_inlet + D.n_outlet ? D.bc_list[j] : D.buf_verts[j - D.n_inlet - D.n_outlet];
+  const int64_t di = D.dense_of[i];
   F* fc = static_cast<F*>(D.c);
   F* fp = static_cast<F*>(D.p);
   F* ubc = static_cast<F*>(D.u_bc);
   const int x = D.bc_xyz[3 * j], y = D.bc_xyz[3 * j + 1], z = D.bc_xyz[3 * j + 2];
-  const R c0 = (R)fc[i];
+  const R c0 = (R)fc[di];
   const R bnd = (R)Pm.bnd_coeff * c0 * (R(1) - c0);
   const bool hbb = Pm.hbb != 0;
   R gx = 0, gy = 0, gz = 0, lap = 0;
   for (int k = 1; k < Q; ++k) {
     const int ex = D.nx > 1 ? lat_cx(k) : 0, ey = D.ny > 1 ? lat_cy(k) : 0, ez = D.nz > 1 ? lat_cz(k) : 0;
-    const int64_t im = site_at(D, x - ex, y - ey, z - ez), ip = site_at(D, x + ex, y + ey, z + ez);
-    const R cm = im >= 0 ? (R)fc[im] : nan_v<R>(), cp = ip >= 0 ? (R)fc[ip] : nan_v<R>();
+    const R cm = (R)fc[grid_entry_node(D, x - ex, y - ey, z - ez)];
+    const R cp = (R)fc[grid_entry_node(D, x + ex, y + ey, z + ez)];
     const R aw = R(ALPHA) * weight<R>(k);
     const R cdv = cd_val(c0, cm, cp, hbb);
     gx += aw * R(lat_cx(k)) * cdv;
@@ -990,7 +1007,7 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
   }
   const R craw = (R) static_cast<const F*>(D.c_raw_bc)[i];
   const R mu = (R)Pm.four_beta * (craw * (R(1) - craw)) * (R(0.5) - craw) + (-(R)Pm.kappa * lap);
-  static_cast<F*>(D.mu)[i] = (F)mu;
+  static_cast<F*>(D.mu)[di] = (F)mu;
   if (D.bcflag[i] & BC_PROC) return;
   const R rho = (R)Pm.rho1 + (R)Pm.drho * c0;
   const R ff = (R)forcing_factor_dev(Pm, *D.ctl);
@@ -999,7 +1016,45 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
   const R uy = (R)ubc[D.n + i] + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff / rho + mor * gy);
   const R uz = (R)ubc[2 * D.n + i] + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
   ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz;
-  fp[i] = (F)((R)fp[i] + R(0.5) * ((R)Pm.drho * (ux * gx + uy * gy + uz * gz)) * R(CS2));
+  fp[di] = (F)((R)fp[di] + R(0.5) * ((R)Pm.drho * (ux * gx + uy * gy + uz * gz)) * R(CS2));
+}
+
+// ---------------------------------------------------------------------------
+// periodic images of the stencil-field grids
+// ---------------------------------------------------------------------------
+// Every grid entry outside the lattice (node coordinate outside [0, n) on an
+// axis) takes the value of the node it wraps to. One warp per grid row
+// (y, z): a row inside the lattice copies its x images, a row outside copies
+// the whole wrapped row. fields: bit 0 c, 1 p, 2 mu, 3 lap(mu). The sources
+// are lattice nodes, never images, so the order of the writes does not
+// matter. Work items: (lattice, first row / GHOST_ROWS).
+constexpr int GHOST_ROWS = CTA / 32;
+enum : int { GF_C = 1, GF_P = 2, GF_MU = 4, GF_LAPMU = 8 };
+template <class F>
+__global__ void __launch_bounds__(CTA) k_ghost(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                int fields) {
+  const int2 wk = work[blockIdx.x];
+  const LatDesc& D = descs[wk.x];
+  const int row = wk.y * GHOST_ROWS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (row >= D.gdy * D.gdz) return;
+  const int gy = row % D.gdy, gz = row / D.gdy;
+  const int y = gy - 2, z = gz - 2 * D.hz;
+  const int wy = (y % D.ny + D.ny) % D.ny, wz = (z % D.nz + D.nz) % D.nz;
+  const bool inside = y == wy && z == wz;
+  const int64_t dst_row = D.gsy * gy + D.gsz * gz;
+  const int64_t src_row = D.gsy * (wy + 2) + D.gsz * (wz + 2 * D.hz);
+  F* const f[4] = {static_cast<F*>(D.c), static_cast<F*>(D.p), static_cast<F*>(D.mu), static_cast<F*>(D.lapmu)};
+  // inside rows: entries gx in [0, 2) and [nx + 2, gdx); outside rows: all
+  const int n_lo = 2, n_hi = D.gdx - 2 - D.nx;
+  const int count = inside ? n_lo + n_hi : D.gdx;
+  for (int q = lane; q < count; q += 32) {
+    const int gx = inside ? (q < n_lo ? q : D.nx + 2 + (q - n_lo)) : q;
+    const int x = gx - 2;
+    const int wx = (x % D.nx + D.nx) % D.nx;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      if (fields & (1 << b)) f[b][dst_row + gx] = f[b][src_row + wx + 2];
+  }
 }
 
 // ---------------------------------------------------------------------------

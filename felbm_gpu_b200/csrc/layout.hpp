@@ -87,6 +87,11 @@ struct DevPrm {
   double c_ref, p_ref, h_scale, g_scale;
 };
 
+// The tensor maps of a lattice's stencil-field grids: the field and the
+// halo of the box (the x halo of every box is 2, so the box starts on a
+// 16-byte boundary).
+enum TensorMapId { TM_C1 = 0, TM_C2 = 1, TM_P2 = 2, TM_MU1 = 3, TM_L2 = 4, TM_N = 5 };
+
 // Per-site open-boundary flags (bcflag[i]).
 enum : uint8_t {
   BC_SITE = 1,      // fields imposed/copied: c_raw_bc, u_bc hold this site's values
@@ -110,13 +115,24 @@ struct LatDesc {
   const int32_t* brick_xyz;    // [nbricks][3]
   const BrickRec* rec;         // [nbricks]
   const int32_t* ref_of;       // site -> reference-order index
-  const int32_t* tile2;        // [nbricks][halo-2 tile] site index or -1 (k_build_tiles)
-  const int32_t* tile1;        // [nbricks][halo-1 tile]
+  const int32_t* tile1;        // [nbricks][halo-1 tile] site index or -1 (k_build_tiles)
   const uint16_t* slots;       // [nbricks][brick slots] fluid slots in site order
   // state: pop[buffer][0 = h, 1 = g]
   void* pop[2][2];
-  // fields (FP64 for FP64 storage, FP32 otherwise)
+  // fields (FP64 for FP64 storage, FP32 otherwise). The stencil fields c,
+  // p, mu and lap(mu) live on a dense node grid covering node coordinates
+  // [-2, nb * B + 2) per axis (z: [0, 1) without a z halo), x fastest; the
+  // positions outside [0, n) per axis hold the periodic image of the node
+  // they wrap to (filled by k_ghost after each pass that writes the field),
+  // solid nodes hold NaN. A brick's halo tile is then one box of the grid,
+  // loaded by one TMA copy. The momentum jx, jy, jz is per site.
   void *c, *p, *jx, *jy, *jz, *mu, *lapmu;
+  int gdx, gdy, gdz;           // grid extents (gdx a multiple of 16 bytes of entries)
+  int hz;                      // 1: the z axis has a halo (3-D bricks)
+  int64_t gsy, gsz;            // entry strides of y and z (x: 1)
+  const int32_t* dense_of;     // site -> grid entry of its node
+  const void* tmap;            // CUtensorMap[TM_N] of the stencil fields (64-byte aligned)
+  int ghost_blocks;            // CTAs of one k_ghost pass over the grid's rows
   // open boundary (null when off)
   const uint8_t* bcflag;
   const int32_t* bcsrc;

@@ -71,11 +71,14 @@ double pop_bytes(int storage) {
 size_t fld_bytes(int storage) { return storage == FE_F64 ? 8 : 4; }
 
 // Device bytes of one resident solve: two ping-pong buffers of h and g, the
-// seven per-site fields, the FP64 transfer buffer (upload/download), and the
-// site/brick tables (generous per-site bound).
-double footprint(int64_t n, int storage) {
-  const double per = 4.0 * 19 * pop_bytes(storage) + 7.0 * fld_bytes(storage) + 2.0 * 19 * 8 + 64;
-  return (double)n * per + (double)(64 << 20);
+// three per-site momentum fields, the four stencil fields on the node grid
+// (the lattice rounded up to bricks plus a two-node ring; bounded here by
+// 20 more nodes per axis), the FP64 transfer buffer (upload/download), and
+// the site/brick tables (generous per-site bound).
+double footprint(int64_t n, int nx, int ny, int nz, int storage) {
+  const double per = 4.0 * 19 * pop_bytes(storage) + 3.0 * fld_bytes(storage) + 2.0 * 19 * 8 + 64;
+  const double cells = (double)(nx + 20) * (double)(ny + 20) * (double)(nz == 1 ? 1 : nz + 20);
+  return (double)n * per + 4.0 * cells * (double)fld_bytes(storage) + (double)(64 << 20);
 }
 
 double percentile(std::vector<double> v, double q) {
@@ -233,9 +236,9 @@ struct fe_server {
     }
   }
 
-  bool fits(int64_t sites) {  // under mu
+  bool fits(const Req& q) {  // under mu
     if (cfg.max_active > 0 && holding >= cfg.max_active) return false;
-    const double need = footprint(sites, cfg.storage);
+    const double need = footprint(q.sites, q.r.nx, q.r.ny, q.r.nz, cfg.storage);
     if (committed + need > budget) return false;
     size_t fr = 0, tot = 0;  // memory other users took since the server started
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
@@ -252,7 +255,7 @@ struct fe_server {
       // with nothing held, the oldest solve is admitted even if its estimate
       // exceeds the budget: engine creation then reports an out-of-memory
       // failure for it instead of a queue that never moves
-      if (!fits(queue.front().sites) && holding > 0) return;
+      if (!fits(queue.front()) && holding > 0) return;
       Live L;
       L.q = std::move(queue.front());
       queue.pop_front();
@@ -260,7 +263,7 @@ struct fe_server {
       ++active;
       peak_active = std::max(peak_active, active);
       L.t_admit = now();
-      L.bytes = footprint(L.q.sites, cfg.storage);
+      L.bytes = footprint(L.q.sites, L.q.r.nx, L.q.r.ny, L.q.r.nz, cfg.storage);
       committed += L.bytes;
       ++holding;
       to_create.push_back(std::move(L));
@@ -355,7 +358,7 @@ struct fe_server {
           if (queue.empty() && to_create.empty() && to_read.empty() && active == 0) cv_idle.notify_all();
           cv.wait(g, [&] {
             return stop || !created.empty() || !to_free.empty() ||
-                   (!queue.empty() && queue.front().ready && (holding == 0 || fits(queue.front().sites)));
+                   (!queue.empty() && queue.front().ready && (holding == 0 || fits(queue.front())));
           });
           continue;
         }
