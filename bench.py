@@ -65,7 +65,7 @@ def parse():
                     help="skip the layout autotuner (default bricks, two steps per graph launch)")
     ap.add_argument("--brick", default="auto", choices=["auto", "8x8x8", "8x8x4", "16x8x8"],
                     help="force a brick shape (skips the autotuner)")
-    ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per solve of the 64-solve sweep")
+    ap.add_argument("--sweep-steps", type=int, default=5000, help="steps per solve of the 64-solve sweep")
     ap.add_argument("--stream-seconds", type=float, default=15.0, help="arrival window of the request stream")
     ap.add_argument("--stream-rate", type=float, default=4.0, help="Poisson arrival rate (requests / s)")
     ap.add_argument("--e2e-steps", type=int, default=500,
