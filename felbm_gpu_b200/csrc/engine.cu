@@ -302,7 +302,6 @@ struct Engine {
   LatDesc* d_desc = nullptr;
   int2* d_work = nullptr;   // (lattice, brick) of the stencil passes
   int2* d_cwork = nullptr;  // (lattice, chunk) of the flat passes
-  int2* d_ghwork = nullptr; // (lattice, row block) of the grid-image refresh
   Ctl* d_ctl = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
@@ -506,7 +505,7 @@ struct Engine {
         D.pop[b][f] = q;
       }
     // momentum per site; the stencil fields on the dense node grid, NaN
-    // everywhere until the passes write the fluid nodes and their images
+    // everywhere until the passes write the fluid nodes
     for (void** f : {&D.jx, &D.jy, &D.jz}) {
       unsigned char* q;
       if ((rc = alloc(&q, (size_t)D.n * fld_size()))) return rc;
@@ -562,7 +561,7 @@ struct Engine {
 
   // The dense node grids of c, p, mu, lap(mu) (node coordinates [-2, nb B + 2)
   // per axis; z only for 3-D bricks), the site -> grid entry table, the
-  // tensor maps of their halo boxes and the row blocks of k_ghost.
+  // tensor maps of their halo boxes.
   int setup_grid() {
     LatDesc& D = hd;
     const int B[3] = {1 << L.lb[0], 1 << L.lb[1], 1 << L.lb[2]};
@@ -592,11 +591,6 @@ struct Engine {
     int rc;
     if ((rc = upload_vec(&dd, dense))) return rc;
     D.dense_of = dd;
-    const int rows = D.gdy * D.gdz;
-    D.ghost_blocks = (rows + GHOST_ROWS - 1) / GHOST_ROWS;
-    std::vector<int2> gw(D.ghost_blocks);
-    for (int b = 0; b < D.ghost_blocks; ++b) gw[b] = make_int2(0, b);
-    if ((rc = upload_vec(&d_ghwork, gw))) return rc;
     FE_DISPATCH(*this, rc = build_tmaps<S FE_COMMA Sh>());
     return rc;
   }
@@ -654,30 +648,26 @@ struct Engine {
   void launch_step_t(int par, cudaStream_t st, cudaEvent_t* ev) {
     const int nb = hd.nbricks;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
-    using F = typename S::fld;
     rec(0);
     k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
-    k_ghost<F><<<hd.ghost_blocks, CTA, 0, st>>>(d_desc, d_ghwork, GF_C | GF_P);
     rec(2);
     if (hd.prm.hbb) k_cfield<S, Sh, 0, true><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
     else k_cfield<S, Sh, 0, false><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
-    k_ghost<F><<<hd.ghost_blocks, CTA, 0, st>>>(d_desc, d_ghwork, GF_MU | GF_P);
     rec(3);
     if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
     else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
-    k_ghost<F><<<hd.ghost_blocks, CTA, 0, st>>>(d_desc, d_ghwork, GF_LAPMU);
     rec(4);
     launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
-    launches += 7;
+    launches += 4;
   }
   void launch_step(int par, cudaStream_t st, cudaEvent_t* ev = nullptr) {
     FE_DISPATCH(*this, launch_step_t<S FE_COMMA Sh>(par, st, ev));
   }
   int kernels_per_step() const {
-    int k = 7;  // four passes and three grid-image refreshes
+    int k = 4;
     if (open_bnd) {
       const int nio = hd.n_inlet + hd.n_outlet;
       k += (nio ? 1 : 0) + (hd.n_buf ? 1 : 0) + (nio + hd.n_buf ? 1 : 0);
@@ -924,10 +914,9 @@ struct Engine {
   void fields_launch(FieldOut o) {
     k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
-    k_ghost<typename S::fld><<<hd.ghost_blocks, CTA, 0, stream>>>(d_desc, d_ghwork, GF_C | GF_P);
     if (hd.prm.hbb) k_cfield<S, Sh, OUT, true><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     else k_cfield<S, Sh, OUT, false><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
-    launches += 3;
+    launches += 2;
   }
   // Corrected velocity of the current state into node-indexed device grids
   // (solid nodes are left as they are), on the engine stream.
@@ -1006,9 +995,8 @@ struct Batch {
   LatDesc* d_desc = nullptr;
   int2* d_cwork = nullptr;
   int2* d_gwork = nullptr;          // the groups' work lists, one after another
-  int2* d_hwork = nullptr;          // the members' grid-image row blocks
-  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0, cap_hwork = 0;  // bytes (grow-only)
-  int ncwork = 0, nhwork = 0;
+  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0;  // bytes (grow-only)
+  int ncwork = 0;
   int64_t since_build = 0;          // steps since the last rebuild
   bool dirty = true;
   int64_t same_members = 0;  // launches since the last membership change
@@ -1028,13 +1016,13 @@ struct Batch {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_arrays() {
-    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork, (void*)d_hwork})
+    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork})
       if (a) cudaFree(a);
     groups.clear();
     d_desc = nullptr;
-    d_cwork = d_gwork = d_hwork = nullptr;
-    cap_desc = cap_cwork = cap_gwork = cap_hwork = 0;
-    ncwork = nhwork = 0;
+    d_cwork = d_gwork = nullptr;
+    cap_desc = cap_cwork = cap_gwork = 0;
+    ncwork = 0;
   }
   void drop_graphs() {
     for (int p = 0; p < 2; ++p) {
@@ -1123,7 +1111,7 @@ struct Batch {
     since_build = 0;
     join_parity.assign(mem.size(), 0);
     std::vector<LatDesc> descs(mem.size());
-    std::vector<int2> cw, hw;
+    std::vector<int2> cw;
     int rc;
     for (size_t q = 0; q < mem.size(); ++q) {
       Engine* e = mem[q];
@@ -1136,7 +1124,6 @@ struct Batch {
       }
       descs[q] = d;
       for (int c = 0; c < d.nchunks; ++c) cw.push_back(make_int2((int)q, c));
-      for (int b = 0; b < d.ghost_blocks; ++b) hw.push_back(make_int2((int)q, b));
       if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;  // queued correction, forcing from t
     }
     std::vector<int2> gw;
@@ -1166,9 +1153,7 @@ struct Batch {
     for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
     if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
     if ((rc = upload_vec(&d_cwork, &cap_cwork, cw))) return rc;
-    if ((rc = upload_vec(&d_hwork, &cap_hwork, hw))) return rc;
     ncwork = (int)cw.size();
-    nhwork = (int)hw.size();
     dirty = false;
     return FE_OK;
   }
@@ -1199,14 +1184,10 @@ struct Batch {
       if (nb) k_bc_buffers<S><<<(nb + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
       if (nall) k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
     }
-    using F = typename S::fld;
-    k_ghost<F><<<nhwork, CTA, 0, st>>>(d_desc, d_hwork, GF_C | GF_P);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p2<S, typename decltype(t)::type>(g, st); });
-    k_ghost<F><<<nhwork, CTA, 0, st>>>(d_desc, d_hwork, GF_MU | GF_P);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p3<S, typename decltype(t)::type>(g, st); });
-    k_ghost<F><<<nhwork, CTA, 0, st>>>(d_desc, d_hwork, GF_LAPMU);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p4<S, typename decltype(t)::type>(g, par, st); });
   }
@@ -1222,7 +1203,7 @@ struct Batch {
   }
   // kernels of one step, the count launch_step_t makes
   int64_t launches_per_step() const {
-    int64_t k = 4 + 3 * (int64_t)groups.size();
+    int64_t k = 1 + 3 * (int64_t)groups.size();
     for (const Engine* e : mem)
       if (e->open_bnd) {
         const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf;

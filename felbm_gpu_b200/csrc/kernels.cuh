@@ -11,7 +11,7 @@
 //   P4 k_collide  c, p stencils to distance 2, lap(mu) to distance 1, own g:
 //                 equilibria + Guo force + BGK/MRT relaxation, push h, g
 // The stencil passes (P2, P3, P4) run one CTA per brick. The stencil fields
-// live on a dense node grid (solid nodes NaN, periodic images around it), so
+// live on a dense node grid (solid nodes NaN), so
 // a brick's field tile (brick + halo) is one box of the grid: one thread
 // issues the box copies (TMA, cp.async.bulk.tensor) and a bulk copy of the
 // brick's slot list, all completing on one mbarrier, and the CTA waits for
@@ -20,8 +20,9 @@
 // logic (central / one-sided / biased, halfway bounce-back, wetting) is
 // derived from tile occupancy with selects, so no per-site tables are read
 // from HBM. P1 and the state transfers touch only a site's own populations
-// and run over flat chunks of CHUNK sites; between the passes, k_ghost
-// refreshes the periodic images of the fields a pass wrote.
+// and run over flat chunks of CHUNK sites. The grid holds each node once; a
+// brick whose halo reaches past a face of the lattice fills those tile
+// positions from the nodes they wrap to after its copies land.
 //
 // Streaming is push, fused into P4: the post-collision value f*_k of site x
 // is written to slot k of x + e_k, or to slot opp(k) of x itself when x + e_k
@@ -364,6 +365,41 @@ __device__ __forceinline__ int64_t grid_entry(const LatDesc& D, int bx, int by, 
   return x + D.gsy * y + D.gsz * z;
 }
 
+// Node coordinates of slot `slot` of the brick at (bx, by, bz).
+template <class Sh>
+__device__ __forceinline__ void slot_node(int bx, int by, int bz, int slot, int& x, int& y, int& z) {
+  x = bx * Sh::BX + (slot & (Sh::BX - 1));
+  y = by * Sh::BY + ((slot >> Sh::LBX) & (Sh::BY - 1));
+  z = bz * Sh::BZ + (slot >> (Sh::LBX + Sh::LBY));
+}
+
+__device__ __forceinline__ int wrap_coord(int c, int n) {
+  c %= n;
+  return c < 0 ? c + n : c;
+}
+
+// Tile positions of a halo tile (TileX<Sh, H>) whose node lies outside the
+// lattice on some axis (a halo that reaches past a face, or slots beyond the
+// lattice's extent) take the value of the node they wrap to, read from the
+// grid: the grid holds each node once, so only bricks at a face need this.
+// NF fields, tile t[f] from grid g[f]; every thread its strided positions.
+template <class Sh, int H, int NF, int NT, class F>
+__device__ __forceinline__ void wrap_tile(const LatDesc& D, int bx, int by, int bz, F* const (&t)[NF],
+                                          const F* const (&g)[NF]) {
+  using T = TileX<Sh, H>;
+  const int x0 = bx * Sh::BX - 2, y0 = by * Sh::BY - H, z0 = Sh::HZ ? bz * Sh::BZ - H : 0;
+  if (x0 >= 0 && x0 + T::TX <= D.nx && y0 >= 0 && y0 + T::TY <= D.ny && z0 >= 0 && z0 + T::TZ <= D.nz) return;
+  for (int q = threadIdx.x; q < T::N; q += NT) {
+    const int tx = q % T::TX, ty = (q / T::TX) % T::TY, tz = q / (T::TX * T::TY);
+    const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
+    if (x >= 0 && x < D.nx && y >= 0 && y < D.ny && z >= 0 && z < D.nz) continue;
+    const int64_t e = (wrap_coord(x, D.nx) + 2) + D.gsy * (wrap_coord(y, D.ny) + 2) +
+                      D.gsz * (wrap_coord(z, D.nz) + 2 * D.hz);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) t[f][q] = g[f][e];
+  }
+}
+
 // The tensor map `id` of the lattice (a CUtensorMap in device memory).
 __device__ __forceinline__ const void* tmap_of(const LatDesc& D, int id) {
   return static_cast<const char*>(D.tmap) + 128 * id;
@@ -556,9 +592,9 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
       if (lat_cy(k)) jy += R(lat_cy(k)) * gv[k];
       if (lat_cz(k)) jz += R(lat_cz(k)) * gv[k];
     }
-    const int64_t di = __ldg(&D.dense_of[i]);
-    fc[di] = (F)c;
-    fp[di] = (F)p;
+    const int64_t de = __ldg(&D.dense_of[i]);
+    fc[de] = (F)c;
+    fp[de] = (F)p;
     if (write_j) {  // read only by P2's pressure correction (drho != 0), the
       fjx[i] = (F)jx;  // open-boundary kernels and field downloads (need_j | forced)
       fjy[i] = (F)jy;
@@ -756,6 +792,11 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   }
   if (threadIdx.x == CTA - 1) load_step_scalars(D, s);
   if (!head_wait(D, &s_bar)) return;
+  {
+    F* const tt[1] = {s_c};
+    const F* const gg[1] = {static_cast<const F*>(D.c)};
+    wrap_tile<Sh, 1, 1, CTA>(D, s.bx, s.by, s.bz, tt, gg);  // the same positions per thread as below
+  }
   correct_tile<T::N, CTA>(s_c, s.lambda);
   __syncthreads();
   const DevPrm& Pm = D.prm;
@@ -854,6 +895,12 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
     tile_copy<Sh, 1>(s_m, D, TM_MU1, s.bx, s.by, s.bz, &s_bar);
   }
   if (!head_wait(D, &s_bar)) return;
+  {
+    F* const tt[1] = {s_m};
+    const F* const gg[1] = {static_cast<const F*>(D.mu)};
+    wrap_tile<Sh, 1, 1, CTA>(D, s.bx, s.by, s.bz, tt, gg);
+    __syncthreads();
+  }
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
   const int cnt = s.cnt;
@@ -1017,44 +1064,6 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
   const R uz = (R)ubc[2 * D.n + i] + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
   ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz;
   fp[di] = (F)((R)fp[di] + R(0.5) * ((R)Pm.drho * (ux * gx + uy * gy + uz * gz)) * R(CS2));
-}
-
-// ---------------------------------------------------------------------------
-// periodic images of the stencil-field grids
-// ---------------------------------------------------------------------------
-// Every grid entry outside the lattice (node coordinate outside [0, n) on an
-// axis) takes the value of the node it wraps to. One warp per grid row
-// (y, z): a row inside the lattice copies its x images, a row outside copies
-// the whole wrapped row. fields: bit 0 c, 1 p, 2 mu, 3 lap(mu). The sources
-// are lattice nodes, never images, so the order of the writes does not
-// matter. Work items: (lattice, first row / GHOST_ROWS).
-constexpr int GHOST_ROWS = CTA / 32;
-enum : int { GF_C = 1, GF_P = 2, GF_MU = 4, GF_LAPMU = 8 };
-template <class F>
-__global__ void __launch_bounds__(CTA) k_ghost(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                int fields) {
-  const int2 wk = work[blockIdx.x];
-  const LatDesc& D = descs[wk.x];
-  const int row = wk.y * GHOST_ROWS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (row >= D.gdy * D.gdz) return;
-  const int gy = row % D.gdy, gz = row / D.gdy;
-  const int y = gy - 2, z = gz - 2 * D.hz;
-  const int wy = (y % D.ny + D.ny) % D.ny, wz = (z % D.nz + D.nz) % D.nz;
-  const bool inside = y == wy && z == wz;
-  const int64_t dst_row = D.gsy * gy + D.gsz * gz;
-  const int64_t src_row = D.gsy * (wy + 2) + D.gsz * (wz + 2 * D.hz);
-  F* const f[4] = {static_cast<F*>(D.c), static_cast<F*>(D.p), static_cast<F*>(D.mu), static_cast<F*>(D.lapmu)};
-  // inside rows: entries gx in [0, 2) and [nx + 2, gdx); outside rows: all
-  const int n_lo = 2, n_hi = D.gdx - 2 - D.nx;
-  const int count = inside ? n_lo + n_hi : D.gdx;
-  for (int q = lane; q < count; q += 32) {
-    const int gx = inside ? (q < n_lo ? q : D.nx + 2 + (q - n_lo)) : q;
-    const int x = gx - 2;
-    const int wx = (x % D.nx + D.nx) % D.nx;
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-      if (fields & (1 << b)) f[b][dst_row + gx] = f[b][src_row + wx + 2];
-  }
 }
 
 // ---------------------------------------------------------------------------
