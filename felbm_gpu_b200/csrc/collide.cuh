@@ -124,12 +124,6 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   }
   if (threadIdx.x == P4T - 1) load_step_scalars(D, s);
   if (!head_wait(D, &s_bar)) return;
-  {
-    F* const tt[3] = {raw_c, raw_p, s_l};
-    const F* const gg[3] = {static_cast<const F*>(D.c), static_cast<const F*>(D.p),
-                            static_cast<const F*>(D.lapmu)};
-    wrap_tile<Sh, 2, 3, P4T>(D, s.bx, s.by, s.bz, tt, gg);  // the same positions per thread as below
-  }
   // (c, p) pairs, with a queued mass correction applied to c
   {
     const double lam = s.lambda;

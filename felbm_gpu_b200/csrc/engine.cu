@@ -302,6 +302,7 @@ struct Engine {
   LatDesc* d_desc = nullptr;
   int2* d_work = nullptr;   // (lattice, brick) of the stencil passes
   int2* d_cwork = nullptr;  // (lattice, chunk) of the flat passes
+  int2* d_iwork = nullptr;  // (lattice, block) of the image refresh
   Ctl* d_ctl = nullptr;
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
@@ -512,7 +513,7 @@ struct Engine {
       FE_CUDA(cudaMemset(q, 0, (size_t)D.n * fld_size()));
       *f = q;
     }
-    if ((rc = setup_grid())) return rc;
+    if ((rc = setup_grid(solid))) return rc;
     if ((rc = alloc(&D.part1, (size_t)D.nchunks * 2))) return rc;
     if ((rc = alloc(&D.part4, (size_t)nbk * P4W * 6))) return rc;
     FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * P4W * 6 * 8));
@@ -561,8 +562,8 @@ struct Engine {
 
   // The dense node grids of c, p, mu, lap(mu) (node coordinates [-2, nb B + 2)
   // per axis; z only for 3-D bricks), the site -> grid entry table, the
-  // tensor maps of their halo boxes.
-  int setup_grid() {
+  // tensor maps of their halo boxes, and the image positions of fluid nodes.
+  int setup_grid(const uint8_t* solid_mask) {
     LatDesc& D = hd;
     const int B[3] = {1 << L.lb[0], 1 << L.lb[1], 1 << L.lb[2]};
     D.hz = L.shape2d ? 0 : 1;
@@ -591,6 +592,28 @@ struct Engine {
     int rc;
     if ((rc = upload_vec(&dd, dense))) return rc;
     D.dense_of = dd;
+    // image positions of fluid nodes: every grid position outside the
+    // lattice whose wrapped node is fluid
+    std::vector<int2> img;
+    const int zlo = D.hz ? -2 : 0, zhi = D.hz ? D.gdz - 2 : 1;
+    auto wrapc = [](int c, int n) { c %= n; return c < 0 ? c + n : c; };
+    for (int z = zlo; z < zhi; ++z)
+      for (int y = -2; y < D.gdy - 2; ++y)
+        for (int x = -2; x < D.gdx - 2; ++x) {
+          if (x >= 0 && x < D.nx && y >= 0 && y < D.ny && z >= 0 && z < D.nz) continue;
+          const int wx = wrapc(x, D.nx), wy = wrapc(y, D.ny), wz = wrapc(z, D.nz);
+          if (solid_mask[wx + (int64_t)D.nx * (wy + (int64_t)D.ny * wz)]) continue;
+          img.push_back(make_int2((int)((x + 2) + D.gsy * (y + 2) + D.gsz * (z + 2 * D.hz)),
+                                  (int)((wx + 2) + D.gsy * (wy + 2) + D.gsz * (wz + 2 * D.hz))));
+        }
+    int2* di;
+    if ((rc = upload_vec(&di, img))) return rc;
+    D.images = di;
+    D.n_images = (int64_t)img.size();
+    D.image_blocks = (int)((img.size() + IMG_BLOCK - 1) / IMG_BLOCK);
+    std::vector<int2> iw(std::max(D.image_blocks, 1));
+    for (int b = 0; b < D.image_blocks; ++b) iw[b] = make_int2(0, b);
+    if ((rc = upload_vec(&d_iwork, iw))) return rc;
     FE_DISPATCH(*this, rc = build_tmaps<S FE_COMMA Sh>());
     return rc;
   }
@@ -648,26 +671,30 @@ struct Engine {
   void launch_step_t(int par, cudaStream_t st, cudaEvent_t* ev) {
     const int nb = hd.nbricks;
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
+    using F = typename S::fld;
     rec(0);
     k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
+    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_C | GF_P);
     rec(2);
     if (hd.prm.hbb) k_cfield<S, Sh, 0, true><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
     else k_cfield<S, Sh, 0, false><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
+    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_P);
     rec(3);
     if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
     else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
+    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_LAPMU);
     rec(4);
     launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
     rec(5);
-    launches += 4;
+    launches += hd.image_blocks ? 7 : 4;
   }
   void launch_step(int par, cudaStream_t st, cudaEvent_t* ev = nullptr) {
     FE_DISPATCH(*this, launch_step_t<S FE_COMMA Sh>(par, st, ev));
   }
   int kernels_per_step() const {
-    int k = 4;
+    int k = hd.image_blocks ? 7 : 4;  // four passes (and three image refreshes)
     if (open_bnd) {
       const int nio = hd.n_inlet + hd.n_outlet;
       k += (nio ? 1 : 0) + (hd.n_buf ? 1 : 0) + (nio + hd.n_buf ? 1 : 0);
@@ -914,9 +941,11 @@ struct Engine {
   void fields_launch(FieldOut o) {
     k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
+    if (hd.image_blocks)
+      k_images<typename S::fld><<<hd.image_blocks, CTA, 0, stream>>>(d_desc, d_iwork, GF_C | GF_P);
     if (hd.prm.hbb) k_cfield<S, Sh, OUT, true><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     else k_cfield<S, Sh, OUT, false><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
-    launches += 2;
+    launches += hd.image_blocks ? 3 : 2;
   }
   // Corrected velocity of the current state into node-indexed device grids
   // (solid nodes are left as they are), on the engine stream.
@@ -995,8 +1024,9 @@ struct Batch {
   LatDesc* d_desc = nullptr;
   int2* d_cwork = nullptr;
   int2* d_gwork = nullptr;          // the groups' work lists, one after another
-  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0;  // bytes (grow-only)
-  int ncwork = 0;
+  int2* d_iwork = nullptr;          // the members' image-refresh blocks
+  size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0, cap_iwork = 0;  // bytes (grow-only)
+  int ncwork = 0, niwork = 0;
   int64_t since_build = 0;          // steps since the last rebuild
   bool dirty = true;
   int64_t same_members = 0;  // launches since the last membership change
@@ -1016,13 +1046,13 @@ struct Batch {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_arrays() {
-    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork})
+    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork, (void*)d_iwork})
       if (a) cudaFree(a);
     groups.clear();
     d_desc = nullptr;
-    d_cwork = d_gwork = nullptr;
-    cap_desc = cap_cwork = cap_gwork = 0;
-    ncwork = 0;
+    d_cwork = d_gwork = d_iwork = nullptr;
+    cap_desc = cap_cwork = cap_gwork = cap_iwork = 0;
+    ncwork = niwork = 0;
   }
   void drop_graphs() {
     for (int p = 0; p < 2; ++p) {
@@ -1111,7 +1141,7 @@ struct Batch {
     since_build = 0;
     join_parity.assign(mem.size(), 0);
     std::vector<LatDesc> descs(mem.size());
-    std::vector<int2> cw;
+    std::vector<int2> cw, iw;
     int rc;
     for (size_t q = 0; q < mem.size(); ++q) {
       Engine* e = mem[q];
@@ -1124,6 +1154,7 @@ struct Batch {
       }
       descs[q] = d;
       for (int c = 0; c < d.nchunks; ++c) cw.push_back(make_int2((int)q, c));
+      for (int b = 0; b < d.image_blocks; ++b) iw.push_back(make_int2((int)q, b));
       if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;  // queued correction, forcing from t
     }
     std::vector<int2> gw;
@@ -1153,7 +1184,9 @@ struct Batch {
     for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
     if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
     if ((rc = upload_vec(&d_cwork, &cap_cwork, cw))) return rc;
+    if ((rc = upload_vec(&d_iwork, &cap_iwork, iw))) return rc;
     ncwork = (int)cw.size();
+    niwork = (int)iw.size();
     dirty = false;
     return FE_OK;
   }
@@ -1184,10 +1217,14 @@ struct Batch {
       if (nb) k_bc_buffers<S><<<(nb + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
       if (nall) k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
     }
+    using F = typename S::fld;
+    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_C | GF_P);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p2<S, typename decltype(t)::type>(g, st); });
+    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_P);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p3<S, typename decltype(t)::type>(g, st); });
+    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_LAPMU);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p4<S, typename decltype(t)::type>(g, par, st); });
   }
@@ -1203,7 +1240,7 @@ struct Batch {
   }
   // kernels of one step, the count launch_step_t makes
   int64_t launches_per_step() const {
-    int64_t k = 1 + 3 * (int64_t)groups.size();
+    int64_t k = 1 + 3 * (int64_t)groups.size() + (niwork ? 3 : 0);
     for (const Engine* e : mem)
       if (e->open_bnd) {
         const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf;

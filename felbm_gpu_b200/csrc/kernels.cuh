@@ -20,9 +20,9 @@
 // logic (central / one-sided / biased, halfway bounce-back, wetting) is
 // derived from tile occupancy with selects, so no per-site tables are read
 // from HBM. P1 and the state transfers touch only a site's own populations
-// and run over flat chunks of CHUNK sites. The grid holds each node once; a
-// brick whose halo reaches past a face of the lattice fills those tile
-// positions from the nodes they wrap to after its copies land.
+// and run over flat chunks of CHUNK sites. Grid positions outside the
+// lattice hold the periodic images of fluid nodes, refreshed by k_images
+// after each pass that writes the field.
 //
 // Streaming is push, fused into P4: the post-collision value f*_k of site x
 // is written to slot k of x + e_k, or to slot opp(k) of x itself when x + e_k
@@ -371,33 +371,6 @@ __device__ __forceinline__ void slot_node(int bx, int by, int bz, int slot, int&
   x = bx * Sh::BX + (slot & (Sh::BX - 1));
   y = by * Sh::BY + ((slot >> Sh::LBX) & (Sh::BY - 1));
   z = bz * Sh::BZ + (slot >> (Sh::LBX + Sh::LBY));
-}
-
-__device__ __forceinline__ int wrap_coord(int c, int n) {
-  c %= n;
-  return c < 0 ? c + n : c;
-}
-
-// Tile positions of a halo tile (TileX<Sh, H>) whose node lies outside the
-// lattice on some axis (a halo that reaches past a face, or slots beyond the
-// lattice's extent) take the value of the node they wrap to, read from the
-// grid: the grid holds each node once, so only bricks at a face need this.
-// NF fields, tile t[f] from grid g[f]; every thread its strided positions.
-template <class Sh, int H, int NF, int NT, class F>
-__device__ __forceinline__ void wrap_tile(const LatDesc& D, int bx, int by, int bz, F* const (&t)[NF],
-                                          const F* const (&g)[NF]) {
-  using T = TileX<Sh, H>;
-  const int x0 = bx * Sh::BX - 2, y0 = by * Sh::BY - H, z0 = Sh::HZ ? bz * Sh::BZ - H : 0;
-  if (x0 >= 0 && x0 + T::TX <= D.nx && y0 >= 0 && y0 + T::TY <= D.ny && z0 >= 0 && z0 + T::TZ <= D.nz) return;
-  for (int q = threadIdx.x; q < T::N; q += NT) {
-    const int tx = q % T::TX, ty = (q / T::TX) % T::TY, tz = q / (T::TX * T::TY);
-    const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
-    if (x >= 0 && x < D.nx && y >= 0 && y < D.ny && z >= 0 && z < D.nz) continue;
-    const int64_t e = (wrap_coord(x, D.nx) + 2) + D.gsy * (wrap_coord(y, D.ny) + 2) +
-                      D.gsz * (wrap_coord(z, D.nz) + 2 * D.hz);
-#pragma unroll
-    for (int f = 0; f < NF; ++f) t[f][q] = g[f][e];
-  }
 }
 
 // The tensor map `id` of the lattice (a CUtensorMap in device memory).
@@ -792,11 +765,6 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   }
   if (threadIdx.x == CTA - 1) load_step_scalars(D, s);
   if (!head_wait(D, &s_bar)) return;
-  {
-    F* const tt[1] = {s_c};
-    const F* const gg[1] = {static_cast<const F*>(D.c)};
-    wrap_tile<Sh, 1, 1, CTA>(D, s.bx, s.by, s.bz, tt, gg);  // the same positions per thread as below
-  }
   correct_tile<T::N, CTA>(s_c, s.lambda);
   __syncthreads();
   const DevPrm& Pm = D.prm;
@@ -895,12 +863,7 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
     tile_copy<Sh, 1>(s_m, D, TM_MU1, s.bx, s.by, s.bz, &s_bar);
   }
   if (!head_wait(D, &s_bar)) return;
-  {
-    F* const tt[1] = {s_m};
-    const F* const gg[1] = {static_cast<const F*>(D.mu)};
-    wrap_tile<Sh, 1, 1, CTA>(D, s.bx, s.by, s.bz, tt, gg);
-    __syncthreads();
-  }
+
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
   const int cnt = s.cnt;
@@ -1064,6 +1027,30 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
   const R uz = (R)ubc[2 * D.n + i] + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff / rho + mor * gz);
   ubc[i] = (F)ux; ubc[D.n + i] = (F)uy; ubc[2 * D.n + i] = (F)uz;
   fp[di] = (F)((R)fp[di] + R(0.5) * ((R)Pm.drho * (ux * gx + uy * gy + uz * gz)) * R(CS2));
+}
+
+// ---------------------------------------------------------------------------
+// periodic images in the stencil-field grids
+// ---------------------------------------------------------------------------
+// Grid positions outside the lattice (node coordinates outside [0, n) on an
+// axis) whose wrapped node is fluid: image[j] = {grid entry, entry of the
+// node it wraps to}, built on the host. Each work item (lattice, block) copies
+// IMG_BLOCK of them for the fields in `fields` (bit 0 c, 1 p, 2 mu, 3 lap mu).
+// Sources are lattice nodes, never images.
+constexpr int IMG_BLOCK = CTA;
+enum : int { GF_C = 1, GF_P = 2, GF_MU = 4, GF_LAPMU = 8 };
+template <class F>
+__global__ void __launch_bounds__(CTA) k_images(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                 int fields) {
+  const int2 wk = work[blockIdx.x];
+  const LatDesc& D = descs[wk.x];
+  const int64_t j = (int64_t)wk.y * IMG_BLOCK + threadIdx.x;
+  if (j >= D.n_images) return;
+  const int2 e = __ldg(&D.images[j]);
+  F* const f[4] = {static_cast<F*>(D.c), static_cast<F*>(D.p), static_cast<F*>(D.mu), static_cast<F*>(D.lapmu)};
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+    if (fields & (1 << b)) f[b][e.x] = f[b][e.y];
 }
 
 // ---------------------------------------------------------------------------

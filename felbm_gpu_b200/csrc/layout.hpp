@@ -121,16 +121,20 @@ struct LatDesc {
   void* pop[2][2];
   // fields (FP64 for FP64 storage, FP32 otherwise). The stencil fields c,
   // p, mu and lap(mu) live on a dense node grid covering node coordinates
-  // [-2, nb * B + 2) per axis (z: [0, 1) without a z halo), x fastest; each
-  // node is held once, at its own coordinates, and solid nodes hold NaN. A
-  // brick's halo tile is then one box of the grid, loaded by one TMA copy; a
-  // brick at a face fills the box positions outside [0, n) from the nodes
-  // they wrap to (wrap_tile). The momentum jx, jy, jz is per site.
+  // [-2, nb * B + 2) per axis (z: [0, 1) without a z halo), x fastest;
+  // solid nodes hold NaN, and positions outside the lattice hold the
+  // periodic image of the node they wrap to (k_images copies those of fluid
+  // nodes after each pass that writes the field). A brick's halo tile is
+  // then one box of the grid, loaded by one TMA copy. The momentum jx, jy, jz
+  // is per site.
   void *c, *p, *jx, *jy, *jz, *mu, *lapmu;
   int gdx, gdy, gdz;           // grid extents (gdx a multiple of 16 bytes of entries)
   int hz;                      // 1: the z axis has a halo (3-D bricks)
   int64_t gsy, gsz;            // entry strides of y and z (x: 1)
   const int32_t* dense_of;     // site -> grid entry of its node
+  const int2* images;          // {grid entry, entry of its fluid node} of each image position
+  int64_t n_images;
+  int image_blocks;            // work items of one k_images pass
   const void* tmap;            // CUtensorMap[TM_N] of the stencil fields (64-byte aligned)
   // open boundary (null when off)
   const uint8_t* bcflag;
