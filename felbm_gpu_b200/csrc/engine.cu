@@ -514,7 +514,7 @@ struct Engine {
       *f = q;
     }
     if ((rc = setup_grid(solid))) return rc;
-    if ((rc = alloc(&D.part1, (size_t)nbk * 2))) return rc;
+    if ((rc = alloc(&D.part1, (size_t)D.nchunks * 2))) return rc;
     if ((rc = alloc(&D.part4, (size_t)nbk * P4W * 6))) return rc;
     FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * P4W * 6 * 8));
     if ((rc = alloc(&d_partm, (size_t)D.nchunks * 2))) return rc;
@@ -673,7 +673,7 @@ struct Engine {
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
     using F = typename S::fld;
     rec(0);
-    k_moments<S, Sh><<<nb, CTA, 0, st>>>(d_desc, d_work, par, 0);
+    k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
     if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_C | GF_P);
@@ -939,7 +939,7 @@ struct Engine {
   // OUT 1: reference site order; OUT 2: node-indexed grids.
   template <class S, class Sh, int OUT>
   void fields_launch(FieldOut o) {
-    k_moments<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, parity, 1);
+    k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
     if (hd.image_blocks)
       k_images<typename S::fld><<<hd.image_blocks, CTA, 0, stream>>>(d_desc, d_iwork, GF_C | GF_P);
@@ -1001,8 +1001,8 @@ struct Engine {
 
 // ---------------------------------------------------------------------------
 // Batch: many lattices advanced together, one launch per pass over the
-// concatenated work lists of all members (their bricks, grouped by brick
-// shape and collision kind; the image refresh over their image lists), captured as
+// concatenated work lists of all members (P1 over their site chunks, P2-P4
+// over their bricks, grouped by brick shape and collision kind), captured as
 // CUDA graphs. Members keep their own buffers, control blocks and
 // reductions; every kernel finds its lattice through the work item, so the
 // result of a member is the one it gets alone. A rebuild (membership change,
@@ -1208,10 +1208,7 @@ struct Batch {
   }
   template <class S>
   void launch_step_t(int par, cudaStream_t st) {
-    for (const Group& g : groups)
-      with_shape<S>(g.shape, [&](auto t) {
-        k_moments<S, typename decltype(t)::type><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, par, 0);
-      });
+    k_moments<S><<<ncwork, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     for (size_t q = 0; q < mem.size(); ++q) {
       const Engine* e = mem[q];
       if (!e->open_bnd) continue;
@@ -1243,7 +1240,7 @@ struct Batch {
   }
   // kernels of one step, the count launch_step_t makes
   int64_t launches_per_step() const {
-    int64_t k = 4 * (int64_t)groups.size() + (niwork ? 3 : 0);
+    int64_t k = 1 + 3 * (int64_t)groups.size() + (niwork ? 3 : 0);
     for (const Engine* e : mem)
       if (e->open_bnd) {
         const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf;

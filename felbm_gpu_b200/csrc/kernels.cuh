@@ -513,17 +513,16 @@ __device__ __forceinline__ void finish_mass(Ctl* C, double M, double Wt) {
 // ---------------------------------------------------------------------------
 // P1: moments of the post-stream state (reference k_moments,
 // device_engine.cuh:116-135, with k_mass_weight, :1109-1126, fused as chunk
-// partials + last-block lambda). One CTA per brick: the brick's sites are one
-// contiguous range and a site's 38 populations sit at one AoSoA base with
-// constant offsets, so each warp reads 38 full 128-byte lines (FP32) and
-// issues them back to back; c and p go to the grid as whole brick rows.
+// partials + last-block lambda). One CTA per chunk of CHUNK sites; a site's 38
+// populations sit at one AoSoA base with constant offsets, so each warp reads
+// 38 full 128-byte lines (FP32) and issues them back to back.
 // ---------------------------------------------------------------------------
 constexpr int CHUNK = 2 * CTA;
 
 // AoSoA index of (site i, direction 0); direction k adds k * AOSOA.
 __device__ __forceinline__ int64_t pbase(int64_t i) { return (i >> 5) * (int64_t)(Q * AOSOA) + (i & (AOSOA - 1)); }
 
-template <class S, class Sh>
+template <class S>
 __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                   int parity, int write_j) {
   using R = typename S::real;
@@ -531,22 +530,13 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   using PG = typename S::gpop;
   using F = typename S::fld;
   __shared__ Red s;
-  __shared__ Head<Sh> hd;
-  __shared__ uint64_t s_bar;
-  // c and p of the brick's slots, written to the grid as whole rows
-  __shared__ __align__(16) F s_cp[2][Sh::C];
   const int2 wk = work[blockIdx.x];
   const LatDesc& D = descs[wk.x];
-  const int brick = wk.y;
-  head_init(&s_bar);
-  if (threadIdx.x == 0) head_begin<Sh>(D, brick, hd, &s_bar, 0);
-  for (int q = threadIdx.x; q < Sh::C; q += CTA) {
-    s_cp[0][q] = nan_v<F>();
-    s_cp[1][q] = nan_v<F>();
-  }
-  if (!head_wait(D, &s_bar)) return;
+  const int chunk = wk.y;
   const PH* __restrict__ hin = static_cast<const PH*>(D.pop[parity][0]);
   const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
+  F* __restrict__ fc = static_cast<F*>(D.c);
+  F* __restrict__ fp = static_cast<F*>(D.p);
   F* __restrict__ fjx = static_cast<F*>(D.jx);
   F* __restrict__ fjy = static_cast<F*>(D.jy);
   F* __restrict__ fjz = static_cast<F*>(D.jz);
@@ -554,9 +544,9 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
   double acc[2] = {0.0, 0.0};
   write_j |= D.prm.need_j;
-  const int first = hd.first, cnt = hd.cnt;
-  for (int r = threadIdx.x; r < cnt; r += CTA) {
-    const int64_t i = first + r;
+  const int64_t i0 = (int64_t)chunk * CHUNK;
+  const int64_t iend = i0 + CHUNK < D.n ? i0 + CHUNK : D.n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
     const int64_t a = pbase(i);
     R hv[Q], gv[Q];
 #pragma unroll
@@ -575,9 +565,9 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
       if (lat_cy(k)) jy += R(lat_cy(k)) * gv[k];
       if (lat_cz(k)) jz += R(lat_cz(k)) * gv[k];
     }
-    const int slot = hd.slot_of[r];
-    s_cp[0][slot] = (F)c;
-    s_cp[1][slot] = (F)p;
+    const int64_t de = __ldg(&D.dense_of[i]);
+    fc[de] = (F)c;
+    fp[de] = (F)p;
     if (write_j) {  // read only by P2's pressure correction (drho != 0), the
       fjx[i] = (F)jx;  // open-boundary kernels and field downloads (need_j | forced)
       fjy[i] = (F)jy;
@@ -588,36 +578,15 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
     acc[0] += cd;
     acc[1] += phi;
   }
-  __syncthreads();
-  // the brick's rows of c and p, pairs of entries at a time (a row starts at
-  // an even grid entry); slots without a site carry NaN, and rows beyond the
-  // lattice's extent are grid images, rewritten by the image refresh
-  {
-    using F2 = typename std::conditional<sizeof(F) == 8, double2, float2>::type;
-    constexpr int PR = Sh::BX / 2;  // pairs a row
-    F* const f[2] = {static_cast<F*>(D.c), static_cast<F*>(D.p)};
-    for (int q = threadIdx.x; q < 2 * (Sh::C / 2); q += CTA) {
-      const int fld = q / (Sh::C / 2), e = q - fld * (Sh::C / 2);
-      const int row = e / PR, k = e - row * PR;
-      const int ly = row & (Sh::BY - 1), lz = row >> Sh::LBY;
-      const int64_t g = (hd.bx * Sh::BX + 2) + D.gsy * (hd.by * Sh::BY + ly + 2) +
-                        D.gsz * (hd.bz * Sh::BZ + lz + 2 * D.hz) + 2 * k;
-      const F* src = &s_cp[fld][row * Sh::BX + 2 * k];
-      F2 v;
-      v.x = src[0];
-      v.y = src[1];
-      *reinterpret_cast<F2*>(f[fld] + g) = v;
-    }
-  }
   if (!D.prm.correct_mass) return;
   block_sum<2>(acc, s);
   if (threadIdx.x == 0) {
-    D.part1[(int64_t)brick * 2 + 0] = acc[0];
-    D.part1[(int64_t)brick * 2 + 1] = acc[1];
+    D.part1[(int64_t)chunk * 2 + 0] = acc[0];
+    D.part1[(int64_t)chunk * 2 + 1] = acc[1];
   }
-  if (!last_block(&D.ctl->count1, (unsigned)D.nbricks, s)) return;
+  if (!last_block(&D.ctl->count1, (unsigned)D.nchunks, s)) return;
   double tot[2];
-  sum_partials<2>(D.part1, D.nbricks, 2, tot, s);
+  sum_partials<2>(D.part1, D.nchunks, 2, tot, s);
   if (threadIdx.x == 0) {
     finish_mass(D.ctl, tot[0], tot[1]);
     D.ctl->count1 = 0;
