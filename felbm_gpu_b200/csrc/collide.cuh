@@ -47,27 +47,24 @@ struct CollideMinBlocks {
 constexpr int NPAIR = (Q - 1) / 2;  // 9 opposite pairs
 
 // Dynamic shared memory of the collide pass (each region 128-byte aligned,
-// the alignment of a TMA destination): the halo-1 site-index tile (push
-// targets), the interleaved (c, p) tile and the lap(mu) tile (halo 2), and
-// the per-thread stash (two pairs and one scalar per opposite pair). The raw
-// c and p tiles land in the stash region and are interleaved from there
-// before the stash is used.
+// the alignment of a TMA destination): the halo-1 tile of push targets, the
+// (c', p') pair tile and the lap(mu) tile (halo 2), and the per-thread stash
+// (two pairs and one scalar per opposite pair).
 template <class S, class Sh>
 struct CollideSmem {
   using R = typename S::real;
   using F = typename S::fld;
   using T = Tile<Sh, 2>;
   using T1 = Tile<Sh, 1>;
+  static_assert(sizeof(R) == sizeof(F), "the pair tile is copied as stored");
   static constexpr int al(int b) { return (b + 127) & ~127; }
   static constexpr int IDX = al(T1::N * 4);
   static constexpr int CP = al(T::N * (int)sizeof(V2<R>));
   static constexpr int LT = al(T::N * (int)sizeof(F));
-  static constexpr int RAW = al(T::N * (int)sizeof(F));  // one raw field tile
   static constexpr int STV = 2 * NPAIR * P4T * (int)sizeof(V2<R>);
   static constexpr int STS = NPAIR * P4T * (int)sizeof(R);
   static constexpr int OFF_CP = IDX, OFF_L = OFF_CP + CP, OFF_ST = OFF_L + LT;
   static constexpr int BYTES = OFF_ST + al(STV + STS);
-  static_assert(2 * RAW <= al(STV + STS), "the raw c and p tiles fit the stash region");
 };
 
 // Per-site scalars shared by every direction of the collision.
@@ -100,8 +97,6 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   int32_t* s_idx = reinterpret_cast<int32_t*>(dsm);  // halo-1 tile
   V* s_cp = reinterpret_cast<V*>(dsm + SM::OFF_CP);
   F* s_l = reinterpret_cast<F*>(dsm + SM::OFF_L);
-  F* raw_c = reinterpret_cast<F*>(dsm + SM::OFF_ST);
-  F* raw_p = reinterpret_cast<F*>(dsm + SM::OFF_ST + SM::RAW);
   V* s_sv = reinterpret_cast<V*>(dsm + SM::OFF_ST) + threadIdx.x;                  // [(2 pr + j) P4T]
   R* s_sc = reinterpret_cast<R*>(dsm + SM::OFF_ST + SM::STV) + threadIdx.x;         // [pr P4T]
   const int2 wk = work[blockIdx.x];
@@ -112,37 +107,19 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     if (threadIdx.x == 0) atomicOr(&D.ctl->status, 8);
     return;
   }
-  // prologue: the brick's slot list, its halo-1 site-index tile and the c, p,
-  // lap(mu) tiles (halo 2) by copy engine, on one barrier
+  // prologue: the brick's slot list, its halo-1 tile of push targets and the
+  // (c', p') and lap(mu) tiles (halo 2) by copy engine, on one barrier; P2
+  // wrote the pairs with the queued mass correction applied, so the tiles
+  // are used as they land
   head_init(&s_bar);
   if (threadIdx.x == 0) {
-    head_begin<Sh>(D, brick, s, &s_bar, (uint32_t)(3 * T::N * sizeof(F) + T1::N * 4));
-    tile_copy<Sh, 2>(raw_c, D, TM_C2, s.bx, s.by, s.bz, &s_bar);
-    tile_copy<Sh, 2>(raw_p, D, TM_P2, s.bx, s.by, s.bz, &s_bar);
+    head_begin<Sh>(D, brick, s, &s_bar, (uint32_t)(T::N * (sizeof(V) + sizeof(F)) + T1::N * 4));
+    tile_copy<Sh, 2, (int)sizeof(V) / 8>(s_cp, D, TM_CP2, s.bx, s.by, s.bz, &s_bar);
     tile_copy<Sh, 2>(s_l, D, TM_L2, s.bx, s.by, s.bz, &s_bar);
     bulk_g2s(s_idx, D.tile1 + (int64_t)brick * T1::N, (uint32_t)(T1::N * 4), &s_bar);
   }
   if (threadIdx.x == P4T - 1) load_step_scalars(D, s);
   if (!head_wait(D, &s_bar)) return;
-  // (c, p) pairs, with a queued mass correction applied to c
-  {
-    const double lam = s.lambda;
-    for (int t = threadIdx.x; t < T::N; t += P4T) {
-      R c = (R)raw_c[t];
-      if (lam != 0.0 && is_site(c)) c = corr_c<R>(c, lam);
-      s_cp[t] = V(c, (R)raw_p[t]);
-    }
-  }
-  if (!WIDE) {
-    // from here on the index tile holds each site's AoSoA population base
-    // (below 2^32 - 1 for narrow offsets; 0xffffffff marks no site), so a
-    // push target is one add
-    for (int t = threadIdx.x; t < T1::N; t += P4T) {
-      const int32_t v = s_idx[t];
-      if (v >= 0) s_idx[t] = (int32_t)((uint32_t)(v >> 5) * (uint32_t)(Q * AOSOA) + (uint32_t)(v & (AOSOA - 1)));
-    }
-  }
-  __syncthreads();
 
   const DevPrm& Pm = D.prm;
   const R cs2 = R(CS2), alpha = R(ALPHA);

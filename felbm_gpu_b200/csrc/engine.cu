@@ -540,7 +540,7 @@ struct Engine {
     FE_DISPATCH(*this, rc = alloc_tiles<Sh>());
     if (rc) return rc;
     if ((rc = upload_desc())) return rc;
-    FE_DISPATCH(*this, (k_build_tiles<Sh><<<nbk, CTA, 0, stream>>>(d_desc, d_work)));
+    FE_DISPATCH(*this, (k_build_tiles<Sh><<<nbk, CTA, 0, stream>>>(d_desc, d_work, wide)));
     FE_CUDA(cudaGetLastError());
     FE_CUDA(cudaStreamSynchronize(stream));
     return FE_OK;
@@ -575,11 +575,12 @@ struct Engine {
     const int64_t cells = D.gsz * D.gdz;
     if (cells >= ((int64_t)1 << 31)) return fe_fail(FE_ERR_ARG, "lattice too large for the 32-bit field grid");
     const size_t es = fld_size();
-    for (void** f : {&D.c, &D.p, &D.mu, &D.lapmu}) {
+    for (void** f : {&D.c, &D.p, &D.mu, &D.lapmu, &D.cp}) {
+      const size_t bytes = (size_t)cells * es * (f == &D.cp ? 2 : 1);
       unsigned char* q;
       int rc;
-      if ((rc = alloc(&q, (size_t)cells * es))) return rc;
-      FE_CUDA(cudaMemset(q, 0xff, (size_t)cells * es));  // all-ones: a NaN in FP32 and FP64
+      if ((rc = alloc(&q, bytes))) return rc;
+      FE_CUDA(cudaMemset(q, 0xff, bytes));  // all-ones: a NaN in FP32 and FP64
       *f = q;
     }
     std::vector<int32_t> dense((size_t)D.n);
@@ -618,8 +619,10 @@ struct Engine {
     return rc;
   }
 
-  // Tensor maps of the halo boxes: c with halo 1 (P2) and 2 (P4), p and
-  // lap(mu) with halo 2 (P4), mu with halo 1 (P3); x halo 2 in every box.
+  // Tensor maps of the halo boxes: c with halo 1 (P2), mu with halo 1 (P3),
+  // the (c', p') pairs and lap(mu) with halo 2 (P4); x halo 2 in every box.
+  // A node of the pair grid is one 8-byte element (FP32 pairs) or two (FP64
+  // pairs); the copy moves bits, so the element type only sets the size.
   template <class S, class Sh>
   int build_tmaps() {
     using F = typename S::fld;
@@ -627,13 +630,14 @@ struct Engine {
     if (!enc) return fe_fail(FE_ERR_CUDA, "cuTensorMapEncodeTiled not available from the driver");
     const LatDesc& D = hd;
     alignas(64) CUtensorMap maps[TM_N];
-    auto make = [&](int id, void* base, int H) -> int {
-      const cuuint64_t dims[3] = {(cuuint64_t)D.gdx, (cuuint64_t)D.gdy, (cuuint64_t)D.gdz};
-      const cuuint64_t strides[2] = {(cuuint64_t)D.gdx * sizeof(F), (cuuint64_t)D.gsz * sizeof(F)};
-      const cuuint32_t box[3] = {(cuuint32_t)(Sh::BX + 4), (cuuint32_t)(Sh::BY + 2 * H),
+    auto make = [&](int id, void* base, int H, size_t node_bytes) -> int {
+      const size_t es = node_bytes >= 8 ? 8 : 4, xm = node_bytes / es;
+      const cuuint64_t dims[3] = {(cuuint64_t)D.gdx * xm, (cuuint64_t)D.gdy, (cuuint64_t)D.gdz};
+      const cuuint64_t strides[2] = {(cuuint64_t)D.gdx * node_bytes, (cuuint64_t)D.gsz * node_bytes};
+      const cuuint32_t box[3] = {(cuuint32_t)((Sh::BX + 4) * xm), (cuuint32_t)(Sh::BY + 2 * H),
                                  (cuuint32_t)(D.hz ? Sh::BZ + 2 * H : 1)};
       const cuuint32_t estr[3] = {1, 1, 1};
-      const CUresult r = enc(&maps[id], sizeof(F) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      const CUresult r = enc(&maps[id], es == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
                              3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -641,8 +645,8 @@ struct Engine {
       return FE_OK;
     };
     int rc;
-    if ((rc = make(TM_C1, D.c, 1)) || (rc = make(TM_C2, D.c, 2)) || (rc = make(TM_P2, D.p, 2)) ||
-        (rc = make(TM_MU1, D.mu, 1)) || (rc = make(TM_L2, D.lapmu, 2)))
+    if ((rc = make(TM_C1, D.c, 1, sizeof(F))) || (rc = make(TM_CP2, D.cp, 2, 2 * sizeof(F))) ||
+        (rc = make(TM_MU1, D.mu, 1, sizeof(F))) || (rc = make(TM_L2, D.lapmu, 2, sizeof(F))))
       return rc;
     unsigned char* q;
     if ((rc = alloc(&q, sizeof(maps)))) return rc;
@@ -676,11 +680,11 @@ struct Engine {
     k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
-    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_C | GF_P);
+    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_C);
     rec(2);
     if (hd.prm.hbb) k_cfield<S, Sh, 0, true><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
     else k_cfield<S, Sh, 0, false><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
-    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_P);
+    if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_CP);
     rec(3);
     if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
     else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
@@ -942,7 +946,7 @@ struct Engine {
     k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
     if (open_bnd) launch_bc<S>(stream);
     if (hd.image_blocks)
-      k_images<typename S::fld><<<hd.image_blocks, CTA, 0, stream>>>(d_desc, d_iwork, GF_C | GF_P);
+      k_images<typename S::fld><<<hd.image_blocks, CTA, 0, stream>>>(d_desc, d_iwork, GF_C);
     if (hd.prm.hbb) k_cfield<S, Sh, OUT, true><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     else k_cfield<S, Sh, OUT, false><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
     launches += hd.image_blocks ? 3 : 2;
@@ -1159,27 +1163,28 @@ struct Batch {
     }
     std::vector<int2> gw;
     std::vector<size_t> offs;
-    // one group per collide variant, so each member runs the kernel it runs alone
+    // one group per collide variant, so each member runs the kernel it runs
+    // alone (the offset width included: it decides what a member's push-target
+    // tiles hold)
     for (int sh = 0; sh < NSHAPE; ++sh)
       for (int mrt = 0; mrt < 3; ++mrt)
-        for (int hbb = 0; hbb < 2; ++hbb) {
-          const size_t off = gw.size();
-          for (size_t q = 0; q < mem.size(); ++q)
-            if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt && (mem[q]->hd.prm.hbb != 0) == (hbb != 0))
-              for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
-          if (gw.size() == off) continue;
-          Group g;
-          for (size_t q = 0; q < mem.size(); ++q)
-            if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt && (mem[q]->hd.prm.hbb != 0) == (hbb != 0) &&
-                mem[q]->wide)
-              g.wide = 1;
-          g.shape = sh;
-          g.mrt = mrt;
-          g.hbb = hbb;
-          g.nwork = (int)(gw.size() - off);
-          groups.push_back(g);
-          offs.push_back(off);
-        }
+        for (int hbb = 0; hbb < 2; ++hbb)
+          for (int wd = 0; wd < 2; ++wd) {
+            const size_t off = gw.size();
+            for (size_t q = 0; q < mem.size(); ++q)
+              if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt && (mem[q]->hd.prm.hbb != 0) == (hbb != 0) &&
+                  (mem[q]->wide != 0) == (wd != 0))
+                for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
+            if (gw.size() == off) continue;
+            Group g;
+            g.wide = wd;
+            g.shape = sh;
+            g.mrt = mrt;
+            g.hbb = hbb;
+            g.nwork = (int)(gw.size() - off);
+            groups.push_back(g);
+            offs.push_back(off);
+          }
     if ((rc = upload_vec(&d_gwork, &cap_gwork, gw))) return rc;
     for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
     if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
@@ -1218,10 +1223,10 @@ struct Batch {
       if (nall) k_bc_final<S><<<(nall + 127) / 128, 128, 0, st>>>(d_desc, (int)q);
     }
     using F = typename S::fld;
-    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_C | GF_P);
+    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_C);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p2<S, typename decltype(t)::type>(g, st); });
-    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_P);
+    if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_CP);
     for (const Group& g : groups)
       with_shape<S>(g.shape, [&](auto t) { launch_group_p3<S, typename decltype(t)::type>(g, st); });
     if (niwork) k_images<F><<<niwork, CTA, 0, st>>>(d_desc, d_iwork, GF_LAPMU);

@@ -379,12 +379,14 @@ __device__ __forceinline__ const void* tmap_of(const LatDesc& D, int id) {
 }
 
 // Box copy of the halo-H tile of brick (bx, by, bz) from a stencil-field
-// grid into shared memory (x0 = bx * BX: 16-byte aligned for the 4- and
-// 8-byte fields).
-template <class Sh, int H>
+// grid into shared memory. XM is the number of tensor-map elements a node
+// holds (the pair grid of FP64 fields counts 8-byte elements, two a node);
+// x0 = bx * BX * XM elements, 16-byte aligned for the 4- and 8-byte element
+// types.
+template <class Sh, int H, int XM = 1>
 __device__ __forceinline__ void tile_copy(void* dst, const LatDesc& D, int id, int bx, int by, int bz,
                                           uint64_t* bar) {
-  tma_box3(dst, tmap_of(D, id), bx * Sh::BX, by * Sh::BY + 2 - H, D.hz ? bz * Sh::BZ + 2 - H : 0, bar);
+  tma_box3(dst, tmap_of(D, id), bx * Sh::BX * XM, by * Sh::BY + 2 - H, D.hz ? bz * Sh::BZ + 2 - H : 0, bar);
 }
 
 // A stencil pass's prologue: thread 0 sets up the transaction barrier and
@@ -418,11 +420,14 @@ __device__ __forceinline__ bool head_wait(const LatDesc& D, uint64_t* bar) {
   return true;
 }
 
-// Setup: the halo-1 site-index tile (the collide pass's push targets) and
-// the slot list of every brick, from the occupancy words; one CTA per brick,
-// run once per lattice.
+// Setup: the halo-1 tile of push targets of the collide pass and the slot
+// list of every brick, from the occupancy words; one CTA per brick, run once
+// per lattice. With 32-bit population offsets (wide == 0) a tile entry is
+// the site's AoSoA population base (below 2^32 - 1; 0xffffffff: no site), so
+// a push target is one add; with 64-bit offsets it is the site index (-1).
 template <class Sh>
-__global__ void __launch_bounds__(CTA) k_build_tiles(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
+__global__ void __launch_bounds__(CTA) k_build_tiles(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                      int wide) {
   using T1 = Tile<Sh, 1>;
   __shared__ Pro<Sh> s;
   __shared__ IdxTile<Sh, 1> t1;
@@ -433,7 +438,10 @@ __global__ void __launch_bounds__(CTA) k_build_tiles(const LatDesc* __restrict__
   build_idx_tile<Sh, 1>(s, t1.idx, t1.rbits, t1.rbase);
   int32_t* g1 = const_cast<int32_t*>(D.tile1) + (int64_t)brick * T1::N;
   uint16_t* gs = const_cast<uint16_t*>(D.slots) + (int64_t)brick * Sh::C;
-  for (int t = threadIdx.x; t < T1::N; t += CTA) g1[t] = t1.idx[t];
+  for (int t = threadIdx.x; t < T1::N; t += CTA) {
+    const int32_t v = t1.idx[t];
+    g1[t] = (wide || v < 0) ? v : (int32_t)((uint32_t)(v >> 5) * (uint32_t)(Q * AOSOA) + (uint32_t)(v & (AOSOA - 1)));
+  }
   for (int r = threadIdx.x; r < Sh::C; r += CTA) gs[r] = r < s.rec.cnt ? s.slot_of[r] : (uint16_t)0;
 }
 
@@ -776,6 +784,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   const F* __restrict__ fjz = static_cast<const F*>(D.jz);
   F* __restrict__ fp = static_cast<F*>(D.p);
   F* __restrict__ fmu = static_cast<F*>(D.mu);
+  V2<F>* __restrict__ fcp = static_cast<V2<F>*>(D.cp);
   const int first = s.first, cnt = s.cnt;
   for (int r = threadIdx.x; r < cnt; r += CTA) {
     const int64_t i = first + r;
@@ -785,6 +794,7 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     const R c0 = (R)s_c[pos];
     const uint8_t flag = Pm.open_bnd ? D.bcflag[i] : 0;
     if (flag & BC_SITE) {
+      fcp[di] = V2<F>((F)c0, fp[di]);
       if (OUT) {
         const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, slot) : (int64_t)D.ref_of[i];
         const F* ub = static_cast<const F*>(D.u_bc);
@@ -818,8 +828,10 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     const R rho = rho1 + drho * c0;
     const R mu = four_beta * (c0 * (R(1) - c0)) * (R(0.5) - c0) + (-kappa * lap);
     fmu[di] = (F)mu;
+    const F p_in = fp[di];
     // the correction changes p only through drho (k_vel_press_corr :194-195);
     // u is needed here only for that, for output, or for the tracers' snapshot
+    if (Pm.drho == 0.0) fcp[di] = V2<F>((F)c0, p_in);
     if (Pm.drho != 0.0 || OUT || D.snap_u[0]) {
       const R irho = R(1) / rho;
       const R inv = irho * R(1.0 / CS2);
@@ -827,8 +839,11 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
       const R ux = (R)fjx[i] * inv + R(0.5) * ((R)Pm.gx + (R)Pm.fx * ff * irho + mor * gx);
       const R uy = (R)fjy[i] * inv + R(0.5) * ((R)Pm.gy + (R)Pm.fy * ff * irho + mor * gy);
       const R uz = (R)fjz[i] * inv + R(0.5) * ((R)Pm.gz + (R)Pm.fz * ff * irho + mor * gz);
-      const R p = (R)fp[di] + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
-      if (Pm.drho != 0.0) fp[di] = (F)p;
+      const R p = (R)p_in + R(0.5) * (drho * (ux * gx + uy * gy + uz * gz)) * cs2;
+      if (Pm.drho != 0.0) {
+        fp[di] = (F)p;
+        fcp[di] = V2<F>((F)c0, (F)p);
+      }
       if (OUT) {
         const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, slot) : (int64_t)D.ref_of[i];
         out.put(q, (double)c0, (double)rho, (double)ux, (double)uy, (double)uz, (double)p, (double)mu);
@@ -1035,10 +1050,10 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
 // Grid positions outside the lattice (node coordinates outside [0, n) on an
 // axis) whose wrapped node is fluid: image[j] = {grid entry, entry of the
 // node it wraps to}, built on the host. Each work item (lattice, block) copies
-// IMG_BLOCK of them for the fields in `fields` (bit 0 c, 1 p, 2 mu, 3 lap mu).
-// Sources are lattice nodes, never images.
+// IMG_BLOCK of them for the fields in `fields` (bit 0 c, 1 p, 2 mu, 3 lap mu,
+// 4 the (c', p') pairs). Sources are lattice nodes, never images.
 constexpr int IMG_BLOCK = CTA;
-enum : int { GF_C = 1, GF_P = 2, GF_MU = 4, GF_LAPMU = 8 };
+enum : int { GF_C = 1, GF_P = 2, GF_MU = 4, GF_LAPMU = 8, GF_CP = 16 };
 template <class F>
 __global__ void __launch_bounds__(CTA) k_images(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                  int fields) {
@@ -1051,6 +1066,10 @@ __global__ void __launch_bounds__(CTA) k_images(const LatDesc* __restrict__ desc
 #pragma unroll
   for (int b = 0; b < 4; ++b)
     if (fields & (1 << b)) f[b][e.x] = f[b][e.y];
+  if (fields & GF_CP) {
+    V2<F>* cp = static_cast<V2<F>*>(D.cp);
+    cp[e.x] = cp[e.y];
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -89,8 +89,8 @@ struct DevPrm {
 
 // The tensor maps of a lattice's stencil-field grids: the field and the
 // halo of the box (the x halo of every box is 2, so the box starts on a
-// 16-byte boundary).
-enum TensorMapId { TM_C1 = 0, TM_C2 = 1, TM_P2 = 2, TM_MU1 = 3, TM_L2 = 4, TM_N = 5 };
+// 16-byte boundary). TM_CP2 covers the (c', p') pair grid.
+enum TensorMapId { TM_C1 = 0, TM_CP2 = 1, TM_MU1 = 2, TM_L2 = 3, TM_N = 4 };
 
 // Per-site open-boundary flags (bcflag[i]).
 enum : uint8_t {
@@ -115,7 +115,9 @@ struct LatDesc {
   const int32_t* brick_xyz;    // [nbricks][3]
   const BrickRec* rec;         // [nbricks]
   const int32_t* ref_of;       // site -> reference-order index
-  const int32_t* tile1;        // [nbricks][halo-1 tile] site index or -1 (k_build_tiles)
+  const int32_t* tile1;        // [nbricks][halo-1 tile] (k_build_tiles): with 32-bit population
+                               // offsets the site's AoSoA population base (0xffffffff: no site),
+                               // with 64-bit ones the site index (-1: no site)
   const uint16_t* slots;       // [nbricks][brick slots] fluid slots in site order
   // state: pop[buffer][0 = h, 1 = g]
   void* pop[2][2];
@@ -126,8 +128,10 @@ struct LatDesc {
   // periodic image of the node they wrap to (k_images copies those of fluid
   // nodes after each pass that writes the field). A brick's halo tile is
   // then one box of the grid, loaded by one TMA copy. The momentum jx, jy, jz
-  // is per site.
-  void *c, *p, *jx, *jy, *jz, *mu, *lapmu;
+  // is per site. cp is the grid of (c', p') pairs that P2 writes for the
+  // collision: the order parameter with the queued mass correction applied
+  // and the corrected pressure, interleaved.
+  void *c, *p, *jx, *jy, *jz, *mu, *lapmu, *cp;
   int gdx, gdy, gdz;           // grid extents (gdx a multiple of 16 bytes of entries)
   int hz;                      // 1: the z axis has a halo (3-D bricks)
   int64_t gsy, gsz;            // entry strides of y and z (x: 1)

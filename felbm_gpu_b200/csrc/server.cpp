@@ -71,14 +71,15 @@ double pop_bytes(int storage) {
 size_t fld_bytes(int storage) { return storage == FE_F64 ? 8 : 4; }
 
 // Device bytes of one resident solve: two ping-pong buffers of h and g, the
-// three per-site momentum fields, the four stencil fields on the node grid
-// (the lattice rounded up to bricks plus a two-node ring; bounded here by
-// 20 more nodes per axis), the FP64 transfer buffer (upload/download), and
-// the site/brick tables (generous per-site bound).
+// three per-site momentum fields, the stencil fields on the node grid (c, p,
+// mu, lap(mu) and the (c', p') pairs: six values a node; the lattice rounded
+// up to bricks plus a two-node ring, bounded here by 20 more nodes per axis),
+// the FP64 transfer buffer (upload/download), and the site/brick tables
+// (generous per-site bound).
 double footprint(int64_t n, int nx, int ny, int nz, int storage) {
   const double per = 4.0 * 19 * pop_bytes(storage) + 3.0 * fld_bytes(storage) + 2.0 * 19 * 8 + 64;
   const double cells = (double)(nx + 20) * (double)(ny + 20) * (double)(nz == 1 ? 1 : nz + 20);
-  return (double)n * per + 4.0 * cells * (double)fld_bytes(storage) + (double)(64 << 20);
+  return (double)n * per + 6.0 * cells * (double)fld_bytes(storage) + (double)(64 << 20);
 }
 
 double percentile(std::vector<double> v, double q) {

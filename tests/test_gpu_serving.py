@@ -98,7 +98,7 @@ def test_admission_by_memory(require_gpu):
     n = int(np.count_nonzero(solid == 0))
     per = 4 * 19 * 4 + 3 * 4 + 2 * 19 * 8 + 64
     nz, ny, nx = solid.shape
-    one = (64 << 20) + n * per + 4 * 4 * (nx + 20) * (ny + 20) * (1 if nz == 1 else nz + 20)
+    one = (64 << 20) + n * per + 6 * 4 * (nx + 20) * (ny + 20) * (1 if nz == 1 else nz + 20)
     frac = max(0.0, (free - 1.5 * one) / total)
     srv = Server(storage="f32", hbm_reserve_frac=frac, chunk_steps=8)
     try:
