@@ -251,6 +251,53 @@ static void launch_collide(int mrt, bool hbb, bool wide, int nwork, size_t smem,
   else if (hbb) launch_collide_w<S, Sh, 0, true>(wide, nwork, smem, st, desc, work, par);
   else launch_collide_w<S, Sh, 0, false>(wide, nwork, smem, st, desc, work, par);
 }
+// CTAs of a persistent stencil pass: as many as the GPU holds at once
+// (occupancy of the kernel, once per kernel and device), at most one per
+// work item.
+static int resident_grid(const void* kernel, int nwork) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<const void*, int>, int>> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int full = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto& e : cache)
+      if (e.first.first == kernel && e.first.second == dev) full = e.second;
+  }
+  if (!full) {
+    int per = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, CTA, 0) != cudaSuccess || per < 1) per = 1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+    full = per * sms;
+    std::lock_guard<std::mutex> lk(mu);
+    cache.push_back({{kernel, dev}, full});
+  }
+  return nwork < full ? nwork : full;
+}
+template <class S, class Sh, int OUT>
+static void launch_cfield(bool hbb, int nwork, cudaStream_t st, const LatDesc* desc, const int2* work,
+                          const FieldOut& o) {
+  if (nwork <= 0) return;
+  if (hbb) {
+    auto k = k_cfield<S, Sh, OUT, true>;
+    k<<<resident_grid((const void*)k, nwork), CTA, 0, st>>>(desc, work, nwork, o);
+  } else {
+    auto k = k_cfield<S, Sh, OUT, false>;
+    k<<<resident_grid((const void*)k, nwork), CTA, 0, st>>>(desc, work, nwork, o);
+  }
+}
+template <class S, class Sh>
+static void launch_lapmu(bool hbb, int nwork, cudaStream_t st, const LatDesc* desc, const int2* work) {
+  if (nwork <= 0) return;
+  if (hbb) {
+    auto k = k_lapmu<S, Sh, true>;
+    k<<<resident_grid((const void*)k, nwork), CTA, 0, st>>>(desc, work, nwork);
+  } else {
+    auto k = k_lapmu<S, Sh, false>;
+    k<<<resident_grid((const void*)k, nwork), CTA, 0, st>>>(desc, work, nwork);
+  }
+}
 template <class S, class Sh>
 static cudaError_t collide_smem_attr(int bytes) {
   const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
@@ -682,12 +729,10 @@ struct Engine {
     if (open_bnd) launch_bc<S>(st);
     if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_C);
     rec(2);
-    if (hd.prm.hbb) k_cfield<S, Sh, 0, true><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
-    else k_cfield<S, Sh, 0, false><<<nb, CTA, 0, st>>>(d_desc, d_work, FieldOut{});
+    launch_cfield<S, Sh, 0>(hd.prm.hbb != 0, nb, st, d_desc, d_work, FieldOut{});
     if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_MU | GF_CP);
     rec(3);
-    if (hd.prm.hbb) k_lapmu<S, Sh, true><<<nb, CTA, 0, st>>>(d_desc, d_work);
-    else k_lapmu<S, Sh, false><<<nb, CTA, 0, st>>>(d_desc, d_work);
+    launch_lapmu<S, Sh>(hd.prm.hbb != 0, nb, st, d_desc, d_work);
     if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_LAPMU);
     rec(4);
     launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
@@ -947,8 +992,7 @@ struct Engine {
     if (open_bnd) launch_bc<S>(stream);
     if (hd.image_blocks)
       k_images<typename S::fld><<<hd.image_blocks, CTA, 0, stream>>>(d_desc, d_iwork, GF_C);
-    if (hd.prm.hbb) k_cfield<S, Sh, OUT, true><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
-    else k_cfield<S, Sh, OUT, false><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work, o);
+    launch_cfield<S, Sh, OUT>(hd.prm.hbb != 0, hd.nbricks, stream, d_desc, d_work, o);
     launches += hd.image_blocks ? 3 : 2;
   }
   // Corrected velocity of the current state into node-indexed device grids
@@ -1198,13 +1242,11 @@ struct Batch {
 
   template <class S, class Sh>
   void launch_group_p2(const Group& g, cudaStream_t st) {
-    if (g.hbb) k_cfield<S, Sh, 0, true><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, FieldOut{});
-    else k_cfield<S, Sh, 0, false><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work, FieldOut{});
+    launch_cfield<S, Sh, 0>(g.hbb != 0, g.nwork, st, d_desc, g.d_work, FieldOut{});
   }
   template <class S, class Sh>
   void launch_group_p3(const Group& g, cudaStream_t st) {
-    if (g.hbb) k_lapmu<S, Sh, true><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work);
-    else k_lapmu<S, Sh, false><<<g.nwork, CTA, 0, st>>>(d_desc, g.d_work);
+    launch_lapmu<S, Sh>(g.hbb != 0, g.nwork, st, d_desc, g.d_work);
   }
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {

@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   const PH* __restrict__ hin = static_cast<const PH*>(D.pop[parity][0]);
   const PG* __restrict__ gin = static_cast<const PG*>(D.pop[parity][1]);
   F* __restrict__ fc = static_cast<F*>(D.c);
-  F* __restrict__ fp = static_cast<F*>(D.p);
+  F* fp = static_cast<F*>(D.p);
   F* __restrict__ fjx = static_cast<F*>(D.jx);
   F* __restrict__ fjy = static_cast<F*>(D.jy);
   F* __restrict__ fjz = static_cast<F*>(D.jz);
@@ -725,6 +725,61 @@ __device__ __forceinline__ R lap_sel(R f0, R fm, R fp, R bnd, bool sm, bool sp) 
 }
 
 // ---------------------------------------------------------------------------
+// Persistent, double-buffered brick pipeline of the stencil passes P2 and P3:
+// a CTA takes the work items blockIdx.x, blockIdx.x + gridDim.x, ... and
+// while it computes one brick from one stage, the copy engine fills the
+// other stage with the next brick's head, slot list and halo-H tile (one
+// mbarrier per stage, phases counted per use). The block barrier after each
+// wait orders the next issue into a stage after every thread has left it.
+// ---------------------------------------------------------------------------
+template <class Sh, class F, int N>
+struct StencilStages {
+  // each stage's tile starts on a 128-byte boundary (a TMA destination)
+  static constexpr int NA = ((N * (int)sizeof(F) + 127) / 128 * 128) / (int)sizeof(F);
+  F tile[2][NA];
+  Head<Sh> head[2];
+  uint64_t bar[2];
+};
+
+template <class Sh, class F, int H, bool SCALARS, class Body>
+__device__ __forceinline__ void stencil_pipeline(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                 int nwork, int tmap_id, StencilStages<Sh, F, TileX<Sh, H>::N>& sm,
+                                                 Body&& body) {
+  using T = TileX<Sh, H>;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.bar[0]);
+    mbar_init(&sm.bar[1]);
+  }
+  __syncthreads();
+  auto issue = [&](int item, int st) {
+    if (threadIdx.x == 0) {
+      const int2 wk = work[item];
+      const LatDesc& D = descs[wk.x];
+      Head<Sh>& h = sm.head[st];
+      head_begin<Sh>(D, wk.y, h, &sm.bar[st], (uint32_t)(T::N * sizeof(F)));
+      tile_copy<Sh, H>(sm.tile[st], D, tmap_id, h.bx, h.by, h.bz, &sm.bar[st]);
+    }
+    if (SCALARS && threadIdx.x == CTA - 1) load_step_scalars(descs[work[item].x], sm.head[st]);
+  };
+  int w = blockIdx.x;
+  if (w < nwork) issue(w, 0);
+  for (int j = 0; w < nwork; w += (int)gridDim.x, ++j) {
+    const int st = j & 1, wn = w + (int)gridDim.x;
+    if (wn < nwork) issue(wn, st ^ 1);
+    const int2 wk = work[w];
+    const LatDesc& D = descs[wk.x];
+    if (!__syncthreads_and(mbar_wait(&sm.bar[st], (uint32_t)((j >> 1) & 1), 1 << 22))) {
+      if (threadIdx.x == 0) atomicOr(&D.ctl->status, 4);
+      // the next brick's copies land before the CTA leaves (bounded)
+      if (wn < nwork) mbar_wait(&sm.bar[st ^ 1], (uint32_t)(((j + 1) >> 1) & 1), 1 << 22);
+      return;
+    }
+    body(D, wk.y, sm.head[st], sm.tile[st]);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // P2: grad_cd(c), Laplacian(c) with the wetting term, mu, velocity/pressure
 // correction (reference k_grad_cd_mf :897-913, k_pack_lap_c :159-165,
 // k_lap_mf :996-1010, k_mu_axpy :149-153, k_vel_press_corr :177-196).
@@ -755,24 +810,13 @@ __device__ __forceinline__ int64_t node_of(const LatDesc& D, int brick, int slot
   return x + (int64_t)D.nx * (y + (int64_t)D.ny * z);
 }
 
+// One brick of P2 from its staged halo-1 tile of c (s_c) and head (s).
 template <class S, class Sh, int OUT, bool HBB>
-__global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                 FieldOut out) {
+__device__ __forceinline__ void cfield_brick(const LatDesc& D, int brick, const Head<Sh>& s,
+                                             typename S::fld* __restrict__ s_c, const FieldOut& out) {
   using R = typename S::real;
   using F = typename S::fld;
   using T = TileX<Sh, 1>;
-  __shared__ Head<Sh> s;
-  __shared__ uint64_t s_bar;
-  __shared__ __align__(128) F s_c[T::N];
-  const int2 wk = work[blockIdx.x];
-  const LatDesc& D = descs[wk.x];
-  head_init(&s_bar);
-  if (threadIdx.x == 0) {
-    head_begin<Sh>(D, wk.y, s, &s_bar, (uint32_t)sizeof(s_c));
-    tile_copy<Sh, 1>(s_c, D, TM_C1, s.bx, s.by, s.bz, &s_bar);
-  }
-  if (threadIdx.x == CTA - 1) load_step_scalars(D, s);
-  if (!head_wait(D, &s_bar)) return;
   correct_tile<T::N, CTA>(s_c, s.lambda);
   __syncthreads();
   const DevPrm& Pm = D.prm;
@@ -796,12 +840,12 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
     if (flag & BC_SITE) {
       fcp[di] = V2<F>((F)c0, fp[di]);
       if (OUT) {
-        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, slot) : (int64_t)D.ref_of[i];
+        const int64_t q = OUT == 2 ? node_of<Sh>(D, brick, slot) : (int64_t)D.ref_of[i];
         const F* ub = static_cast<const F*>(D.u_bc);
         out.put(q, (double)c0, (double)(rho1 + drho * c0), (double)ub[i], (double)ub[D.n + i],
                 (double)ub[2 * D.n + i], (double)fp[di], (double)fmu[di]);
       } else if (D.snap_u[0]) {
-        const int64_t q = node_of<Sh>(D, wk.y, slot);
+        const int64_t q = node_of<Sh>(D, brick, slot);
         const F* ub = static_cast<const F*>(D.u_bc);
         D.snap_u[0][q] = (double)ub[i];
         D.snap_u[1][q] = (double)ub[D.n + i];
@@ -811,28 +855,34 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
       continue;  // fields resolved by the open-boundary kernels
     }
     const R bnd = bnd_coeff * c0 * (R(1) - c0);
-    // opposite pairs: the central difference is antisymmetric and the
-    // Laplacian term symmetric, so each pair counts its leading direction twice
-    R gx = 0, gy = 0, gz = 0, lap = 0;
+    // opposite pairs: the Laplacian term is symmetric and the central
+    // difference antisymmetric, so each pair counts its leading direction twice
+    R lap = 0;
 #pragma unroll
     for (int k = 1; k < Q; k += 2) {
       const R cm = (R)s_c[pos - T::off(k)], cp = (R)s_c[pos + T::off(k)];
       const R aw2 = R(2) * alpha * weight<R>(k);
-      const bool sm = is_site(cm), sp = is_site(cp);
-      const R cdv = cd_sel<HBB>(c0, cm, cp, sm, sp);
-      if (lat_cx(k)) gx += aw2 * R(lat_cx(k)) * cdv;
-      if (lat_cy(k)) gy += aw2 * R(lat_cy(k)) * cdv;
-      if (lat_cz(k)) gz += aw2 * R(lat_cz(k)) * cdv;
-      lap += aw2 * lap_sel<HBB>(c0, cm, cp, bnd, sm, sp);
+      lap += aw2 * lap_sel<HBB>(c0, cm, cp, bnd, is_site(cm), is_site(cp));
     }
     const R rho = rho1 + drho * c0;
     const R mu = four_beta * (c0 * (R(1) - c0)) * (R(0.5) - c0) + (-kappa * lap);
     fmu[di] = (F)mu;
     const F p_in = fp[di];
     // the correction changes p only through drho (k_vel_press_corr :194-195);
-    // u is needed here only for that, for output, or for the tracers' snapshot
+    // u (and the gradient of c) is needed here only for that, for output, or
+    // for the tracers' snapshot
     if (Pm.drho == 0.0) fcp[di] = V2<F>((F)c0, p_in);
     if (Pm.drho != 0.0 || OUT || D.snap_u[0]) {
+      R gx = 0, gy = 0, gz = 0;
+#pragma unroll
+      for (int k = 1; k < Q; k += 2) {
+        const R cm = (R)s_c[pos - T::off(k)], cp = (R)s_c[pos + T::off(k)];
+        const R aw2 = R(2) * alpha * weight<R>(k);
+        const R cdv = cd_sel<HBB>(c0, cm, cp, is_site(cm), is_site(cp));
+        if (lat_cx(k)) gx += aw2 * R(lat_cx(k)) * cdv;
+        if (lat_cy(k)) gy += aw2 * R(lat_cy(k)) * cdv;
+        if (lat_cz(k)) gz += aw2 * R(lat_cz(k)) * cdv;
+      }
       const R irho = R(1) / rho;
       const R inv = irho * R(1.0 / CS2);
       const R mor = mu * irho;
@@ -845,10 +895,10 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
         fcp[di] = V2<F>((F)c0, (F)p);
       }
       if (OUT) {
-        const int64_t q = OUT == 2 ? node_of<Sh>(D, wk.y, slot) : (int64_t)D.ref_of[i];
+        const int64_t q = OUT == 2 ? node_of<Sh>(D, brick, slot) : (int64_t)D.ref_of[i];
         out.put(q, (double)c0, (double)rho, (double)ux, (double)uy, (double)uz, (double)p, (double)mu);
       } else if (D.snap_u[0]) {
-        const int64_t q = node_of<Sh>(D, wk.y, slot);
+        const int64_t q = node_of<Sh>(D, brick, slot);
         D.snap_u[0][q] = (double)ux;
         D.snap_u[1][q] = (double)uy;
         D.snap_u[2][q] = (double)uz;
@@ -858,27 +908,34 @@ __global__ void __launch_bounds__(CTA) k_cfield(const LatDesc* __restrict__ desc
   }
 }
 
+// P2 over `nwork` bricks on a persistent grid (at most the CTAs that fit
+// the GPU at once): four CTAs an SM with FP32 arithmetic (64 registers),
+// three with FP64.
+template <class S>
+struct CfieldMinBlocks {
+  static constexpr int value = sizeof(typename S::real) == 8 ? 3 : 4;
+};
+template <class S, class Sh, int OUT, bool HBB>
+__global__ void __launch_bounds__(CTA, CfieldMinBlocks<S>::value)
+    k_cfield(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int nwork, FieldOut out) {
+  using F = typename S::fld;
+  __shared__ __align__(128) StencilStages<Sh, F, TileX<Sh, 1>::N> sm;
+  stencil_pipeline<Sh, F, 1, true>(descs, work, nwork, TM_C1, sm,
+                                   [&](const LatDesc& D, int brick, const Head<Sh>& s, F* s_c) {
+                                     cfield_brick<S, Sh, OUT, HBB>(D, brick, s, s_c, out);
+                                   });
+}
+
 // ---------------------------------------------------------------------------
 // P3: Laplacian of mu, boundary half zero (reference k_pack_lap_zero :168-173
-// + k_lap_mf); symmetric within an opposite pair.
+// + k_lap_mf); symmetric within an opposite pair. Persistent like P2.
 // ---------------------------------------------------------------------------
 template <class S, class Sh, bool HBB>
-__global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
+__device__ __forceinline__ void lapmu_brick(const LatDesc& D, const Head<Sh>& s,
+                                            const typename S::fld* __restrict__ s_m) {
   using R = typename S::real;
   using F = typename S::fld;
   using T = TileX<Sh, 1>;
-  __shared__ Head<Sh> s;
-  __shared__ uint64_t s_bar;
-  __shared__ __align__(128) F s_m[T::N];
-  const int2 wk = work[blockIdx.x];
-  const LatDesc& D = descs[wk.x];
-  head_init(&s_bar);
-  if (threadIdx.x == 0) {
-    head_begin<Sh>(D, wk.y, s, &s_bar, (uint32_t)sizeof(s_m));
-    tile_copy<Sh, 1>(s_m, D, TM_MU1, s.bx, s.by, s.bz, &s_bar);
-  }
-  if (!head_wait(D, &s_bar)) return;
-
   const R alpha = R(ALPHA);
   F* __restrict__ flm = static_cast<F*>(D.lapmu);
   const int cnt = s.cnt;
@@ -894,6 +951,17 @@ __global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs
     }
     flm[grid_entry<Sh>(D, s.bx, s.by, s.bz, slot)] = (F)lap;
   }
+}
+
+template <class S, class Sh, bool HBB>
+__global__ void __launch_bounds__(CTA) k_lapmu(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                int nwork) {
+  using F = typename S::fld;
+  __shared__ __align__(128) StencilStages<Sh, F, TileX<Sh, 1>::N> sm;
+  stencil_pipeline<Sh, F, 1, false>(descs, work, nwork, TM_MU1, sm,
+                                    [&](const LatDesc& D, int, const Head<Sh>& s, F* s_m) {
+                                      lapmu_brick<S, Sh, HBB>(D, s, s_m);
+                                    });
 }
 
 // P4 (k_collide) lives in collide.cuh.
@@ -1050,10 +1118,10 @@ __global__ void k_bc_final(const LatDesc* __restrict__ descs, int lat) {
 // Grid positions outside the lattice (node coordinates outside [0, n) on an
 // axis) whose wrapped node is fluid: image[j] = {grid entry, entry of the
 // node it wraps to}, built on the host. Each work item (lattice, block) copies
-// IMG_BLOCK of them for the fields in `fields` (bit 0 c, 1 p, 2 mu, 3 lap mu,
-// 4 the (c', p') pairs). Sources are lattice nodes, never images.
+// IMG_BLOCK of them for the fields in `fields` (bit 0 c, 1 mu, 2 lap mu,
+// 3 the (c', p') pairs). Sources are lattice nodes, never images.
 constexpr int IMG_BLOCK = CTA;
-enum : int { GF_C = 1, GF_P = 2, GF_MU = 4, GF_LAPMU = 8, GF_CP = 16 };
+enum : int { GF_C = 1, GF_MU = 2, GF_LAPMU = 4, GF_CP = 8 };
 template <class F>
 __global__ void __launch_bounds__(CTA) k_images(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                  int fields) {
@@ -1062,9 +1130,9 @@ __global__ void __launch_bounds__(CTA) k_images(const LatDesc* __restrict__ desc
   const int64_t j = (int64_t)wk.y * IMG_BLOCK + threadIdx.x;
   if (j >= D.n_images) return;
   const int2 e = __ldg(&D.images[j]);
-  F* const f[4] = {static_cast<F*>(D.c), static_cast<F*>(D.p), static_cast<F*>(D.mu), static_cast<F*>(D.lapmu)};
+  F* const f[3] = {static_cast<F*>(D.c), static_cast<F*>(D.mu), static_cast<F*>(D.lapmu)};
 #pragma unroll
-  for (int b = 0; b < 4; ++b)
+  for (int b = 0; b < 3; ++b)
     if (fields & (1 << b)) f[b][e.x] = f[b][e.y];
   if (fields & GF_CP) {
     V2<F>* cp = static_cast<V2<F>*>(D.cp);

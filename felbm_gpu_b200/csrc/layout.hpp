@@ -122,7 +122,8 @@ struct LatDesc {
   // state: pop[buffer][0 = h, 1 = g]
   void* pop[2][2];
   // fields (FP64 for FP64 storage, FP32 otherwise). The stencil fields c,
-  // p, mu and lap(mu) live on a dense node grid covering node coordinates
+  // p, mu, lap(mu) and the (c', p') pairs live on a dense node grid covering
+  // node coordinates
   // [-2, nb * B + 2) per axis (z: [0, 1) without a z halo), x fastest;
   // solid nodes hold NaN, and positions outside the lattice hold the
   // periodic image of the node they wrap to (k_images copies those of fluid
@@ -130,7 +131,9 @@ struct LatDesc {
   // then one box of the grid, loaded by one TMA copy. The momentum jx, jy, jz
   // is per site. cp is the grid of (c', p') pairs that P2 writes for the
   // collision: the order parameter with the queued mass correction applied
-  // and the corrected pressure, interleaved.
+  // and the corrected pressure, interleaved. P2 writes each pair whole (with
+  // P1 storing p into the second lane and P2 the order parameter into the
+  // first, P2 ran six times slower; the cause was not found).
   void *c, *p, *jx, *jy, *jz, *mu, *lapmu, *cp;
   int gdx, gdy, gdz;           // grid extents (gdx a multiple of 16 bytes of entries)
   int hz;                      // 1: the z axis has a halo (3-D bricks)
