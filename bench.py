@@ -65,6 +65,8 @@ def parse():
                     help="skip the layout autotuner (default bricks, two steps per graph launch)")
     ap.add_argument("--brick", default="auto", choices=["auto", "8x8x8", "8x8x4", "16x8x8"],
                     help="force a brick shape (skips the autotuner)")
+    ap.add_argument("--pop-layout", default="two_buffers", choices=["two_buffers", "in_place"],
+                    help="population layout of the benched engine (in_place: one buffer, AA pattern)")
     ap.add_argument("--sweep-steps", type=int, default=5000, help="steps per solve of the 64-solve sweep")
     ap.add_argument("--stream-seconds", type=float, default=15.0, help="arrival window of the request stream")
     ap.add_argument("--stream-rate", type=float, default=4.0, help="Poisson arrival rate (requests / s)")
@@ -680,6 +682,7 @@ def main():
     from felbm_gpu_b200 import _capi
     solid, por, p, h0, g0 = workload(args.size, seed=args.seed + rank)
     p.storage = _capi.STORAGE[args.storage]
+    p.pop_layout = 1 if args.pop_layout == "in_place" else 0
     tuned = None
     if args.brick != "auto":
         p.brick = _capi.BRICK[args.brick]
@@ -826,7 +829,7 @@ def main():
                                        f"slab IC, {args.storage} populations",
                            "sites": int(n), "porosity": por, "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (state > 1 GB), no flush",
-                           "layout": {"brick": brick, "graph_steps": graph_steps,
+                           "layout": {"brick": brick, "graph_steps": graph_steps, "populations": args.pop_layout,
                                       "autotune": tuned["candidates"] if tuned else None}},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk.summary(), "production": production, "serving": serving,

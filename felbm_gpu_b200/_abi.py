@@ -32,6 +32,7 @@ class FeParams(C.Structure):
         ("storage", C.c_int),
         ("c_ref", C.c_double), ("p_ref", C.c_double),
         ("brick", C.c_int), ("graph_steps", C.c_int),
+        ("pop_layout", C.c_int),
     ]
 
 

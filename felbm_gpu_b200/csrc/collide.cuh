@@ -77,9 +77,13 @@ struct SiteScal {
   R hdr, u_drm, u_fg_f, drho_cs2;
 };
 
-template <class S, class Sh, int MRT, bool HBB, bool WIDE>
+// AAP: 0 two population buffers; 1, 2 the in-place layout from phase 0
+// (reads the own slots, writes f*_k into the own slot opp(k)) and from phase
+// 1 (reads f_k where the last step left it, pushes like the two-buffer pass).
+template <class S, class Sh, int MRT, bool HBB, bool WIDE, int AAP = 0>
 __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
+  static_assert(AAP == 0 || !WIDE, "the in-place layout takes 32-bit population offsets");
   using R = typename S::real;
   using V = V2<R>;
   using PH = typename S::hpop;
@@ -153,12 +157,19 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     R g0 = ld_pop<GV<S>>(gin, a0, 0, shg);
     V gp[NPAIR];
 #pragma unroll
-    for (int k = 1; k < Q; k += 2)
-      gp[k >> 1] = V(ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg), ld_pop<GV<S>>(gin, a0 + (k + 1) * AOSOA, k + 1, shg));
+    for (int k = 1; k < Q; k += 2) {
+      if constexpr (AAP == 2)
+        gp[k >> 1] = V(ld_pop<GV<S>>(gin, aa_src<T1>(s_idx, pos1, (uint32_t)a0, k), k, shg),
+                       ld_pop<GV<S>>(gin, aa_src<T1>(s_idx, pos1, (uint32_t)a0, k + 1), k + 1, shg));
+      else
+        gp[k >> 1] = V(ld_pop<GV<S>>(gin, a0 + k * AOSOA, k, shg), ld_pop<GV<S>>(gin, a0 + (k + 1) * AOSOA, k + 1, shg));
+    }
     // push target of direction k: slot k of x + e_k, or slot opp(k) of x
     // (halfway bounce-back) when x + e_k is solid
     auto dst = [&](int k) -> IX {
-      if constexpr (WIDE) {
+      if constexpr (AAP == 1) {
+        return a0 + (IX)(lat_opp(k) * AOSOA);
+      } else if constexpr (WIDE) {
         const int dn = s_idx[pos1 + T1::off(k)];
         return dn >= 0 ? (IX)(dn >> 5) * (IX)(Q * AOSOA) + (IX)(k * AOSOA + (dn & (AOSOA - 1)))
                        : a0 + (IX)(lat_opp(k) * AOSOA);

@@ -242,9 +242,28 @@ static void launch_collide_w(bool wide, int nwork, size_t smem, cudaStream_t st,
   if (wide) k_collide<S, Sh, MRT, HBB, true><<<nwork, P4T, smem, st>>>(desc, work, par);
   else k_collide<S, Sh, MRT, HBB, false><<<nwork, P4T, smem, st>>>(desc, work, par);
 }
+// The in-place layout's two phases (aap 1: from the standard layout, 2: from
+// the swapped one), FP64 and FP32 storage with 32-bit offsets.
+template <class S>
+struct InPlaceStorage {
+  static constexpr bool value = std::is_same<S, StF32>::value || std::is_same<S, StF64>::value;
+};
+template <class S, class Sh, int AAP>
+static void launch_collide_aa(int mrt, bool hbb, int nwork, size_t smem, cudaStream_t st, const LatDesc* desc,
+                              const int2* work, int par) {
+  if constexpr (InPlaceStorage<S>::value) {
+    if (mrt == 2 && hbb) k_collide<S, Sh, 2, true, false, AAP><<<nwork, P4T, smem, st>>>(desc, work, par);
+    else if (mrt && hbb) k_collide<S, Sh, 1, true, false, AAP><<<nwork, P4T, smem, st>>>(desc, work, par);
+    else if (mrt) k_collide<S, Sh, 1, false, false, AAP><<<nwork, P4T, smem, st>>>(desc, work, par);
+    else if (hbb) k_collide<S, Sh, 0, true, false, AAP><<<nwork, P4T, smem, st>>>(desc, work, par);
+    else k_collide<S, Sh, 0, false, false, AAP><<<nwork, P4T, smem, st>>>(desc, work, par);
+  }
+}
 template <class S, class Sh>
 static void launch_collide(int mrt, bool hbb, bool wide, int nwork, size_t smem, cudaStream_t st,
-                           const LatDesc* desc, const int2* work, int par) {
+                           const LatDesc* desc, const int2* work, int par, int aap = 0) {
+  if (aap == 1) return launch_collide_aa<S, Sh, 1>(mrt, hbb, nwork, smem, st, desc, work, par);
+  if (aap == 2) return launch_collide_aa<S, Sh, 2>(mrt, hbb, nwork, smem, st, desc, work, par);
   if (mrt == 2 && hbb && !wide) k_collide<S, Sh, 2, true, false><<<nwork, P4T, smem, st>>>(desc, work, par);
   else if (mrt && hbb) launch_collide_w<S, Sh, 1, true>(wide, nwork, smem, st, desc, work, par);
   else if (mrt) launch_collide_w<S, Sh, 1, false>(wide, nwork, smem, st, desc, work, par);
@@ -288,6 +307,11 @@ static void launch_cfield(bool hbb, int nwork, cudaStream_t st, const LatDesc* d
   }
 }
 template <class S, class Sh>
+static void launch_moments_aa(int nwork, int write_j, cudaStream_t st, const LatDesc* desc, const int2* work) {
+  auto k = k_moments_aa<S, Sh>;
+  k<<<resident_grid((const void*)k, nwork), CTA, 0, st>>>(desc, work, nwork, write_j);
+}
+template <class S, class Sh>
 static void launch_lapmu(bool hbb, int nwork, cudaStream_t st, const LatDesc* desc, const int2* work) {
   if (nwork <= 0) return;
   if (hbb) {
@@ -314,6 +338,18 @@ static cudaError_t collide_smem_attr(int bytes) {
   set((const void*)k_collide<S, Sh, 1, true, false>);
   set((const void*)k_collide<S, Sh, 1, true, true>);
   set((const void*)k_collide<S, Sh, 2, true, false>);
+  if constexpr (InPlaceStorage<S>::value) {
+    set((const void*)k_collide<S, Sh, 0, false, false, 1>);
+    set((const void*)k_collide<S, Sh, 0, true, false, 1>);
+    set((const void*)k_collide<S, Sh, 1, false, false, 1>);
+    set((const void*)k_collide<S, Sh, 1, true, false, 1>);
+    set((const void*)k_collide<S, Sh, 2, true, false, 1>);
+    set((const void*)k_collide<S, Sh, 0, false, false, 2>);
+    set((const void*)k_collide<S, Sh, 0, true, false, 2>);
+    set((const void*)k_collide<S, Sh, 1, false, false, 2>);
+    set((const void*)k_collide<S, Sh, 1, true, false, 2>);
+    set((const void*)k_collide<S, Sh, 2, true, false, 2>);
+  }
   return e;
 }
 // cuTensorMapEncodeTiled from the driver (no link against libcuda), looked
@@ -343,6 +379,7 @@ struct Engine {
   int shape = 0;              // kShapeLb index
   int graph_steps = 2;        // steps per graph launch of fe_run
   int wide = 0;               // 64-bit population offsets in the collide pass
+  int aa = 0;                 // in-place population layout (one buffer; parity = its phase)
   int device = 0;
   HostLayout L;
   LatDesc hd{};               // host copy of the descriptor
@@ -524,6 +561,12 @@ struct Engine {
       const char* w = std::getenv("FELBM_WIDE_OFFSETS");
       wide = (pops_wide(L.n) || (w && w[0] == '1')) ? 1 : 0;
     }
+    aa = P.pop_layout == FE_POP_IN_PLACE ? 1 : 0;
+    if (P.pop_layout != FE_POP_TWO_BUFFERS && P.pop_layout != FE_POP_IN_PLACE)
+      return fe_fail(FE_ERR_ARG, "unknown pop_layout");
+    if (aa && storage != FE_F64 && storage != FE_F32)
+      return fe_fail(FE_ERR_ARG, "the in-place population layout takes FE_F64 or FE_F32 storage");
+    if (aa && wide) return fe_fail(FE_ERR_ARG, "the in-place population layout takes lattices below 2^32 population entries");
     const int nbk = L.nbricks();
     LatDesc& D = hd;
     D.nx = nx; D.ny = ny; D.nz = nz;
@@ -547,6 +590,10 @@ struct Engine {
     const size_t popn = (size_t)Q * D.n_pad;
     for (int b = 0; b < 2; ++b)
       for (int f = 0; f < 2; ++f) {
+        if (aa && b == 1) {  // one buffer: both phases address it
+          D.pop[1][f] = D.pop[0][f];
+          continue;
+        }
         unsigned char* q;
         if ((rc = alloc(&q, popn * pop_size(f)))) return rc;
         FE_CUDA(cudaMemset(q, 0, popn * pop_size(f)));
@@ -561,7 +608,7 @@ struct Engine {
       *f = q;
     }
     if ((rc = setup_grid(solid))) return rc;
-    if ((rc = alloc(&D.part1, (size_t)D.nchunks * 2))) return rc;
+    if ((rc = alloc(&D.part1, (size_t)std::max(D.nchunks, nbk) * 2))) return rc;  // per chunk, or per brick
     if ((rc = alloc(&D.part4, (size_t)nbk * P4W * 6))) return rc;
     FE_CUDA(cudaMemset(D.part4, 0, (size_t)nbk * P4W * 6 * 8));
     if ((rc = alloc(&d_partm, (size_t)D.nchunks * 2))) return rc;
@@ -724,7 +771,8 @@ struct Engine {
     auto rec = [&](int q) { if (ev) cudaEventRecord(ev[q], st); };
     using F = typename S::fld;
     rec(0);
-    k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
+    if (aa && par) launch_moments_aa<S, Sh>(nb, 0, st, d_desc, d_work);
+    else k_moments<S><<<hd.nchunks, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
     rec(1);
     if (open_bnd) launch_bc<S>(st);
     if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_C);
@@ -735,7 +783,8 @@ struct Engine {
     launch_lapmu<S, Sh>(hd.prm.hbb != 0, nb, st, d_desc, d_work);
     if (hd.image_blocks) k_images<F><<<hd.image_blocks, CTA, 0, st>>>(d_desc, d_iwork, GF_LAPMU);
     rec(4);
-    launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par);
+    launch_collide<S, Sh>(collide_variant(), hd.prm.hbb != 0, wide != 0, nb, smem_p4, st, d_desc, d_work, par,
+                          aa ? 1 + par : 0);
     rec(5);
     launches += hd.image_blocks ? 7 : 4;
   }
@@ -853,7 +902,24 @@ struct Engine {
     return FE_OK;
   }
 
+  // The in-place layout's phase 1 turned into the standard layout (phase 0)
+  // in place, before a pass that reads each site's own slots.
+  template <class S, class Sh>
+  void to_standard_t() {
+    k_aa_swap<S, Sh><<<hd.nbricks, CTA, 0, stream>>>(d_desc, d_work);
+    ++launches;
+  }
+  int to_standard() {
+    if (!aa || parity == 0) return FE_OK;
+    FE_DISPATCH(*this, to_standard_t<S FE_COMMA Sh>());
+    FE_CUDA(cudaGetLastError());
+    parity = 0;
+    return FE_OK;
+  }
+
   int mass_pass() {
+    int rc;
+    if ((rc = to_standard())) return rc;
     FE_DISPATCH(*this, (k_mass<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_partm)));
     ++launches;
     FE_CUDA(cudaGetLastError());
@@ -890,6 +956,7 @@ struct Engine {
     const int64_t Vn = (int64_t)Q * hd.n;
     int rc;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
+    if ((rc = to_standard())) return rc;
     Ctl c;
     if ((rc = read_ctl(&c))) return rc;
     int apply = 0;
@@ -947,7 +1014,7 @@ struct Engine {
     if ((rc = tracer_hook(-1, state_id, false))) return rc;
     if ((rc = read_ctl(&c))) return rc;
     if (!c.pending || !hd.prm.correct_mass) return FE_OK;
-    if ((rc = mass_pass())) return rc;
+    if ((rc = mass_pass())) return rc;  // (in the standard layout from here)
     FE_DISPATCH(*this, (k_inject<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity)));
     ++launches;
     FE_CUDA(cudaGetLastError());
@@ -963,6 +1030,7 @@ struct Engine {
     if ((rc = tracer_hook(-1, state_id, false))) return rc;  // deferred tracer advances see the old state
     ++state_id;
     if ((rc = ensure_tmp(2 * Vn))) return rc;
+    if (aa) parity = 0;  // the upload writes the standard layout
     Staging* sg = narrow_transfers(Vn);
     if (sg) {  // narrowed on the host, as the device's conversion would
       float* t = reinterpret_cast<float*>(d_tmp);
@@ -988,7 +1056,11 @@ struct Engine {
   // OUT 1: reference site order; OUT 2: node-indexed grids.
   template <class S, class Sh, int OUT>
   void fields_launch(FieldOut o) {
-    k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
+    if (aa && parity) {
+      launch_moments_aa<S, Sh>(hd.nbricks, 1, stream, d_desc, d_work);
+    } else {
+      k_moments<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, 1);
+    }
     if (open_bnd) launch_bc<S>(stream);
     if (hd.image_blocks)
       k_images<typename S::fld><<<hd.image_blocks, CTA, 0, stream>>>(d_desc, d_iwork, GF_C);
@@ -1744,6 +1816,8 @@ int fe_set_params(fe_engine* e, const fe_params* p) {
   FE_GUARD(e);
   if (!p) return fe_fail(FE_ERR_ARG, "null params");
   if (p->storage != e->e.storage) return fe_fail(FE_ERR_ARG, "storage cannot change after create");
+  if ((p->pop_layout == FE_POP_IN_PLACE) != (e->e.aa != 0))
+    return fe_fail(FE_ERR_ARG, "pop_layout cannot change after create");
   if (p->correct_op_mass && e->e.open_bnd)
     return fe_fail(FE_ERR_ARG, "correct_op_mass must be false with open boundaries");
   // fill_prm leaves the open-boundary block of fe_set_open_bnd untouched
@@ -2072,6 +2146,7 @@ int fe_batch_destroy(fe_batch* b) {
 int fe_batch_add(fe_batch* b, fe_engine* e) {
   FE_BGUARD(b);
   FE_GUARD(e);
+  if (e->e.aa) return fe_fail(FE_ERR_ARG, "engines with the in-place population layout do not join batches");
   return b->b.add(&e->e);
 }
 

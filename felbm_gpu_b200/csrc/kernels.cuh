@@ -404,8 +404,10 @@ __device__ __forceinline__ void head_begin(const LatDesc& D, int brick, Head<Sh>
   s.bx = __ldg(&D.brick_xyz[3 * brick + 0]);
   s.by = __ldg(&D.brick_xyz[3 * brick + 1]);
   s.bz = __ldg(&D.brick_xyz[3 * brick + 2]);
-  mbar_arrive_expect_tx(bar, tile_bytes + (uint32_t)(Sh::C * sizeof(uint16_t)));
-  bulk_g2s(s.slot_of, D.slots + (int64_t)brick * Sh::C, (uint32_t)(Sh::C * sizeof(uint16_t)), bar);
+  // the slot list up to the brick's site count, in whole 16-byte pieces
+  const uint32_t sb = ((uint32_t)s.cnt * (uint32_t)sizeof(uint16_t) + 15u) & ~15u;
+  mbar_arrive_expect_tx(bar, tile_bytes + sb);
+  bulk_g2s(s.slot_of, D.slots + (int64_t)brick * Sh::C, sb, bar);
 }
 
 // Every thread waits for the prologue's copies (bounded). False in every
@@ -601,6 +603,224 @@ __global__ void __launch_bounds__(CTA) k_moments(const LatDesc* __restrict__ des
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent, double-buffered brick pipeline (P2, P3, in-place P1):
+// a CTA takes the work items blockIdx.x, blockIdx.x + gridDim.x, ... and
+// while it computes one brick from one stage, the copy engine fills the
+// other stage with the next brick's head, slot list and halo-H tile (one
+// mbarrier per stage, phases counted per use). The block barrier after each
+// wait orders the next issue into a stage after every thread has left it.
+// ---------------------------------------------------------------------------
+template <class Sh, class F, int N>
+struct StencilStages {
+  // each stage's tile starts on a 128-byte boundary (a TMA destination)
+  static constexpr int NA = ((N * (int)sizeof(F) + 127) / 128 * 128) / (int)sizeof(F);
+  F tile[2][NA];
+  Head<Sh> head[2];
+  uint64_t bar[2];
+};
+
+// copies(D, brick, head, tile, bar), run by thread 0, starts a brick's
+// copies on bar (head_begin and the tile's copy); body(D, brick, head, tile)
+// computes it, every thread.
+template <class Sh, class F, int N, bool SCALARS, class Copies, class Body>
+__device__ __forceinline__ void brick_pipeline(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                               int nwork, StencilStages<Sh, F, N>& sm, Copies&& copies,
+                                               Body&& body) {
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.bar[0]);
+    mbar_init(&sm.bar[1]);
+  }
+  __syncthreads();
+  auto issue = [&](int item, int st) {
+    if (threadIdx.x == 0) {
+      const int2 wk = work[item];
+      copies(descs[wk.x], wk.y, sm.head[st], sm.tile[st], &sm.bar[st]);
+    }
+    if (SCALARS && threadIdx.x == CTA - 1) load_step_scalars(descs[work[item].x], sm.head[st]);
+  };
+  int w = blockIdx.x;
+  if (w < nwork) issue(w, 0);
+  for (int j = 0; w < nwork; w += (int)gridDim.x, ++j) {
+    const int st = j & 1, wn = w + (int)gridDim.x;
+    if (wn < nwork) issue(wn, st ^ 1);
+    const int2 wk = work[w];
+    const LatDesc& D = descs[wk.x];
+    if (!__syncthreads_and(mbar_wait(&sm.bar[st], (uint32_t)((j >> 1) & 1), 1 << 22))) {
+      if (threadIdx.x == 0) atomicOr(&D.ctl->status, 4);
+      // the next brick's copies land before the CTA leaves (bounded)
+      if (wn < nwork) mbar_wait(&sm.bar[st ^ 1], (uint32_t)(((j + 1) >> 1) & 1), 1 << 22);
+      return;
+    }
+    body(D, wk.y, sm.head[st], sm.tile[st]);
+    __syncthreads();
+  }
+}
+
+// The stencil passes' pipeline: the halo-H box of the field grid `tmap_id`.
+template <class Sh, class F, int H, bool SCALARS, class Body>
+__device__ __forceinline__ void stencil_pipeline(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                 int nwork, int tmap_id, StencilStages<Sh, F, TileX<Sh, H>::N>& sm,
+                                                 Body&& body) {
+  using T = TileX<Sh, H>;
+  brick_pipeline<Sh, F, T::N, SCALARS>(
+      descs, work, nwork, sm,
+      [&](const LatDesc& D, int brick, Head<Sh>& h, F* tile, uint64_t* bar) {
+        head_begin<Sh>(D, brick, h, bar, (uint32_t)(T::N * sizeof(F)));
+        tile_copy<Sh, H>(tile, D, tmap_id, h.bx, h.by, h.bz, bar);
+      },
+      body);
+}
+
+// ---------------------------------------------------------------------------
+// The in-place (AA) population layout keeps one buffer. A step taken from the
+// standard layout (phase 0) writes each site's post-collision f*_k into its
+// own slot opp(k); the state between the two steps is then: post-stream
+// f_k(x) = f*_k(x - e_k), found in slot opp(k) of the upstream site x - e_k,
+// or, when x - e_k is solid (halfway bounce-back), in x's own slot k (phase
+// 1). A step taken from phase 1 reads there and pushes f*_k into slot k of
+// x + e_k (or slot opp(k) of x), which is the standard layout again. Both
+// steps read and write the same 19 slots per site, so no other site's data
+// is overwritten before it is read.
+// ---------------------------------------------------------------------------
+// AoSoA index of the post-stream population k of the site at base a0 (slot
+// position pos1 in the brick's halo-1 tile of population bases) in phase 1.
+template <class T1>
+__device__ __forceinline__ uint32_t aa_src(const int32_t* __restrict__ s_idx, int pos1, uint32_t a0, int k) {
+  const uint32_t b = (uint32_t)s_idx[pos1 - T1::off(k)];
+  return b != 0xffffffffu ? b + (uint32_t)(lat_opp(k) * AOSOA) : a0 + (uint32_t)(k * AOSOA);
+}
+
+// P1 from phase 1 of the in-place layout: the same moments and writes as
+// k_moments, on the persistent brick pipeline (the halo-1 tile of population
+// bases by bulk copy); mass partials per brick, summed by the CTA that
+// finishes last (one lattice per launch: in-place engines do not batch).
+template <class S, class Sh>
+__global__ void __launch_bounds__(CTA, 4) k_moments_aa(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
+                                                     int nwork, int write_j) {
+  using R = typename S::real;
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
+  using F = typename S::fld;
+  using T1 = Tile<Sh, 1>;
+  __shared__ __align__(128) StencilStages<Sh, int32_t, T1::N> sm;
+  __shared__ Red red;
+  brick_pipeline<Sh, int32_t, T1::N, false>(
+      descs, work, nwork, sm,
+      [&](const LatDesc& D, int brick, Head<Sh>& h, int32_t* tile, uint64_t* bar) {
+        head_begin<Sh>(D, brick, h, bar, (uint32_t)(T1::N * 4));
+        bulk_g2s(tile, D.tile1 + (int64_t)brick * T1::N, (uint32_t)(T1::N * 4), bar);
+      },
+      [&](const LatDesc& D, int brick, const Head<Sh>& s, const int32_t* s_idx) {
+        const PH* __restrict__ hin = static_cast<const PH*>(D.pop[0][0]);
+        const PG* __restrict__ gin = static_cast<const PG*>(D.pop[0][1]);
+        F* __restrict__ fc = static_cast<F*>(D.c);
+        F* __restrict__ fp = static_cast<F*>(D.p);
+        F* __restrict__ fjx = static_cast<F*>(D.jx);
+        F* __restrict__ fjy = static_cast<F*>(D.jy);
+        F* __restrict__ fjz = static_cast<F*>(D.jz);
+        const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
+        const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
+        const int wj = write_j | D.prm.need_j;
+        double acc[2] = {0.0, 0.0};
+        for (int r = threadIdx.x; r < s.cnt; r += CTA) {
+          const int64_t i = s.first + r;
+          const int slot = s.slot_of[r];
+          const int pos1 = T1::pos(slot);
+          const uint32_t a0 = (uint32_t)pbase(i);
+          R hv[Q], gv[Q];
+#pragma unroll
+          for (int k = 0; k < Q; ++k) {
+            const uint32_t a = k == 0 ? a0 : aa_src<T1>(s_idx, pos1, a0, k);
+            hv[k] = ld_pop<HV<S>>(hin, a, k, shh);
+            gv[k] = ld_pop<GV<S>>(gin, a, k, shg);
+          }
+          R c = 0, p = 0, jx = 0, jy = 0, jz = 0;
+          double cd = 0.0;
+#pragma unroll
+          for (int k = 0; k < Q; ++k) {
+            c += hv[k];
+            cd += (double)hv[k];
+            p += gv[k];
+            if (lat_cx(k)) jx += R(lat_cx(k)) * gv[k];
+            if (lat_cy(k)) jy += R(lat_cy(k)) * gv[k];
+            if (lat_cz(k)) jz += R(lat_cz(k)) * gv[k];
+          }
+          const int64_t de = grid_entry<Sh>(D, s.bx, s.by, s.bz, slot);
+          fc[de] = (F)c;
+          fp[de] = (F)p;
+          if (wj) {
+            fjx[i] = (F)jx;
+            fjy[i] = (F)jy;
+            fjz[i] = (F)jz;
+          }
+          double phi = cd * (1.0 - cd);
+          if (phi < 0.0) phi = 0.0;
+          acc[0] += cd;
+          acc[1] += phi;
+        }
+        if (!D.prm.correct_mass) return;
+        block_sum<2>(acc, red);
+        if (threadIdx.x == 0) {
+          D.part1[(int64_t)brick * 2 + 0] = acc[0];
+          D.part1[(int64_t)brick * 2 + 1] = acc[1];
+        }
+      });
+  if (blockIdx.x >= nwork) return;
+  const LatDesc& D = descs[work[blockIdx.x].x];
+  if (!D.prm.correct_mass) return;
+  if (!last_block(&D.ctl->count1, gridDim.x, red)) return;
+  double tot[2];
+  sum_partials<2>(D.part1, D.nbricks, 2, tot, red);
+  if (threadIdx.x == 0) {
+    finish_mass(D.ctl, tot[0], tot[1]);
+    D.ctl->count1 = 0;
+  }
+}
+
+// Phase 1 of the in-place layout to the standard layout, in place: for the
+// leading direction k of each opposite pair, slot k of x (holding f*_opp(k)
+// of x, bound for x - e_k) and slot opp(k) of x - e_k (holding f*_k of
+// x - e_k, bound for x) trade places; with x - e_k solid both are where the
+// standard layout keeps them. Every slot takes part in at most one trade.
+template <class S, class Sh>
+__global__ void __launch_bounds__(CTA) k_aa_swap(const LatDesc* __restrict__ descs, const int2* __restrict__ work) {
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
+  using T1 = Tile<Sh, 1>;
+  __shared__ Head<Sh> s;
+  __shared__ uint64_t s_bar;
+  __shared__ __align__(128) int32_t s_idx[T1::N];
+  const int2 wk = work[blockIdx.x];
+  const LatDesc& D = descs[wk.x];
+  const int brick = wk.y;
+  head_init(&s_bar);
+  if (threadIdx.x == 0) {
+    head_begin<Sh>(D, brick, s, &s_bar, (uint32_t)(T1::N * 4));
+    bulk_g2s(s_idx, D.tile1 + (int64_t)brick * T1::N, (uint32_t)(T1::N * 4), &s_bar);
+  }
+  if (!head_wait(D, &s_bar)) return;
+  PH* __restrict__ h = static_cast<PH*>(D.pop[0][0]);
+  PG* __restrict__ g = static_cast<PG*>(D.pop[0][1]);
+  for (int r = threadIdx.x; r < s.cnt; r += CTA) {
+    const int slot = s.slot_of[r];
+    const int pos1 = T1::pos(slot);
+    const uint32_t a0 = (uint32_t)pbase(s.first + r);
+#pragma unroll
+    for (int k = 1; k < Q; k += 2) {
+      const uint32_t b = (uint32_t)s_idx[pos1 - T1::off(k)];
+      if (b == 0xffffffffu) continue;
+      const uint32_t x = a0 + (uint32_t)(k * AOSOA), y = b + (uint32_t)((k + 1) * AOSOA);
+      const PH hx = h[x], hy = h[y];
+      h[x] = hy;
+      h[y] = hx;
+      const PG gx = g[x], gy = g[y];
+      g[x] = gy;
+      g[y] = gx;
+    }
+  }
+}
+
 // corrected order parameter c' = c - lambda * max(c(1-c), 0): the reference's
 // k_inject_mass (device_engine.cuh:1128-1139) applied to c instead of h; h is
 // never read by the collision (the h update is eq_h + force_h), so the next
@@ -722,61 +942,6 @@ __device__ __forceinline__ R lap_sel(R f0, R fm, R fp, R bnd, bool sm, bool sp) 
   const R f1v = sm ? fm : fp;
   const R one = HBB ? (f1v - f0 - bnd) : (R(2) * f1v - R(2) * f0 - R(2) * bnd);
   return (sm && sp) ? both : ((sm || sp) ? one : R(0));
-}
-
-// ---------------------------------------------------------------------------
-// Persistent, double-buffered brick pipeline of the stencil passes P2 and P3:
-// a CTA takes the work items blockIdx.x, blockIdx.x + gridDim.x, ... and
-// while it computes one brick from one stage, the copy engine fills the
-// other stage with the next brick's head, slot list and halo-H tile (one
-// mbarrier per stage, phases counted per use). The block barrier after each
-// wait orders the next issue into a stage after every thread has left it.
-// ---------------------------------------------------------------------------
-template <class Sh, class F, int N>
-struct StencilStages {
-  // each stage's tile starts on a 128-byte boundary (a TMA destination)
-  static constexpr int NA = ((N * (int)sizeof(F) + 127) / 128 * 128) / (int)sizeof(F);
-  F tile[2][NA];
-  Head<Sh> head[2];
-  uint64_t bar[2];
-};
-
-template <class Sh, class F, int H, bool SCALARS, class Body>
-__device__ __forceinline__ void stencil_pipeline(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
-                                                 int nwork, int tmap_id, StencilStages<Sh, F, TileX<Sh, H>::N>& sm,
-                                                 Body&& body) {
-  using T = TileX<Sh, H>;
-  if (threadIdx.x == 0) {
-    mbar_init(&sm.bar[0]);
-    mbar_init(&sm.bar[1]);
-  }
-  __syncthreads();
-  auto issue = [&](int item, int st) {
-    if (threadIdx.x == 0) {
-      const int2 wk = work[item];
-      const LatDesc& D = descs[wk.x];
-      Head<Sh>& h = sm.head[st];
-      head_begin<Sh>(D, wk.y, h, &sm.bar[st], (uint32_t)(T::N * sizeof(F)));
-      tile_copy<Sh, H>(sm.tile[st], D, tmap_id, h.bx, h.by, h.bz, &sm.bar[st]);
-    }
-    if (SCALARS && threadIdx.x == CTA - 1) load_step_scalars(descs[work[item].x], sm.head[st]);
-  };
-  int w = blockIdx.x;
-  if (w < nwork) issue(w, 0);
-  for (int j = 0; w < nwork; w += (int)gridDim.x, ++j) {
-    const int st = j & 1, wn = w + (int)gridDim.x;
-    if (wn < nwork) issue(wn, st ^ 1);
-    const int2 wk = work[w];
-    const LatDesc& D = descs[wk.x];
-    if (!__syncthreads_and(mbar_wait(&sm.bar[st], (uint32_t)((j >> 1) & 1), 1 << 22))) {
-      if (threadIdx.x == 0) atomicOr(&D.ctl->status, 4);
-      // the next brick's copies land before the CTA leaves (bounded)
-      if (wn < nwork) mbar_wait(&sm.bar[st ^ 1], (uint32_t)(((j + 1) >> 1) & 1), 1 << 22);
-      return;
-    }
-    body(D, wk.y, sm.head[st], sm.tile[st]);
-    __syncthreads();
-  }
 }
 
 // ---------------------------------------------------------------------------

@@ -38,6 +38,8 @@ def default_params(**kw) -> capi.FeParams:
             v = capi.STORAGE[v]
         if k == "brick" and isinstance(v, str):
             v = capi.BRICK[v]
+        if k == "pop_layout" and isinstance(v, str):
+            v = {"two_buffers": 0, "in_place": 1}[v]
         if k in ("mrt_rate_mode", "mrt_rate_value"):
             arr = getattr(p, k)
             for i, x in v.items() if isinstance(v, dict) else enumerate(v):

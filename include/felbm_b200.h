@@ -104,7 +104,20 @@ typedef struct fe_params {
    * tuned or default 2) */
   int brick;
   int graph_steps;
+  /* population layout (no reference counterpart; the reference's own
+   * in-place streaming is the op program of stream_inplace): FE_POP_TWO_BUFFERS
+   * (default) streams from one buffer into the other; FE_POP_IN_PLACE keeps
+   * one buffer and alternates the two phases of the AA pattern (a step from
+   * the standard layout writes each site's post-collision populations into
+   * its own opposite slots; the next step reads them from the upstream sites
+   * and pushes its results to the downstream ones, which restores the
+   * standard layout). Half the population memory; FE_F64 and FE_F32 storage,
+   * lattices whose population arrays stay below 2^32 entries, not in batches. */
+  int pop_layout;
 } fe_params;
+
+#define FE_POP_TWO_BUFFERS 0
+#define FE_POP_IN_PLACE 1
 
 /* Brick shapes. 16x16x1 is the one for lattices with nz == 1; 8x8x4 exists
  * for FE_F64 and FE_F32 storage. Without a tuned choice, 3-D lattices get
@@ -358,7 +371,8 @@ int fe_mass_weight_noalloc(const double* d_h, int64_t n, double* d_out, void* st
  * behaves as fe_run on every member (queued mass correction after each step,
  * forcing factor from the step counter) and returns when the steps are done.
  * Engines stay usable on their own between batch runs; fe_engine_destroy of
- * a member removes it first. */
+ * a member removes it first. Engines with the in-place population layout
+ * (FE_POP_IN_PLACE) are refused (FE_ERR_ARG). */
 typedef struct fe_batch fe_batch;
 int fe_batch_create(int device, fe_batch** out);
 int fe_batch_destroy(fe_batch* b);
