@@ -1131,7 +1131,7 @@ struct Engine {
 // ---------------------------------------------------------------------------
 struct Batch {
   struct Group {
-    int shape = 0, mrt = 0, hbb = 0, wide = 0;
+    int shape = 0, mrt = 0, hbb = 0, wide = 0, aa = 0;
     int2* d_work = nullptr;
     int nwork = 0;
   };
@@ -1145,8 +1145,12 @@ struct Batch {
   int2* d_cwork = nullptr;
   int2* d_gwork = nullptr;          // the groups' work lists, one after another
   int2* d_iwork = nullptr;          // the members' image-refresh blocks
+  int2* d_cwork_std = nullptr;      // chunks of the two-buffer members
+  int2* d_bwork_aa = nullptr;       // bricks of the in-place members (their phase-1 P1)
   size_t cap_desc = 0, cap_cwork = 0, cap_gwork = 0, cap_iwork = 0;  // bytes (grow-only)
-  int ncwork = 0, niwork = 0;
+  size_t cap_cwork_std = 0, cap_bwork_aa = 0;
+  int ncwork = 0, niwork = 0, ncwork_std = 0, nbwork_aa = 0;
+  int aa_off[NSHAPE] = {}, aa_cnt[NSHAPE] = {};  // the in-place bricks of each shape in d_bwork_aa
   int64_t since_build = 0;          // steps since the last rebuild
   bool dirty = true;
   int64_t same_members = 0;  // launches since the last membership change
@@ -1166,13 +1170,14 @@ struct Batch {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_arrays() {
-    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork, (void*)d_iwork})
+    for (void* a : {(void*)d_desc, (void*)d_cwork, (void*)d_gwork, (void*)d_iwork, (void*)d_cwork_std,
+                    (void*)d_bwork_aa})
       if (a) cudaFree(a);
     groups.clear();
     d_desc = nullptr;
-    d_cwork = d_gwork = d_iwork = nullptr;
-    cap_desc = cap_cwork = cap_gwork = cap_iwork = 0;
-    ncwork = niwork = 0;
+    d_cwork = d_gwork = d_iwork = d_cwork_std = d_bwork_aa = nullptr;
+    cap_desc = cap_cwork = cap_gwork = cap_iwork = cap_cwork_std = cap_bwork_aa = 0;
+    ncwork = niwork = ncwork_std = nbwork_aa = 0;
   }
   void drop_graphs() {
     for (int p = 0; p < 2; ++p) {
@@ -1261,10 +1266,13 @@ struct Batch {
     since_build = 0;
     join_parity.assign(mem.size(), 0);
     std::vector<LatDesc> descs(mem.size());
-    std::vector<int2> cw, iw;
+    std::vector<int2> cw, cws, bwa, iw;
     int rc;
     for (size_t q = 0; q < mem.size(); ++q) {
       Engine* e = mem[q];
+      // an in-place member joins in the standard layout, so the batch's step
+      // parity is its phase
+      if ((rc = e->to_standard())) return rc;
       FE_CUDA(cudaStreamSynchronize(e->stream));
       join_parity[q] = e->parity;
       LatDesc d = e->hd;
@@ -1274,6 +1282,8 @@ struct Batch {
       }
       descs[q] = d;
       for (int c = 0; c < d.nchunks; ++c) cw.push_back(make_int2((int)q, c));
+      if (!e->aa)
+        for (int c = 0; c < d.nchunks; ++c) cws.push_back(make_int2((int)q, c));
       for (int b = 0; b < d.image_blocks; ++b) iw.push_back(make_int2((int)q, b));
       if ((rc = e->set_ctl_mode(1, e->ff_manual))) return rc;  // queued correction, forcing from t
     }
@@ -1285,28 +1295,43 @@ struct Batch {
     for (int sh = 0; sh < NSHAPE; ++sh)
       for (int mrt = 0; mrt < 3; ++mrt)
         for (int hbb = 0; hbb < 2; ++hbb)
-          for (int wd = 0; wd < 2; ++wd) {
-            const size_t off = gw.size();
-            for (size_t q = 0; q < mem.size(); ++q)
-              if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt && (mem[q]->hd.prm.hbb != 0) == (hbb != 0) &&
-                  (mem[q]->wide != 0) == (wd != 0))
-                for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
-            if (gw.size() == off) continue;
-            Group g;
-            g.wide = wd;
-            g.shape = sh;
-            g.mrt = mrt;
-            g.hbb = hbb;
-            g.nwork = (int)(gw.size() - off);
-            groups.push_back(g);
-            offs.push_back(off);
-          }
+          for (int wd = 0; wd < 2; ++wd)
+            for (int aa = 0; aa < 2; ++aa) {
+              const size_t off = gw.size();
+              for (size_t q = 0; q < mem.size(); ++q)
+                if (mem[q]->shape == sh && mem[q]->collide_variant() == mrt &&
+                    (mem[q]->hd.prm.hbb != 0) == (hbb != 0) && (mem[q]->wide != 0) == (wd != 0) &&
+                    (mem[q]->aa != 0) == (aa != 0))
+                  for (int b = 0; b < mem[q]->hd.nbricks; ++b) gw.push_back(make_int2((int)q, b));
+              if (gw.size() == off) continue;
+              Group g;
+              g.wide = wd;
+              g.aa = aa;
+              g.shape = sh;
+              g.mrt = mrt;
+              g.hbb = hbb;
+              g.nwork = (int)(gw.size() - off);
+              groups.push_back(g);
+              offs.push_back(off);
+            }
     if ((rc = upload_vec(&d_gwork, &cap_gwork, gw))) return rc;
     for (size_t k = 0; k < groups.size(); ++k) groups[k].d_work = d_gwork + offs[k];
     if ((rc = upload_vec(&d_desc, &cap_desc, descs))) return rc;
     if ((rc = upload_vec(&d_cwork, &cap_cwork, cw))) return rc;
+    if ((rc = upload_vec(&d_cwork_std, &cap_cwork_std, cws))) return rc;
+    // the in-place members' bricks, one run per brick shape
+    for (int sh = 0; sh < NSHAPE; ++sh) {
+      aa_off[sh] = (int)bwa.size();
+      for (size_t q = 0; q < mem.size(); ++q)
+        if (mem[q]->aa && mem[q]->shape == sh)
+          for (int b = 0; b < mem[q]->hd.nbricks; ++b) bwa.push_back(make_int2((int)q, b));
+      aa_cnt[sh] = (int)bwa.size() - aa_off[sh];
+    }
+    if ((rc = upload_vec(&d_bwork_aa, &cap_bwork_aa, bwa))) return rc;
     if ((rc = upload_vec(&d_iwork, &cap_iwork, iw))) return rc;
     ncwork = (int)cw.size();
+    ncwork_std = (int)cws.size();
+    nbwork_aa = (int)bwa.size();
     niwork = (int)iw.size();
     dirty = false;
     return FE_OK;
@@ -1323,11 +1348,21 @@ struct Batch {
   template <class S, class Sh>
   void launch_group_p4(const Group& g, int par, cudaStream_t st) {
     const size_t sm = CollideSmem<S, Sh>::BYTES;
-    launch_collide<S, Sh>(g.mrt, g.hbb != 0, g.wide != 0, g.nwork, sm, st, d_desc, g.d_work, par);
+    launch_collide<S, Sh>(g.mrt, g.hbb != 0, g.wide != 0, g.nwork, sm, st, d_desc, g.d_work, par,
+                          g.aa ? 1 + par : 0);
   }
   template <class S>
   void launch_step_t(int par, cudaStream_t st) {
-    k_moments<S><<<ncwork, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
+    if (par == 0 || !nbwork_aa) {
+      k_moments<S><<<ncwork, CTA, 0, st>>>(d_desc, d_cwork, par, 0);
+    } else {  // the in-place members' phase 1: their P1 gathers, per brick shape
+      if (ncwork_std) k_moments<S><<<ncwork_std, CTA, 0, st>>>(d_desc, d_cwork_std, par, 0);
+      for (int sh = 0; sh < NSHAPE; ++sh)
+        if (aa_cnt[sh])
+          with_shape<S>(sh, [&](auto t) {
+            launch_moments_aa<S, typename decltype(t)::type>(aa_cnt[sh], 0, st, d_desc, d_bwork_aa + aa_off[sh]);
+          });
+    }
     for (size_t q = 0; q < mem.size(); ++q) {
       const Engine* e = mem[q];
       if (!e->open_bnd) continue;
@@ -1357,9 +1392,13 @@ struct Batch {
       default: launch_step_t<StBF16G>(par, st); break;
     }
   }
-  // kernels of one step, the count launch_step_t makes
-  int64_t launches_per_step() const {
+  // kernels of one step of parity par, the count launch_step_t makes
+  int64_t launches_per_step(int par) const {
     int64_t k = 1 + 3 * (int64_t)groups.size() + (niwork ? 3 : 0);
+    if (par && nbwork_aa) {
+      k -= ncwork_std ? 0 : 1;
+      for (int sh = 0; sh < NSHAPE; ++sh) k += aa_cnt[sh] ? 1 : 0;
+    }
     for (const Engine* e : mem)
       if (e->open_bnd) {
         const int nio = e->hd.n_inlet + e->hd.n_outlet, nb = e->hd.n_buf;
@@ -1408,23 +1447,24 @@ struct Batch {
   // nsteps on the batch stream (after prepare): graph launches, or plain
   // launches while the membership is new
   int run_async(int nsteps) {
-    const int64_t kps = launches_per_step();
     int par = (int)(since_build & 1);
     int s = 0;
     if (!graph1[0]) {
-      for (; s < nsteps; ++s, par ^= 1) launch_step(par, stream);
-      launches += (int64_t)nsteps * kps;
+      for (; s < nsteps; ++s, par ^= 1) {
+        launch_step(par, stream);
+        launches += launches_per_step(par);
+      }
     }
     while (s < nsteps) {
       if (nsteps - s >= 2) {
         FE_CUDA(cudaGraphLaunch(graph2[par], stream));
         s += 2;
-        launches += 2 * kps;
+        launches += launches_per_step(0) + launches_per_step(1);
       } else {
         FE_CUDA(cudaGraphLaunch(graph1[par], stream));
+        launches += launches_per_step(par);
         par ^= 1;
         s += 1;
-        launches += kps;
       }
     }
     FE_CUDA(cudaGetLastError());
@@ -2146,7 +2186,6 @@ int fe_batch_destroy(fe_batch* b) {
 int fe_batch_add(fe_batch* b, fe_engine* e) {
   FE_BGUARD(b);
   FE_GUARD(e);
-  if (e->e.aa) return fe_fail(FE_ERR_ARG, "engines with the in-place population layout do not join batches");
   return b->b.add(&e->e);
 }
 

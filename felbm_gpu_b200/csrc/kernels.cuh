@@ -693,8 +693,9 @@ __device__ __forceinline__ uint32_t aa_src(const int32_t* __restrict__ s_idx, in
 
 // P1 from phase 1 of the in-place layout: the same moments and writes as
 // k_moments, on the persistent brick pipeline (the halo-1 tile of population
-// bases by bulk copy); mass partials per brick, summed by the CTA that
-// finishes last (one lattice per launch: in-place engines do not batch).
+// bases by bulk copy); mass partials per brick, summed by the CTA whose brick
+// is the lattice's last to finish (work items of several lattices may share
+// a launch).
 template <class S, class Sh>
 __global__ void __launch_bounds__(CTA, 4) k_moments_aa(const LatDesc* __restrict__ descs, const int2* __restrict__ work,
                                                      int nwork, int write_j) {
@@ -765,17 +766,14 @@ __global__ void __launch_bounds__(CTA, 4) k_moments_aa(const LatDesc* __restrict
           D.part1[(int64_t)brick * 2 + 0] = acc[0];
           D.part1[(int64_t)brick * 2 + 1] = acc[1];
         }
+        if (!last_block(&D.ctl->count1, (unsigned)D.nbricks, red)) return;
+        double tot[2];
+        sum_partials<2>(D.part1, D.nbricks, 2, tot, red);
+        if (threadIdx.x == 0) {
+          finish_mass(D.ctl, tot[0], tot[1]);
+          D.ctl->count1 = 0;
+        }
       });
-  if (blockIdx.x >= nwork) return;
-  const LatDesc& D = descs[work[blockIdx.x].x];
-  if (!D.prm.correct_mass) return;
-  if (!last_block(&D.ctl->count1, gridDim.x, red)) return;
-  double tot[2];
-  sum_partials<2>(D.part1, D.nbricks, 2, tot, red);
-  if (threadIdx.x == 0) {
-    finish_mass(D.ctl, tot[0], tot[1]);
-    D.ctl->count1 = 0;
-  }
 }
 
 // Phase 1 of the in-place layout to the standard layout, in place: for the

@@ -70,14 +70,16 @@ double pop_bytes(int storage) {
 }
 size_t fld_bytes(int storage) { return storage == FE_F64 ? 8 : 4; }
 
-// Device bytes of one resident solve: two ping-pong buffers of h and g, the
+// Device bytes of one resident solve: two buffers of h and g (one with the
+// in-place layout), the
 // three per-site momentum fields, the stencil fields on the node grid (c, p,
 // mu, lap(mu) and the (c', p') pairs: six values a node; the lattice rounded
 // up to bricks plus a two-node ring, bounded here by 20 more nodes per axis),
 // the FP64 transfer buffer (upload/download), and the site/brick tables
 // (generous per-site bound).
-double footprint(int64_t n, int nx, int ny, int nz, int storage) {
-  const double per = 4.0 * 19 * pop_bytes(storage) + 3.0 * fld_bytes(storage) + 2.0 * 19 * 8 + 64;
+double footprint(int64_t n, int nx, int ny, int nz, int storage, int pop_layout = FE_POP_TWO_BUFFERS) {
+  const double bufs = pop_layout == FE_POP_IN_PLACE ? 2.0 : 4.0;  // h and g, one or two buffers each
+  const double per = bufs * 19 * pop_bytes(storage) + 3.0 * fld_bytes(storage) + 2.0 * 19 * 8 + 64;
   const double cells = (double)(nx + 20) * (double)(ny + 20) * (double)(nz == 1 ? 1 : nz + 20);
   return (double)n * per + 6.0 * cells * (double)fld_bytes(storage) + (double)(64 << 20);
 }
@@ -186,6 +188,7 @@ struct fe_server {
     Req& q = L.q;
     fe_params p = q.r.params;
     p.storage = cfg.storage;
+    p.pop_layout = cfg.pop_layout;
     if (q.prep_status) {
       fail(L, fe_fail(q.prep_status, q.prep_message));
       return false;
@@ -239,7 +242,7 @@ struct fe_server {
 
   bool fits(const Req& q) {  // under mu
     if (cfg.max_active > 0 && holding >= cfg.max_active) return false;
-    const double need = footprint(q.sites, q.r.nx, q.r.ny, q.r.nz, cfg.storage);
+    const double need = footprint(q.sites, q.r.nx, q.r.ny, q.r.nz, cfg.storage, cfg.pop_layout);
     if (committed + need > budget) return false;
     size_t fr = 0, tot = 0;  // memory other users took since the server started
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
@@ -264,7 +267,7 @@ struct fe_server {
       ++active;
       peak_active = std::max(peak_active, active);
       L.t_admit = now();
-      L.bytes = footprint(L.q.sites, L.q.r.nx, L.q.r.ny, L.q.r.nz, cfg.storage);
+      L.bytes = footprint(L.q.sites, L.q.r.nx, L.q.r.ny, L.q.r.nz, cfg.storage, cfg.pop_layout);
       committed += L.bytes;
       ++holding;
       to_create.push_back(std::move(L));
@@ -450,6 +453,10 @@ int fe_server_create(const fe_server_config* cfg, fe_server** out) {
   if (!cfg || !out) return fe_fail(FE_ERR_ARG, "fe_server_create: bad arguments");
   if (cfg->chunk_steps < 1) return fe_fail(FE_ERR_ARG, "chunk_steps must be > 0");
   if (cfg->storage < FE_F64 || cfg->storage > FE_BF16G) return fe_fail(FE_ERR_ARG, "unknown storage");
+  if (cfg->pop_layout == FE_POP_IN_PLACE && cfg->storage != FE_F64 && cfg->storage != FE_F32)
+    return fe_fail(FE_ERR_ARG, "the in-place population layout takes FE_F64 or FE_F32 storage");
+  if (cfg->pop_layout != FE_POP_TWO_BUFFERS && cfg->pop_layout != FE_POP_IN_PLACE)
+    return fe_fail(FE_ERR_ARG, "unknown pop_layout");
   if (cfg->hbm_reserve_frac < 0.0 || cfg->hbm_reserve_frac >= 1.0)
     return fe_fail(FE_ERR_ARG, "hbm_reserve_frac must be in [0, 1)");
   *out = nullptr;

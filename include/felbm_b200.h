@@ -112,7 +112,7 @@ typedef struct fe_params {
    * its own opposite slots; the next step reads them from the upstream sites
    * and pushes its results to the downstream ones, which restores the
    * standard layout). Half the population memory; FE_F64 and FE_F32 storage,
-   * lattices whose population arrays stay below 2^32 entries, not in batches. */
+   * lattices whose population arrays stay below 2^32 entries. */
   int pop_layout;
 } fe_params;
 
@@ -371,8 +371,9 @@ int fe_mass_weight_noalloc(const double* d_h, int64_t n, double* d_out, void* st
  * behaves as fe_run on every member (queued mass correction after each step,
  * forcing factor from the step counter) and returns when the steps are done.
  * Engines stay usable on their own between batch runs; fe_engine_destroy of
- * a member removes it first. Engines with the in-place population layout
- * (FE_POP_IN_PLACE) are refused (FE_ERR_ARG). */
+ * a member removes it first. A member with the in-place population layout
+ * joins in the standard layout (a pending phase is swapped back in place),
+ * so the batch's step parity is its phase. */
 typedef struct fe_batch fe_batch;
 int fe_batch_create(int device, fe_batch** out);
 int fe_batch_destroy(fe_batch* b);
@@ -417,6 +418,9 @@ typedef struct fe_server_config {
   int chunk_steps;            /* steps between admission points (> 0)     */
   int storage;                /* FE_F64 .. FE_BF16S, all requests          */
   int64_t fill_sites;         /* sites per chunk (<= 0: every resident solve) */
+  int pop_layout;             /* FE_POP_TWO_BUFFERS or FE_POP_IN_PLACE (FE_F64 /
+                                 FE_F32 storage): the population layout of
+                                 every solve, and of its charged footprint  */
 } fe_server_config;
 typedef struct fe_request {
   int64_t id;

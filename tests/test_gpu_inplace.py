@@ -140,11 +140,75 @@ def test_in_place_refused_where_unsupported(require_gpu):
     case = make_case("spheres_bgk")
     with pytest.raises(FeError):
         MultiPhaseGPU(in_place(case.params, "f16g"), case.solid)
-    e = MultiPhaseGPU(in_place(case.params), case.solid)
+
+
+def test_batch_with_in_place_members_vs_oracle(require_gpu):
+    """A batch of in-place members of two brick shapes (3-D porous with mass
+    correction, the 2-D cylinder pack) beside a two-buffer member: odd step
+    counts, a state read between the runs (which swaps that member back to
+    the standard layout and makes the batch rebuild), each member against
+    the FP64 oracle after 63 steps."""
+    from parity import run_oracle
+    names = {"grf_mrt_mass": 1, "cyl2d_mrt": 1, "spheres_mrt_wet": 0}
+    engines = {}
     b = Batch()
     try:
-        with pytest.raises(FeError):
+        for n, layout in names.items():
+            case = make_case(n)
+            p = with_storage(case.params, "f64")
+            p.pop_layout = layout
+            e = MultiPhaseGPU(p, case.solid)
+            e.upload_state(case.h0, case.g0)
+            if case.correct_mass:
+                e.record_target_mass()
+            engines[n] = e
             b.add(e)
+        b.run(37)
+        engines["grf_mrt_mass"].download_state()
+        b.run(26)
+        for n, e in engines.items():
+            h, g = e.download_state()
+            f = e.download()
+            ho, go, fo, _ = run_oracle(make_case(n), 63)
+            assert_fp64(h, g, f, ho, go, fo, n)
     finally:
         b.free()
-        e.free()
+        for e in engines.values():
+            e.free()
+
+
+def test_served_in_place_equals_alone(require_gpu):
+    """The request loop with every solve in place: each result bit-for-bit
+    the same solve run alone in place."""
+    import time
+    from felbm_gpu_b200 import geometry
+    from felbm_gpu_b200.serving import Server
+    from test_gpu_serving import collect, solve_spec
+    specs = [solve_spec(k) for k in range(6)]
+    srv = Server(storage="f32", max_active=3, chunk_steps=16, pop_layout="in_place")
+    try:
+        for k, (p, solid, init, W, steps) in enumerate(specs):
+            srv.submit(k, p, solid, steps, init=init, init_width=W)
+            time.sleep(0.01)
+        res = collect(srv, len(specs))
+    finally:
+        srv.close()
+    assert len(res) == len(specs)
+    for r in res:
+        assert r.status == 0, r.message
+        p, solid, init, W, steps = specs[r.id]
+        kind, a = init
+        c = geometry.order_parameter(solid, "slab", W, origin=a[:3], axis=int(a[3]), thickness=a[4])
+        h0, g0 = geometry.equilibrium(c, 1.0, p.rho0, p.rho1)
+        e = MultiPhaseGPU(in_place(p, "f32"), solid)
+        try:
+            e.upload_state(h0, g0)
+            e.record_target_mass()
+            e.run(steps)
+            f = e.download()
+            m = e.current_mass()
+        finally:
+            e.free()
+        for k in ("c", "rho", "ux", "uy", "uz", "p"):
+            assert np.array_equal(r.fields[k], f[k]), (r.id, k, np.max(np.abs(r.fields[k] - f[k])))
+        assert r.mass_final == m
