@@ -95,6 +95,9 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
   // population offsets: 32-bit while the lattice's arrays stay below 2^32
   // entries (the host picks WIDE otherwise)
   using IX = typename std::conditional<WIDE, int64_t, uint32_t>::type;
+  // keep the 32-bit push targets of the h stores for the g stores of the
+  // moment forms (the in-place layout's own-slot targets are one add)
+  constexpr bool KEEP_DST = MRT != 0 && !WIDE && AAP != 1;
   __shared__ Head<Sh> s;
   __shared__ uint64_t s_bar;
   extern __shared__ __align__(128) unsigned char dsm[];
@@ -358,8 +361,12 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const V T1 = fma2(V(q.drho_cs2), DC, V(-q.u_drm));
       const V T2 = fma2(V(q.mu), DC, V(fproj - q.u_fg_f, -fproj - q.u_fg_f));
       const V Zk = fma2(T2, G, fma2(T1, WUT, gp[pr]));
-      st_pop<HV<S>>(hout, dst(k), k, H.x(), shh);
-      st_pop<HV<S>>(hout, dst(k + 1), k + 1, H.y(), shh);
+      const IX tk = dst(k), tk1 = dst(k + 1);
+      st_pop<HV<S>>(hout, tk, k, H.x(), shh);
+      st_pop<HV<S>>(hout, tk1, k + 1, H.y(), shh);
+      // the pair's push targets wait in its (now read) stash slot for the g
+      // stores after the moment sums
+      if constexpr (KEEP_DST) *reinterpret_cast<uint2*>(&s_sv[(2 * pr) * P4T]) = make_uint2(tk, tk1);
       if (MRT == 2) {
         const R sx = X.x() + X.y(), dx = X.x() - X.y();
         sumx += sx;
@@ -396,8 +403,14 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       for (int k = 1; k < Q; k += 2) {
         const R ej = qx * R(lat_cx(k)) + qy * R(lat_cy(k)) + qz * R(lat_cz(k));
         const V out = zp[k >> 1] - V(mx + ej, mx - ej);
-        st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
-        st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
+        if constexpr (KEEP_DST) {
+          const uint2 t = *reinterpret_cast<const uint2*>(&s_sv[(2 * (k >> 1)) * P4T]);
+          st_pop<GV<S>>(gout, (IX)t.x, k, out.x(), shg);
+          st_pop<GV<S>>(gout, (IX)t.y, k + 1, out.y(), shg);
+        } else {
+          st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
+          st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
+        }
       }
     }
     if (MRT == 1) {
@@ -430,8 +443,14 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
           else if (mjk != 0) acc += R(mjk) * mom[j];
         }
         const V out = zp[k >> 1] + V(E + O, E - O);
-        st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
-        st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
+        if constexpr (KEEP_DST) {
+          const uint2 t = *reinterpret_cast<const uint2*>(&s_sv[(2 * (k >> 1)) * P4T]);
+          st_pop<GV<S>>(gout, (IX)t.x, k, out.x(), shg);
+          st_pop<GV<S>>(gout, (IX)t.y, k + 1, out.y(), shg);
+        } else {
+          st_pop<GV<S>>(gout, dst(k), k, out.x(), shg);
+          st_pop<GV<S>>(gout, dst(k + 1), k + 1, out.y(), shg);
+        }
       }
     }
   }
