@@ -30,11 +30,18 @@ def test_server_arguments():
     assert lib.fe_server_create(C.byref(bad), C.byref(h)) == _capi.FE_ERR_ARG
     bad = _capi.FeServerConfig(0, 0, 0.1, 10, 9, 0)
     assert lib.fe_server_create(C.byref(bad), C.byref(h)) == _capi.FE_ERR_ARG
+    # the in-place population layout: FP64 / FP32 storage only; known layouts only
+    bad = _capi.FeServerConfig(0, 0, 0.1, 10, _capi.STORAGE["f16g"], 0, 1)
+    assert lib.fe_server_create(C.byref(bad), C.byref(h)) == _capi.FE_ERR_ARG
+    bad = _capi.FeServerConfig(0, 0, 0.1, 10, _capi.FE_F32, 0, 2)
+    assert lib.fe_server_create(C.byref(bad), C.byref(h)) == _capi.FE_ERR_ARG
     assert lib.fe_server_submit(None, None) == _capi.FE_ERR_ARG
     assert lib.fe_server_destroy(None) == 0
     assert lib.fe_server_free_result(None) == 0
     if not torch.cuda.is_available():
         ok = _capi.FeServerConfig(0, 0, 0.1, 10, _capi.FE_F32, 0)
+        assert lib.fe_server_create(C.byref(ok), C.byref(h)) == _capi.FE_ERR_NO_DEVICE
+        ok = _capi.FeServerConfig(0, 0, 0.1, 10, _capi.FE_F32, 0, 1)
         assert lib.fe_server_create(C.byref(ok), C.byref(h)) == _capi.FE_ERR_NO_DEVICE
 
 
