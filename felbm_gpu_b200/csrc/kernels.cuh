@@ -126,11 +126,6 @@ template <class T> __device__ __forceinline__ T from_f(float v);
 template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
-// AoSoA population index of (site i, direction k)
-__device__ __forceinline__ int64_t pidx(int64_t i, int k) {
-  return (i >> 5) * (int64_t)(Q * AOSOA) + k * AOSOA + (i & (AOSOA - 1));
-}
-
 struct Shift {
   float ref, inv_scale, scale;
 };
@@ -363,14 +358,6 @@ __device__ __forceinline__ int64_t grid_entry(const LatDesc& D, int bx, int by, 
   const int y = by * Sh::BY + ((slot >> Sh::LBX) & (Sh::BY - 1)) + 2;
   const int z = bz * Sh::BZ + (slot >> (Sh::LBX + Sh::LBY)) + 2 * D.hz;
   return x + D.gsy * y + D.gsz * z;
-}
-
-// Node coordinates of slot `slot` of the brick at (bx, by, bz).
-template <class Sh>
-__device__ __forceinline__ void slot_node(int bx, int by, int bz, int slot, int& x, int& y, int& z) {
-  x = bx * Sh::BX + (slot & (Sh::BX - 1));
-  y = by * Sh::BY + ((slot >> Sh::LBX) & (Sh::BY - 1));
-  z = bz * Sh::BZ + (slot >> (Sh::LBX + Sh::LBY));
 }
 
 // The tensor map `id` of the lattice (a CUtensorMap in device memory).
@@ -853,48 +840,19 @@ __device__ __forceinline__ R cd_val(R f0, R fm, R fp, bool hbb) {
   if (hbb) return R(0.5) * ((f1 ? fp : f0) - (b1 ? fm : f0));
   return (b1 && f1) ? R(0.5) * (fp - fm) : R(0);
 }
-// biased value of direction k (bd_dir_val): fp2 = f(x + 2e), fm2 = f(x - 2e)
-template <class R>
-__device__ __forceinline__ R bd_val(R f0, R fm, R fp, R fm2, R fp2, bool hbb) {
-  const bool b1 = is_site(fm), f1 = is_site(fp), f2 = is_site(fp2);
-  if (f1) {
-    if (f2) return R(-1.5) * f0 + R(2.0) * fp + R(-0.5) * fp2;
-    return hbb ? R(-1.5) * f0 + R(1.5) * fp : R(-2.0) * f0 + R(2.0) * fp;
-  }
-  if (hbb) return b1 ? R(0.5) * f0 + R(-0.5) * fm : R(0);
-  return (b1 && is_site(fm2)) ? R(-1.5) * f0 + R(2.0) * fm + R(-0.5) * fm2 : R(0);
-}
-// The same two stencils for one opposite pair (e, -e) of both tiles, branch
-// free, the near-wall case fixed at compile time by HBB: c and p share their
-// solid positions, so the four neighbour flags are taken once. Outputs the
-// central values of c and p for +e, and the biased values of c and p for +e
-// (a) and -e (b). Same arithmetic as cd_val / bd_val in every case.
-template <bool HBB, class R>
-__device__ __forceinline__ R bd_sel(R f0, R fm, R fp, R fm2, R fp2, bool sm, bool sp, bool sm2, bool sp2) {
-  const R two = R(-1.5) * f0 + R(2.0) * fp + R(-0.5) * fp2;
-  const R one = HBB ? R(-1.5) * f0 + R(1.5) * fp : R(-2.0) * f0 + R(2.0) * fp;
-  const R back = HBB ? (sm ? R(0.5) * f0 + R(-0.5) * fm : R(0))
-                     : ((sm && sm2) ? R(-1.5) * f0 + R(2.0) * fm + R(-0.5) * fm2 : R(0));
-  return sp ? (sp2 ? two : one) : back;
-}
+// The central stencil value of direction k (cd_dir_val), branch free with
+// the near-wall case fixed at compile time by HBB (one-sided next to a solid
+// neighbour under halfway bounce-back, else zero).
 template <bool HBB, class R>
 __device__ __forceinline__ R cd_sel(R f0, R fm, R fp, bool sm, bool sp) {
   if (HBB) return R(0.5) * ((sp ? fp : f0) - (sm ? fm : f0));
   return (sm && sp) ? R(0.5) * (fp - fm) : R(0);
 }
-template <bool HBB, class R>
-__device__ __forceinline__ void pair_derivs(R c0, R cm, R cp, R cm2, R cp2, R p0, R pm, R pp, R pm2, R pp2, R& cdc,
-                                            R& cdp, R& bca, R& bcb, R& bpa, R& bpb) {
-  const bool sm = is_site(cm), sp = is_site(cp), sm2 = is_site(cm2), sp2 = is_site(cp2);
-  cdc = cd_sel<HBB>(c0, cm, cp, sm, sp);
-  cdp = cd_sel<HBB>(p0, pm, pp, sm, sp);
-  bca = bd_sel<HBB>(c0, cm, cp, cm2, cp2, sm, sp, sm2, sp2);
-  bcb = bd_sel<HBB>(c0, cp, cm, cp2, cm2, sp, sm, sp2, sm2);
-  bpa = bd_sel<HBB>(p0, pm, pp, pm2, pp2, sm, sp, sm2, sp2);
-  bpb = bd_sel<HBB>(p0, pp, pm, pp2, pm2, sp, sm, sp2, sm2);
-}
-// cd_sel / bd_sel on two-lane (c, p) pairs: the same cases, both fields per
-// instruction.
+// The central and the biased (bd_dir_val: fp2 = f(x + 2e), fm2 = f(x - 2e))
+// stencil values on two-lane (c, p) pairs (c and p share their solid
+// positions): both fields per instruction. Biased: the 3-point difference
+// when x + e and x + 2e are fluid, 2-point when only x + e is, one-sided
+// backwards (or zero) when x + e is solid.
 template <bool HBB, class R>
 __device__ __forceinline__ V2<R> cd_sel2(V2<R> f0, V2<R> fm, V2<R> fp, bool sm, bool sp) {
   using V = V2<R>;
@@ -911,8 +869,8 @@ __device__ __forceinline__ V2<R> bd_sel2(V2<R> f0, V2<R> fm, V2<R> fp, V2<R> fm2
                      : sel(sm && sm2, fma2(V(R(-0.5)), fm2, fma2(V(R(2)), fm, V(R(-1.5)) * f0)), V(R(0)));
   return sel(sp, sel(sp2, two, one), back);
 }
-// pair_derivs on (c, p) pairs: central value for +e, biased values for +e (ba)
-// and -e (bb); the solid positions are read from the c lane.
+// One opposite pair of (c, p): central value for +e, biased values for +e
+// (ba) and -e (bb); the solid positions are read from the c lane.
 template <bool HBB, class R>
 __device__ __forceinline__ void pair_derivs2(V2<R> f0, V2<R> fm, V2<R> fp, V2<R> fm2, V2<R> fp2, V2<R>& cd,
                                              V2<R>& ba, V2<R>& bb) {

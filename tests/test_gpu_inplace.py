@@ -212,3 +212,49 @@ def test_served_in_place_equals_alone(require_gpu):
         for k in ("c", "rho", "ux", "uy", "uz", "p"):
             assert np.array_equal(r.fields[k], f[k]), (r.id, k, np.max(np.abs(r.fields[k] - f[k])))
         assert r.mass_final == m
+
+
+def test_in_place_tracers_and_checkpoint_equal_two_buffers(require_gpu, tmp_path):
+    """Tracers on an in-place engine (the fused snapshot of the next step and
+    the explicit refresh pass from either phase) and a checkpoint written
+    after an odd step count: trajectories, line elements and the restarted
+    run bit-equal to the two-buffer engine's (FP32, no mass correction)."""
+    from felbm_gpu_b200 import files
+    from felbm_gpu_b200.tracers import Tracers, seed
+    case = make_case("spheres_mrt_wet")
+    pos0, _ = seed(case.solid, 150, rng_seed=8)
+    kw = dict(substeps=2, order=2, rng_seed=5, stretching=True)
+    out = {}
+    for layout in (0, 1):
+        p = with_storage(case.params, "f32")
+        p.pop_layout = layout
+        e = MultiPhaseGPU(p, case.solid)
+        try:
+            e.upload_state(case.h0, case.g0)
+            fused = Tracers(e, pos0, 1e-3, **kw)
+            plain = Tracers(e, pos0, 1e-3, **kw)
+            for s in range(9):
+                e.run(1 if s % 4 else 3)
+                fused.step()
+                plain.step()
+            pf, vf = fused.download()
+            pp, vp = plain.download()
+            fused.free()
+            plain.free()
+            ck = str(tmp_path / f"ck{layout}.h5")
+            files.write_checkpoint(e, ck, 15)
+            e.run(5)
+            h, g = e.download_state()
+        finally:
+            e.free()
+        r = MultiPhaseGPU(p, case.solid)  # restart from the checkpoint
+        try:
+            assert files.read_checkpoint(r, ck) == 15
+            r.run(5)
+            hr, gr = r.download_state()
+        finally:
+            r.free()
+        assert np.array_equal(hr, h) and np.array_equal(gr, g)
+        out[layout] = (pf, vf, pp, vp, h, g)
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b, equal_nan=True)
