@@ -80,9 +80,14 @@ struct SiteScal {
 // AAP: 0 two population buffers; 1, 2 the in-place layout from phase 0
 // (reads the own slots, writes f*_k into the own slot opp(k)) and from phase
 // 1 (reads f_k where the last step left it, pushes like the two-buffer pass).
-template <class S, class Sh, int MRT, bool HBB, bool WIDE, int AAP = 0>
+// MRT_: 0 BGK, 1 general MRT, 2 two-rate MRT, 3 two-rate MRT of a lattice
+// without density contrast (rho0 = rho1: the drho terms are zero and dropped;
+// the same results bit for bit).
+template <class S, class Sh, int MRT_, bool HBB, bool WIDE, int AAP = 0>
 __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     k_collide(const LatDesc* __restrict__ descs, const int2* __restrict__ work, int parity) {
+  constexpr int MRT = MRT_ == 3 ? 2 : MRT_;
+  constexpr bool NODRHO = MRT_ == 3;
   static_assert(AAP == 0 || !WIDE, "the in-place layout takes 32-bit population offsets");
   using R = typename S::real;
   using V = V2<R>;
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     const R epx = ec[0].y(), epy = ec[1].y(), epz = ec[2].y();
     const R bcx = eb[0].x(), bcy = eb[1].x(), bcz = eb[2].x();
     const R bpx = eb[0].y(), bpy = eb[1].y(), bpz = eb[2].y();
-    const R rho = rho1 + drho * c;
+    const R rho = NODRHO ? rho1 : rho1 + drho * c;
     const R irho = R(1) / rho;
     const R cm_ = (flag & BC_SITE) ? (R) static_cast<const F*>(D.c_raw_bc)[i] : c;
     // relaxation rate (reference k_moments :130-132)
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     // site scalars (device_engine.cuh:563-583)
     const R rho_cs2 = rho * cs2;
     const R c_over = c * irho * R(1.0 / CS2);
-    q.drho_cs2 = drho * cs2;
+    q.drho_cs2 = NODRHO ? R(0) : drho * cs2;
     q.hdr = R(0.5) * q.drho_cs2;
     q.mob = (R)Pm.mobility;
     const R bfx = rho * gxa + fxa, bfy = rho * gya + fya, bfz = rho * gza + fza;
@@ -279,15 +284,15 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     const R ffhx = fdcx - c_over * (fdpx - ffgx), ffhy = fdcy - c_over * (fdpy - ffgy),
             ffhz = fdcz - c_over * (fdpz - ffgz);
     const R u_force_g = ux * efgx + uy * efgy + uz * efgz;
-    const R u_drho = q.drho_cs2 * (ux * ecx + uy * ecy + uz * ecz);
+    const R u_drho = NODRHO ? R(0) : q.drho_cs2 * (ux * ecx + uy * ecy + uz * ecz);
     const R S_h = R(0.5) * (ux * efhx + uy * efhy + uz * efhz) - (ux * ffhx + uy * ffhy + uz * ffhz);
     q.u_fg_f = ux * ffgx + uy * ffgy + uz * ffgz;
-    q.u_drm = q.drho_cs2 * (ux * fdcx + uy * fdcy + uz * fdcz);
+    q.u_drm = NODRHO ? R(0) : q.drho_cs2 * (ux * fdcx + uy * fdcy + uz * fdcz);
     q.C0 = c + S_h;
     q.hk1 = R(0.5) * (R(1) + c_over * q.mu);
     q.hco = R(0.5) * c_over;
     q.A1 = p + R(0.5) * u_force_g;
-    q.A2 = rho_cs2 + R(0.5) * (u_drho + u_force_g);
+    q.A2 = NODRHO ? rho_cs2 + R(0.5) * u_force_g : rho_cs2 + R(0.5) * (u_drho + u_force_g);
     st[0] += (double)ux; st[1] += (double)uy; st[2] += (double)uz; st[3] += (double)u2; st[4] += (double)c;
     st[5] = fmax(st[5], (double)u2);
     bad |= !(u2 < R(1e30));
@@ -311,7 +316,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       const R wut = -w * q.gu2, G = w + wut;
       const R h0 = G * (q.C0 + q.mob * lmu);
       const R x0 = (w * q.A1 + q.A2 * wut) - g0;
-      z0 = g0 - q.u_drm * wut - q.u_fg_f * G;
+      z0 = NODRHO ? g0 - q.u_fg_f * G : g0 - q.u_drm * wut - q.u_fg_f * G;
       st_pop<HV<S>>(hout, a0, 0, h0, shh);
       if (MRT == 1) {
 #pragma unroll
@@ -350,7 +355,7 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       // m1 = mu cd_c + F.e in the MRT equilibrium, -(mu cd_c + F.e) in the BGK
       // one (device_engine.cuh:517 vs :598)
       const R m1 = MRT ? q.mu * cdc + fproj : -(q.mu * cdc + fproj);
-      const R o1 = (R(0.5) * w) * m1, o2 = R(0.5) * m1 - q.hdr * cdc;
+      const R o1 = (R(0.5) * w) * m1, o2 = NODRHO ? R(0.5) * m1 : R(0.5) * m1 - q.hdr * cdc;
       const R wa1 = w * q.A1;
       const V EG = fma2(V(q.A2), WUT, fma2(V(o2, -o2), WUT, V(wa1 + o1, wa1 - o1)));
       const V X = EG - gp[pr];
@@ -358,9 +363,14 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
       // dc = (+-cd_c + bd_c) / 2 (device_engine.cuh:609)
       const R hc = R(0.5) * cdc;
       const V DC = fma2(V(R(0.5)), BC, V(hc, -hc));
-      const V T1 = fma2(V(q.drho_cs2), DC, V(-q.u_drm));
       const V T2 = fma2(V(q.mu), DC, V(fproj - q.u_fg_f, -fproj - q.u_fg_f));
-      const V Zk = fma2(T2, G, fma2(T1, WUT, gp[pr]));
+      V Zk;
+      if constexpr (NODRHO) {
+        Zk = fma2(T2, G, gp[pr]);
+      } else {
+        const V T1 = fma2(V(q.drho_cs2), DC, V(-q.u_drm));
+        Zk = fma2(T2, G, fma2(T1, WUT, gp[pr]));
+      }
       const IX tk = dst(k), tk1 = dst(k + 1);
       st_pop<HV<S>>(hout, tk, k, H.x(), shh);
       st_pop<HV<S>>(hout, tk1, k + 1, H.y(), shh);

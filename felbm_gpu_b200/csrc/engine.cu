@@ -262,9 +262,10 @@ static void launch_collide_aa(int mrt, bool hbb, int nwork, size_t smem, cudaStr
 template <class S, class Sh>
 static void launch_collide(int mrt, bool hbb, bool wide, int nwork, size_t smem, cudaStream_t st,
                            const LatDesc* desc, const int2* work, int par, int aap = 0) {
-  if (aap == 1) return launch_collide_aa<S, Sh, 1>(mrt, hbb, nwork, smem, st, desc, work, par);
-  if (aap == 2) return launch_collide_aa<S, Sh, 2>(mrt, hbb, nwork, smem, st, desc, work, par);
-  if (mrt == 2 && hbb && !wide) k_collide<S, Sh, 2, true, false><<<nwork, P4T, smem, st>>>(desc, work, par);
+  if (aap == 1) return launch_collide_aa<S, Sh, 1>(mrt == 3 ? 2 : mrt, hbb, nwork, smem, st, desc, work, par);
+  if (aap == 2) return launch_collide_aa<S, Sh, 2>(mrt == 3 ? 2 : mrt, hbb, nwork, smem, st, desc, work, par);
+  if (mrt == 3 && hbb && !wide) k_collide<S, Sh, 3, true, false><<<nwork, P4T, smem, st>>>(desc, work, par);
+  else if (mrt >= 2 && hbb && !wide) k_collide<S, Sh, 2, true, false><<<nwork, P4T, smem, st>>>(desc, work, par);
   else if (mrt && hbb) launch_collide_w<S, Sh, 1, true>(wide, nwork, smem, st, desc, work, par);
   else if (mrt) launch_collide_w<S, Sh, 1, false>(wide, nwork, smem, st, desc, work, par);
   else if (hbb) launch_collide_w<S, Sh, 0, true>(wide, nwork, smem, st, desc, work, par);
@@ -338,6 +339,7 @@ static cudaError_t collide_smem_attr(int bytes) {
   set((const void*)k_collide<S, Sh, 1, true, false>);
   set((const void*)k_collide<S, Sh, 1, true, true>);
   set((const void*)k_collide<S, Sh, 2, true, false>);
+  set((const void*)k_collide<S, Sh, 3, true, false>);
   if constexpr (InPlaceStorage<S>::value) {
     set((const void*)k_collide<S, Sh, 0, false, false, 1>);
     set((const void*)k_collide<S, Sh, 0, true, false, 1>);
@@ -468,7 +470,8 @@ struct Engine {
   // two-rate form (halfway bounce-back, 32-bit offsets).
   int collide_variant() const {
     if (!hd.prm.use_mrt) return 0;
-    return (hd.prm.two_rate && hd.prm.hbb && !wide) ? 2 : 1;
+    if (!(hd.prm.two_rate && hd.prm.hbb && !wide)) return 1;
+    return hd.prm.drho == 0.0 ? 3 : 2;  // 3: no density contrast
   }
 
   void fill_prm() {
@@ -1293,7 +1296,7 @@ struct Batch {
     // alone (the offset width included: it decides what a member's push-target
     // tiles hold)
     for (int sh = 0; sh < NSHAPE; ++sh)
-      for (int mrt = 0; mrt < 3; ++mrt)
+      for (int mrt = 0; mrt < 4; ++mrt)
         for (int hbb = 0; hbb < 2; ++hbb)
           for (int wd = 0; wd < 2; ++wd)
             for (int aa = 0; aa < 2; ++aa) {
