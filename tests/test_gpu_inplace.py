@@ -258,3 +258,33 @@ def test_in_place_tracers_and_checkpoint_equal_two_buffers(require_gpu, tmp_path
         out[layout] = (pf, vf, pp, vp, h, g)
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("brick", ["8x8x8", "8x8x4"])
+def test_in_place_other_bricks_vs_oracle(require_gpu, brick):
+    """The in-place phases on the other brick shapes (their halo-1 tiles of
+    population bases differ), 37 steps (the state read back from phase 1)."""
+    from felbm_gpu_b200 import _capi
+    case = make_case("grf_mrt_mass")
+    p = in_place(case.params)
+    p.brick = _capi.BRICK[brick]
+    e = MultiPhaseGPU(p, case.solid)
+    try:
+        e.upload_state(case.h0, case.g0)
+        e.record_target_mass()
+        e.run(37)
+        h, g = e.download_state()
+        f = e.download()
+    finally:
+        e.free()
+    ho, go, fo, _ = run_oracle(case, 37)
+    assert_fp64(h, g, f, ho, go, fo, brick)
+
+
+def test_in_place_refused_with_wide_offsets(require_gpu, monkeypatch):
+    """Lattices that need 64-bit population offsets keep two buffers (the
+    in-place passes address populations with 32-bit bases)."""
+    monkeypatch.setenv("FELBM_WIDE_OFFSETS", "1")
+    case = make_case("spheres_bgk")
+    with pytest.raises(FeError):
+        MultiPhaseGPU(in_place(case.params), case.solid)
