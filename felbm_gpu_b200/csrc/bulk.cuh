@@ -23,6 +23,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
+// A hint: bytes (a multiple of 16) of global memory at src (16-byte
+// aligned) brought into L2 by the copy engine; nothing waits for it.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // bytes (a multiple of 16) from global src to shared dst, both 16-byte
 // aligned; completion is counted on bar.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {

@@ -131,6 +131,16 @@ __global__ void __launch_bounds__(P4T, CollideMinBlocks<S>::value)
     bulk_g2s(s_idx, D.tile1 + (int64_t)brick * T1::N, (uint32_t)(T1::N * 4), &s_bar);
   }
   if (threadIdx.x == P4T - 1) load_step_scalars(D, s);
+  // the brick's own g blocks (its sites are one contiguous AoSoA range) into
+  // L2 while the tiles land, so the per-site g loads below hit L2
+  if constexpr (AAP != 2) {
+    if (threadIdx.x >= 32 && threadIdx.x < 64) {
+      const int first = __ldg(&D.rec[brick].first), cnt = __ldg(&D.rec[brick].cnt);
+      const PG* gsrc = static_cast<const PG*>(D.pop[parity][1]);
+      for (int64_t b = (first >> 5) + (threadIdx.x - 32); b <= (int64_t)((first + cnt - 1) >> 5); b += 32)
+        bulk_prefetch_l2(gsrc + b * (Q * AOSOA), (uint32_t)(Q * AOSOA * sizeof(PG)));
+    }
+  }
   if (!head_wait(D, &s_bar)) return;
 
   const DevPrm& Pm = D.prm;
