@@ -41,6 +41,7 @@ SIGNATURES = {
     "fe_set_params": (C.c_int, [_vp, C.POINTER(FeParams)]),
     "fe_engine_stream": (C.c_void_p, [_vp]),
     "fe_upload_state": (C.c_int, [_vp, _dp, _dp, C.c_int64]),
+    "fe_upload_equilibrium": (C.c_int, [_vp, _dp, _dp, C.c_double, C.c_int64]),
     "fe_download_state": (C.c_int, [_vp, _dp, _dp, C.c_int64]),
     "fe_set_open_bnd": (C.c_int, [_vp, C.POINTER(FeOpenBnd)]),
     "fe_step": (C.c_int, [_vp, C.c_int]),

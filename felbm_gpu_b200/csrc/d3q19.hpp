@@ -56,4 +56,19 @@ constexpr double ALPHA = 3.0;
 constexpr double GAMMA = 1.5;
 constexpr double BETA = 4.5;
 
+// Plain equilibrium of direction k (reference k_open_bnd,
+// device_engine.cuh:790-797): h_k = w c (1 + u_term), g_k = w (p + rho cs^2
+// u_term), u_term = e.u (ALPHA + BETA e.u) - GAMMA u.u. The host's initial
+// state (fe_init_equilibrium) and the device's (fe_upload_equilibrium, at
+// rest) both evaluate it here.
+FE_HD void equilibrium_k(int k, double c, double p, double rho, double vx, double vy, double vz, double& h,
+                         double& g) {
+  const double w = weight<double>(k);
+  const double u_sq = vx * vx + vy * vy + vz * vz;
+  const double uk = vx * lat_cx(k) + vy * lat_cy(k) + vz * lat_cz(k);
+  const double u_term = uk * (ALPHA + BETA * uk) - GAMMA * u_sq;
+  h = c * w * (1.0 + u_term);
+  g = w * (p + rho * CS2 * u_term);
+}
+
 }  // namespace fe

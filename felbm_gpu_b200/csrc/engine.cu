@@ -1055,6 +1055,30 @@ struct Engine {
     return FE_OK;
   }
 
+  // The equilibrium state at rest of per-site c and p (reference site order;
+  // p null: p_uniform), built on the device from n (or 2n) uploaded values
+  // instead of the 38n of a host-built state; the same state as upload() of
+  // fe_init_equilibrium's arrays.
+  int upload_equilibrium(const double* c, const double* p, double p_uniform) {
+    const int64_t n = hd.n;
+    int rc;
+    if ((rc = tracer_hook(-1, state_id, false))) return rc;
+    ++state_id;
+    if ((rc = ensure_tmp(2 * n))) return rc;
+    if (aa) parity = 0;
+    FE_CUDA(copy_to_device(d_tmp, c, n * sizeof(double)));
+    if (p) FE_CUDA(copy_to_device(d_tmp + n, p, n * sizeof(double)));
+    FE_DISPATCH(*this, (k_upload_equilibrium<S><<<hd.nchunks, CTA, 0, stream>>>(d_desc, d_cwork, parity, d_tmp,
+                                                                                   p ? d_tmp + n : nullptr,
+                                                                                   p_uniform)));
+    ++launches;
+    FE_CUDA(cudaGetLastError());
+    int32_t zero = 0;
+    if ((rc = write_ctl_field(offsetof(Ctl, pending), &zero, 4))) return rc;
+    FE_CUDA(cudaStreamSynchronize(stream));
+    return FE_OK;
+  }
+
   // download()/download_raw(): P1 (+BC) and P2 in output mode, no step.
   // OUT 1: reference site order; OUT 2: node-indexed grids.
   template <class S, class Sh, int OUT>
@@ -1874,6 +1898,12 @@ int fe_upload_state(fe_engine* e, const double* h, const double* g, int64_t vn) 
   FE_GUARD(e);
   if (!h || !g || vn != (int64_t)fe::Q * e->e.hd.n) return fe_fail(FE_ERR_ARG, "fe_upload_state: size mismatch");
   return e->e.upload(h, g);
+}
+
+int fe_upload_equilibrium(fe_engine* e, const double* c, const double* p, double p_uniform, int64_t n) {
+  FE_GUARD(e);
+  if (!c || n != e->e.hd.n) return fe_fail(FE_ERR_ARG, "fe_upload_equilibrium: size mismatch");
+  return e->e.upload_equilibrium(c, p, p_uniform);
 }
 
 int fe_download_state(fe_engine* e, double* h, double* g, int64_t vn) {

@@ -424,14 +424,7 @@ int fe_init_equilibrium(int64_t n, const double* c, const double* p, const doubl
   for (int64_t i = 0; i < n; ++i) {
     const double vx = ux ? ux[i] : 0.0, vy = uy ? uy[i] : 0.0, vz = uz ? uz[i] : 0.0;
     const double rho = rho1 + (rho0 - rho1) * c[i];
-    const double u_sq = vx * vx + vy * vy + vz * vz;
-    for (int k = 0; k < Q; ++k) {
-      const double w = weight<double>(k);
-      const double uk = vx * lat_cx(k) + vy * lat_cy(k) + vz * lat_cz(k);
-      const double u_term = uk * (ALPHA + BETA * uk) - GAMMA * u_sq;
-      h[k * n + i] = c[i] * w * (1.0 + u_term);
-      g[k * n + i] = w * (p[i] + rho * CS2 * u_term);
-    }
+    for (int k = 0; k < Q; ++k) equilibrium_k(k, c[i], p[i], rho, vx, vy, vz, h[k * n + i], g[k * n + i]);
   }
   return FE_OK;
 }

@@ -1371,6 +1371,41 @@ __global__ void __launch_bounds__(CTA) k_upload_state(const LatDesc* __restrict_
   }
 }
 
+// The equilibrium state at rest of per-site c and p (reference site order;
+// p_in null: p_uniform everywhere), built on the device: the values
+// fe_init_equilibrium gives at zero velocity, stored as k_upload_state
+// stores them, so the state equals that of fe_upload_state on the host's
+// arrays.
+template <class S>
+__global__ void __launch_bounds__(CTA) k_upload_equilibrium(const LatDesc* __restrict__ descs,
+                                                             const int2* __restrict__ work, int parity,
+                                                             const double* __restrict__ c_in,
+                                                             const double* __restrict__ p_in, double p_uniform) {
+  using PH = typename S::hpop;
+  using PG = typename S::gpop;
+  const int2 wk = work[blockIdx.x];
+  const LatDesc& D = descs[wk.x];
+  PH* hb = static_cast<PH*>(D.pop[parity][0]);
+  PG* gb = static_cast<PG*>(D.pop[parity][1]);
+  const Shift shh{(float)D.prm.c_ref, (float)(1.0 / D.prm.h_scale), (float)D.prm.h_scale};
+  const Shift shg{(float)D.prm.p_ref, (float)(1.0 / D.prm.g_scale), (float)D.prm.g_scale};
+  const double rho0 = D.prm.rho0, rho1 = D.prm.rho1;
+  const int64_t n = D.n, i0 = (int64_t)wk.y * CHUNK;
+  const int64_t iend = i0 + CHUNK < n ? i0 + CHUNK : n;
+  for (int64_t i = i0 + threadIdx.x; i < iend; i += CTA) {
+    const int64_t a = pbase(i), q = D.ref_of[i];
+    const double c = c_in[q], p = p_in ? p_in[q] : p_uniform;
+    const double rho = rho1 + (rho0 - rho1) * c;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      double hv, gv;
+      equilibrium_k(k, c, p, rho, 0.0, 0.0, 0.0, hv, gv);
+      st_pop<HV<S>>(hb, a + k * AOSOA, k, (typename S::real)hv, shh);
+      st_pop<GV<S>>(gb, a + k * AOSOA, k, (typename S::real)gv, shg);
+    }
+  }
+}
+
 // M = sum c, W = sum c(1-c)^+ of the post-stream state (reference
 // k_mass_weight :1109-1126) into ctl->M, ctl->W, and the lambda of a queued
 // correction as P1 forms it.

@@ -8,8 +8,9 @@
 //    remaining work, up to fill_sites sites, as one batch (the GPU's
 //    throughput saturates at a few million sites, so adding more solves to a
 //    chunk only slows every member's step rate);
-//  * overlap: a prep thread builds initial states on the host ahead of
-//    admission, creator threads build engines and a finisher thread
+//  * overlap: a prep thread builds the order parameter of each initial state
+//    on the host ahead of admission (the device builds the equilibrium
+//    state from it), creator threads build engines and a finisher thread
 //    reads back retired solves, all on their engines' own streams while
 //    chunks run, so the loop thread only launches chunks and changes batch
 //    membership; retired engines are freed by the loop after a chunk
@@ -41,7 +42,8 @@ using Clock = std::chrono::steady_clock;
 struct Req {
   fe_request r;               // arrays are held by the owned vectors below
   std::vector<uint8_t> solid;
-  std::vector<double> h0, g0;
+  std::vector<double> h0, g0;  // a given initial state, or
+  std::vector<double> c0;      // the order parameter of the built one (equilibrium at rest, init_p)
   int64_t sites = 0;
   double t_submit = 0.0;
   bool ready = false;         // initial state present (given, or built by the prep thread)
@@ -195,19 +197,24 @@ struct fe_server {
     }
     int rc = fe_engine_create(&p, q.r.nx, q.r.ny, q.r.nz, q.solid.data(), cfg.device, &L.e);
     if (rc) { fail(L, rc); return false; }
-    const int64_t vn = 19 * q.sites;
-    if ((rc = fe_upload_state(L.e, q.h0.data(), q.g0.data(), vn))) { fail(L, rc); return false; }
+    if (!q.c0.empty())  // built on the device from c (n values across the link, not 38n)
+      rc = fe_upload_equilibrium(L.e, q.c0.data(), nullptr, q.r.init_p, q.sites);
+    else
+      rc = fe_upload_state(L.e, q.h0.data(), q.g0.data(), 19 * q.sites);
+    if (rc) { fail(L, rc); return false; }
     std::vector<double>().swap(q.h0);  // the state lives on the device now
     std::vector<double>().swap(q.g0);
+    std::vector<double>().swap(q.c0);
     std::vector<uint8_t>().swap(q.solid);
     if (p.correct_op_mass && (rc = fe_record_target_mass(L.e))) { fail(L, rc); return false; }
     if ((rc = fe_current_mass(L.e, &L.mass0))) { fail(L, rc); return false; }
     return true;
   }
 
-  // Builds the initial states of queued solves (oldest first) on the host,
-  // ahead of their admission, so the loop thread only creates engines and
-  // uploads. Queue elements stay in place: the loop pops only ready ones.
+  // Builds the order parameter of queued solves' initial states (oldest
+  // first) on the host, ahead of their admission; the creator thread uploads
+  // it and the device builds the equilibrium state from it. Queue elements
+  // stay in place: the loop pops only ready ones.
   void prep_loop() {
     for (;;) {
       Req* q = nullptr;
@@ -223,15 +230,11 @@ struct fe_server {
         q = next();
         q->preparing = true;
       }
-      std::vector<double> c(q->sites), pr(q->sites, q->r.init_p), h(19 * q->sites), gg(19 * q->sites);
-      int rc = fe_init_order_parameter(q->solid.data(), q->r.nx, q->r.ny, q->r.nz, q->r.init_kind, q->r.init_a,
-                                       q->r.init_width, c.data());
-      if (!rc)
-        rc = fe_init_equilibrium(q->sites, c.data(), pr.data(), nullptr, nullptr, nullptr, q->r.params.rho0,
-                                 q->r.params.rho1, h.data(), gg.data());
+      std::vector<double> c(q->sites);
+      const int rc = fe_init_order_parameter(q->solid.data(), q->r.nx, q->r.ny, q->r.nz, q->r.init_kind,
+                                             q->r.init_a, q->r.init_width, c.data());
       std::lock_guard<std::mutex> g(mu);
-      q->h0.swap(h);
-      q->g0.swap(gg);
+      q->c0.swap(c);
       q->prep_status = rc;
       if (rc) q->prep_message = fe_last_error();
       q->preparing = false;

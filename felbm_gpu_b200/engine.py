@@ -207,6 +207,21 @@ class MultiPhaseGPU:
         g = np.ascontiguousarray(g, dtype=np.float64)
         check(lib.fe_upload_state(self._h, _dptr(h), _dptr(g), self.Vn))
 
+    def upload_equilibrium(self, c: np.ndarray, p=1.0):
+        """The equilibrium state at rest of the per-site order parameter c
+        and pressure p (an array of n values or one number), built on the
+        device: the state upload_state gives for geometry.equilibrium(c, p)."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        if c.size != self.n:
+            raise ValueError(f"c holds {c.size} values, the lattice has {self.n} sites")
+        if np.ndim(p) == 0:
+            check(lib.fe_upload_equilibrium(self._h, _dptr(c), None, float(p), self.n))
+        else:
+            pa = np.ascontiguousarray(p, dtype=np.float64)
+            if pa.size != self.n:
+                raise ValueError(f"p holds {pa.size} values, the lattice has {self.n} sites")
+            check(lib.fe_upload_equilibrium(self._h, _dptr(c), _dptr(pa), 0.0, self.n))
+
     def download_state(self, h: np.ndarray = None, g: np.ndarray = None):
         """The state as FP64 (h, g) in the reference layout f[k*n + i]. Given
         h and g (contiguous float64 arrays of 19 n entries), writes into them

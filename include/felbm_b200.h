@@ -237,6 +237,13 @@ void* fe_engine_stream(fe_engine* e);
  * (narrowed on the host, the conversion the device would apply); the
  * stored state is the same either way. */
 int fe_upload_state(fe_engine* e, const double* h, const double* g, int64_t vn);
+/* No counterpart in the reference: the equilibrium state at rest of per-site
+ * order parameter c and pressure p (n doubles each, reference site order;
+ * p NULL: p_uniform at every site), built on the device. The stored state is
+ * the one fe_upload_state gives for the arrays of fe_init_equilibrium(n, c,
+ * p, NULL, NULL, NULL, ...), from n (or 2n) values across the link instead
+ * of 38n. */
+int fe_upload_equilibrium(fe_engine* e, const double* c, const double* p, double p_uniform, int64_t n);
 /* Replaces download_state (multiphase_gpu.cuh:449-455); includes a pending
  * order-parameter mass correction, as the reference's state would. Storages
  * other than FE_F64 hold FP32 values, which large downloads move as FP32 and

@@ -70,6 +70,10 @@ class MultiPhaseGPU {
   }
   // :354-359 (host FP64, layout k*n+i)
   void upload_state(const double* h, const double* g) { check(fe_upload_state(e_, h, g, Vn_)); }
+  // the equilibrium state at rest of per-site c and p (p null: p_uniform)
+  void upload_equilibrium(const double* c, const double* p, double p_uniform = 1.0) {
+    check(fe_upload_equilibrium(e_, c, p, p_uniform, Vn_ / 19));
+  }
   // :449-455
   void download_state(std::vector<double>& h, std::vector<double>& g) {
     h.resize(Vn_);
