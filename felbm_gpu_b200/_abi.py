@@ -101,7 +101,7 @@ class FeTracerConfig(C.Structure):
 class FeServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("max_active", C.c_int), ("hbm_reserve_frac", C.c_double),
                 ("chunk_steps", C.c_int), ("storage", C.c_int), ("fill_sites", C.c_int64),
-                ("pop_layout", C.c_int)]
+                ("pop_layout", C.c_int), ("latency_first", C.c_int)]
 
 
 class FeRequest(C.Structure):

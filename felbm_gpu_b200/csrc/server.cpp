@@ -329,15 +329,25 @@ struct fe_server {
   }
 
   // The chunk's running set: least remaining work first, up to fill_sites.
+  // latency_first also caps it at the sites that keep the step of the solve
+  // with the least remaining work within twice its step alone: a step costs
+  // about a launch floor plus sites / rate, the floor worth STEP_FLOOR_SITES
+  // sites on a B200 (about 25 us at 5 G site updates a second), so that cap
+  // is 2 s1 + STEP_FLOOR_SITES. Small requests then finish at about their
+  // own step rate instead of a large member's; a backlog of many solves
+  // submitted at once loses throughput to the smaller chunks.
+  static constexpr int64_t STEP_FLOOR_SITES = 131072;
   std::vector<int> choose() {
     std::vector<int> idx(live.size());
     for (size_t q = 0; q < live.size(); ++q) idx[q] = (int)q;
     auto work = [&](int q) { return (double)live[q].q.sites * (double)(live[q].q.r.steps - live[q].done); };
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return work(a) < work(b); });
     std::vector<int> run;
-    int64_t sites = 0;
+    int64_t sites = 0, cap = cfg.fill_sites;
+    if (cfg.latency_first && cap > 0 && !idx.empty())
+      cap = std::min<int64_t>(cap, 2 * live[idx[0]].q.sites + STEP_FLOOR_SITES);
     for (int q : idx) {
-      if (!run.empty() && cfg.fill_sites > 0 && sites + live[q].q.sites > cfg.fill_sites) continue;
+      if (!run.empty() && cap > 0 && sites + live[q].q.sites > cap) continue;
       run.push_back(q);
       sites += live[q].q.sites;
     }

@@ -44,9 +44,9 @@ class Server:
 
     def __init__(self, storage: str = "f32", device: int = 0, max_active: int = 0,
                  hbm_reserve_frac: float = 0.1, chunk_steps: int = 100, fill_sites: int = 2_000_000,
-                 pop_layout: str = "two_buffers"):
+                 pop_layout: str = "two_buffers", latency_first: bool = False):
         cfg = capi.FeServerConfig(device, max_active, hbm_reserve_frac, chunk_steps, capi.STORAGE[storage],
-                                  fill_sites, {"two_buffers": 0, "in_place": 1}[pop_layout])
+                                  fill_sites, {"two_buffers": 0, "in_place": 1}[pop_layout], int(latency_first))
         h = C.c_void_p()
         check(lib.fe_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

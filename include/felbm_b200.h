@@ -428,6 +428,12 @@ typedef struct fe_server_config {
   int pop_layout;             /* FE_POP_TWO_BUFFERS or FE_POP_IN_PLACE (FE_F64 /
                                  FE_F32 storage): the population layout of
                                  every solve, and of its charged footprint  */
+  int latency_first;          /* nonzero (with fill_sites > 0): a chunk also
+                                 holds no more sites than 2 s1 + 131072, s1
+                                 the sites of its solve with the least
+                                 remaining work, so small requests step at
+                                 about their own rate (lower time-to-result
+                                 under light load, fewer sites a chunk)     */
 } fe_server_config;
 typedef struct fe_request {
   int64_t id;

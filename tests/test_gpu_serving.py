@@ -58,10 +58,13 @@ def collect(srv, count, timeout=300.0):
     return out
 
 
-@pytest.mark.parametrize("storage", ["f32", "f64"])
-def test_served_equals_alone(require_gpu, storage):
+@pytest.mark.parametrize("storage,latency_first", [("f32", False), ("f64", False), ("f32", True)])
+def test_served_equals_alone(require_gpu, storage, latency_first):
+    """Each served result bit-equal to the solve alone, with the default
+    chunks and with latency-first chunks (which split the resident solves
+    into smaller batches)."""
     specs = [solve_spec(k) for k in range(8)]
-    srv = Server(storage=storage, max_active=3, chunk_steps=16)
+    srv = Server(storage=storage, max_active=3, chunk_steps=16, latency_first=latency_first)
     try:
         for k in range(4):
             p, solid, init, W, steps = specs[k]
