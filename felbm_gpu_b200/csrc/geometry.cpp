@@ -378,37 +378,48 @@ int fe_geom_sites(const uint8_t* solid, int nx, int ny, int nz, int64_t* n, int6
 int fe_init_order_parameter(const uint8_t* solid, int nx, int ny, int nz, int kind, const double* a,
                             double width, double* c_out) {
   if (!solid || !c_out || !a) return fe_fail(FE_ERR_ARG, "fe_init_order_parameter: bad arguments");
-  const int64_t total = (int64_t)nx * ny * nz;
-  int64_t s = 0;
   const int N[3] = {nx, ny, nz};
-  for (int64_t node = 0; node < total; ++node) {
-    if (solid[node]) continue;
-    const double x = (double)(node % nx), y = (double)((node / nx) % ny), z = (double)(node / ((int64_t)nx * ny));
-    double c;
-    if (kind == 0) {
-      c = a[0];
-    } else if (kind == 1) {
+  auto value = [&](double x, double y, double z) -> double {
+    if (kind == 0) return a[0];
+    const double pos[3] = {x, y, z};
+    if (kind == 1) {
       const int axis = (int)a[3];
-      const double pos[3] = {x, y, z};
       const double L = N[axis], T = a[4];
       double sd = std::fmod(pos[axis] - a[axis], L);
       if (sd < 0) sd += L;
       // sd in [0, L): inside when sd + 0.5 in (0, T)
       const double u = sd + 0.5;
-      double d = (u < T) ? std::min(u, T - u) : -std::min(u - T, L - u);
-      c = 0.5 * (1.0 + std::tanh(2.0 * d / width));
-    } else {
-      const double pos[3] = {x, y, z};
-      double r2 = 0.0;
-      for (int q = 0; q < 3; ++q) {
-        double dd = std::fabs(pos[q] - a[q]);
-        dd = std::min(dd, N[q] - dd);
-        r2 += dd * dd;
-      }
-      const double d = a[3] - std::sqrt(r2);
-      c = 0.5 * (1.0 + std::tanh(2.0 * d / width));
+      const double d = (u < T) ? std::min(u, T - u) : -std::min(u - T, L - u);
+      return 0.5 * (1.0 + std::tanh(2.0 * d / width));
     }
-    c_out[s++] = c;
+    double r2 = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      double dd = std::fabs(pos[q] - a[q]);
+      dd = std::min(dd, N[q] - dd);
+      r2 += dd * dd;
+    }
+    const double d = a[3] - std::sqrt(r2);
+    return 0.5 * (1.0 + std::tanh(2.0 * d / width));
+  };
+  // sites in node order: the fluid nodes of each (z, y) row are counted,
+  // the rows' first sites follow by prefix sum, then rows fill in parallel
+  const int64_t rows = (int64_t)ny * nz;
+  std::vector<int64_t> first(rows + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < rows; ++r) {
+    const uint8_t* row = solid + r * nx;
+    int64_t k = 0;
+    for (int x = 0; x < nx; ++x) k += row[x] == 0;
+    first[r + 1] = k;
+  }
+  for (int64_t r = 0; r < rows; ++r) first[r + 1] += first[r];
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < rows; ++r) {
+    const uint8_t* row = solid + r * nx;
+    const double y = (double)(r % ny), z = (double)(r / ny);
+    int64_t s = first[r];
+    for (int x = 0; x < nx; ++x)
+      if (!row[x]) c_out[s++] = value((double)x, y, z);
   }
   return FE_OK;
 }
