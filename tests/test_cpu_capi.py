@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from felbm_gpu_b200 import _capi, default_params, geometry
 
@@ -106,6 +107,54 @@ def test_equilibrium_moments():
     assert np.allclose(h.reshape(19, -1).sum(0), c, atol=1e-15)
     assert np.allclose(g.reshape(19, -1).sum(0), 0.7, atol=1e-15)
     del m
+
+
+def _order_parameter_np(solid, kind, width, a):
+    """The initial order parameter per site in node order, restated with
+    numpy: slab of thickness a[4] from a[axis] along axis a[3] (periodic),
+    droplet of radius a[3] at a[0:3] (periodic), or uniform a[0]."""
+    nz, ny, nx = solid.shape
+    z, y, x = np.nonzero(solid == 0)
+    pos = [x.astype(np.float64), y.astype(np.float64), z.astype(np.float64)]
+    N = [nx, ny, nz]
+    if kind == 0:
+        return np.full(x.size, a[0])
+    if kind == 1:
+        ax = int(a[3])
+        L, T = float(N[ax]), a[4]
+        sd = np.fmod(pos[ax] - a[ax], L)
+        sd = np.where(sd < 0, sd + L, sd)
+        u = sd + 0.5
+        d = np.where(u < T, np.minimum(u, T - u), -np.minimum(u - T, L - u))
+    else:
+        r2 = np.zeros(x.size)
+        for q in range(3):
+            dd = np.abs(pos[q] - a[q])
+            dd = np.minimum(dd, N[q] - dd)
+            r2 += dd * dd
+        d = a[3] - np.sqrt(r2)
+    return 0.5 * (1.0 + np.tanh(2.0 * d / width))
+
+
+@pytest.mark.parametrize("shape", [(9, 7, 13), (1, 40, 33), (6, 1, 1), (12, 12, 12)])
+def test_initial_order_parameter(shape):
+    """fe_init_order_parameter (rows filled in parallel from per-row site
+    counts) against a numpy restatement: site order and values, for the
+    uniform, slab (each axis) and droplet fields on a random mask."""
+    rng = np.random.default_rng(sum(shape))
+    solid = (rng.random(shape) < 0.4).astype(np.uint8)
+    nz, ny, nx = shape
+    runs = [("uniform", 0, dict(c=0.3), [0.3, 0, 0, 0, 0]),
+            ("droplet", 2, dict(centre=(nx / 2, ny / 3, nz / 4), radius=3.0), [nx / 2, ny / 3, nz / 4, 3.0, 0])]
+    for ax in range(3):
+        o = (1.5, 2.0, 0.5)
+        runs.append(("slab", 1, dict(origin=o, axis=ax, thickness=[nx, ny, nz][ax] / 3.0),
+                     [o[0], o[1], o[2], float(ax), [nx, ny, nz][ax] / 3.0]))
+    for name, kind, kw, a in runs:
+        c = geometry.order_parameter(solid, name, 4.0, **kw)
+        want = _order_parameter_np(solid, kind, 4.0, a)
+        assert c.shape == want.shape
+        assert np.max(np.abs(c - want), initial=0.0) <= 1e-15, (name, a)
 
 
 def test_autotune_table_round_trip(tmp_path):
